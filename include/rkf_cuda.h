@@ -1,0 +1,452 @@
+/*
+ * rkf_cuda.h — C ABI of the B200 (sm_100a) SDF ray-march engine.
+ *
+ * This header is the drop-in boundary for the RKIField march path.  Every
+ * entry point names the reference interface it replaces (paths are relative
+ * to the RKIField workspace root).  The ABI is plain C: POD structs, raw
+ * pointers and sizes, status codes; no exceptions or aborts cross it.
+ *
+ * Ownership: the caller owns every host buffer it passes; a context owns all
+ * device memory it allocates.  Output buffers may be host or device pointers
+ * (see rkf_mem_kind).  A context is externally synchronised for import, edit
+ * and direct march calls; rkf_submit / rkf_poll are thread-safe.
+ */
+#ifndef RKF_CUDA_H
+#define RKF_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RKF_ABI_VERSION 1u
+
+#if defined(__GNUC__)
+#define RKF_API __attribute__((visibility("default")))
+#else
+#define RKF_API
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                             */
+/* ------------------------------------------------------------------------ */
+typedef enum rkf_status {
+    RKF_OK = 0,
+    RKF_INVALID_ARG = 1,   /* bad pointer, size, enum or layout            */
+    RKF_OOM = 2,           /* device allocation failed / budget exceeded   */
+    RKF_CUDA_ERROR = 3,    /* a CUDA runtime call failed                    */
+    RKF_TIMEOUT = 4,       /* rkf_poll timed out / bounded device wait hit  */
+    RKF_BUSY = 5,          /* admission refused: no slot or memory budget  */
+    RKF_EPOCH_STALE = 6,   /* request pinned an epoch that was retired     */
+    RKF_NOT_READY = 7,     /* result not complete yet (non-blocking poll)  */
+    RKF_UNSUPPORTED = 8,   /* feature not available on this device/build   */
+    RKF_CANCELLED = 9      /* request was cancelled before completion      */
+} rkf_status;
+
+/* ------------------------------------------------------------------------ */
+/* Reference-layout sentinels and constants                                 */
+/* crates/rkf-core/src/brick_map.rs:31-37 and ray_march.wgsl:25-48          */
+/* ------------------------------------------------------------------------ */
+#define RKF_EMPTY_SLOT    0xFFFFFFFFu
+#define RKF_INTERIOR_SLOT 0xFFFFFFFEu
+#define RKF_BRICK_DIM     8u
+#define RKF_BRICK_VOXELS  512u
+
+/* sdf_type / primitive_type / blend_mode of rkf_gpu_object
+ * (crates/rkf-render/src/gpu_object.rs:97-125). */
+#define RKF_SDF_NONE        0u
+#define RKF_SDF_ANALYTICAL  1u
+#define RKF_SDF_VOXELIZED   2u
+#define RKF_PRIM_SPHERE   0u
+#define RKF_PRIM_BOX      1u
+#define RKF_PRIM_CAPSULE  2u
+#define RKF_PRIM_TORUS    3u
+#define RKF_PRIM_CYLINDER 4u
+#define RKF_PRIM_PLANE    5u
+
+/* ------------------------------------------------------------------------ */
+/* Reference structs, byte-for-byte                                         */
+/* ------------------------------------------------------------------------ */
+
+/* CameraUniforms, 144 B (crates/rkf-render/src/camera.rs:196-213).
+ * right/up are pre-scaled by tan(fov/2)*aspect and tan(fov/2)
+ * (camera.rs:161-184).  prev_vp is column-major. */
+typedef struct rkf_camera {
+    float position[4];
+    float forward[4];
+    float right[4];
+    float up[4];
+    float resolution[2];
+    float jitter[2];
+    float prev_vp[16];
+} rkf_camera;
+
+/* SceneUniforms, 16 B (crates/rkf-render/src/gpu_scene.rs:23-43). */
+typedef struct rkf_scene_uniforms {
+    uint32_t num_objects;
+    uint32_t max_steps;
+    float max_distance;
+    float hit_threshold;
+} rkf_scene_uniforms;
+
+/* GpuObject, 256 B (crates/rkf-render/src/gpu_object.rs:41-95). */
+typedef struct rkf_gpu_object {
+    float inverse_world[16]; /* column-major mat4 */
+    float aabb_min[4];
+    float aabb_max[4];
+    uint32_t brick_map_offset;
+    uint32_t brick_map_dims[3];
+    float voxel_size;
+    uint32_t material_id;
+    uint32_t sdf_type;
+    uint32_t blend_mode;
+    float blend_radius;
+    float sdf_params[4];
+    float accumulated_scale[3];
+    uint32_t lod_level;
+    uint32_t object_id;
+    uint32_t primitive_type;
+    float geometry_aabb_min[3];
+    float geometry_aabb_max[3];
+    float _padding[15];
+} rkf_gpu_object;
+
+/* ------------------------------------------------------------------------ */
+/* March parameters: SceneUniforms plus the shader's compile-time constants */
+/* as explicit fields (ray_march.wgsl:28-41).                               */
+/* ------------------------------------------------------------------------ */
+typedef struct rkf_march_params {
+    rkf_scene_uniforms scene;        /* num_objects is filled by the ctx   */
+    uint32_t hard_max_steps;         /* HARD_MAX_STEPS = 1024              */
+    uint32_t bisect_steps;           /* BISECT_STEPS = 8                   */
+    float min_step;                  /* MIN_STEP = 0.0005                  */
+    float near_surface_threshold;    /* NEAR_SURFACE_THRESHOLD = 0.02      */
+} rkf_march_params;
+
+/* Fill p with the reference defaults (gpu_scene.rs:34-43, ray_march.wgsl:28-41). */
+RKF_API void rkf_march_params_default(rkf_march_params* p);
+
+/* ------------------------------------------------------------------------ */
+/* Context                                                                  */
+/* ------------------------------------------------------------------------ */
+typedef struct rkf_ctx rkf_ctx;
+
+/* Distance-plane storage precision of the device pool. */
+typedef enum rkf_precision {
+    RKF_PRECISION_F16 = 0,  /* reference VoxelSample distance (default)     */
+    RKF_PRECISION_F32 = 1,  /* full float distances                          */
+    RKF_PRECISION_U8 = 2    /* band-normalised u8 with a per-brick scale     */
+} rkf_precision;
+
+typedef enum rkf_mem_kind {
+    RKF_MEM_HOST = 0,       /* pointers are host memory (pageable or pinned) */
+    RKF_MEM_DEVICE = 1      /* pointers are device memory of ctx's device    */
+} rkf_mem_kind;
+
+typedef struct rkf_config {
+    int device;                     /* CUDA ordinal                          */
+    uint32_t pool_capacity_bricks;  /* slots reserved for the brick pool     */
+    uint32_t precision;             /* rkf_precision                         */
+    uint32_t keep_reference_pool;   /* also keep the AoS VoxelSample pool    */
+                                    /* (needed by rkf_march_plain)           */
+    uint64_t mem_budget_bytes;      /* serving admission budget, 0 = auto    */
+    uint32_t max_inflight;          /* serving slots, 0 = default (64)       */
+    uint32_t reserved[7];
+} rkf_config;
+
+RKF_API void rkf_config_default(rkf_config* cfg);
+
+/* Replaces RenderContext + GpuScene construction
+ * (crates/rkf-render/src/context.rs:29, gpu_scene.rs:52). */
+RKF_API rkf_status rkf_create(const rkf_config* cfg, rkf_ctx** out);
+RKF_API rkf_status rkf_destroy(rkf_ctx* ctx);
+/* Human-readable message for the last failed call on this thread. */
+RKF_API const char* rkf_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* Scene import (the reference's upload path)                               */
+/* ------------------------------------------------------------------------ */
+
+/* Upload reference VoxelSample bricks (2 u32 per voxel, x+8y+64z within a
+ * brick) into slots [first_slot, first_slot+n_bricks).
+ * Replaces the whole-pool write_buffer of render.rs:106-126 and
+ * GpuScene::set_brick_pool (gpu_scene.rs:231). */
+RKF_API rkf_status rkf_pool_import_voxelsample(rkf_ctx* ctx, const uint32_t* words,
+                                       uint32_t first_slot, uint32_t n_bricks);
+
+/* Upload the packed BrickMapAllocator buffer (brick_map.rs:246 as_slice).
+ * Replaces GpuScene::upload_brick_maps (gpu_scene.rs:170). */
+RKF_API rkf_status rkf_brickmap_import(rkf_ctx* ctx, const uint32_t* packed, uint64_t n);
+
+/* Upload GpuObject records.  Replaces GpuScene::upload_objects
+ * (gpu_scene.rs:141).  Builds the device two-level brick index for every
+ * voxelized object from the imported brick maps. */
+RKF_API rkf_status rkf_objects_import(rkf_ctx* ctx, const rkf_gpu_object* objects, uint32_t n);
+
+/* Counts of what the context holds. */
+typedef struct rkf_scene_info {
+    uint32_t num_objects;
+    uint32_t pool_bricks_used;
+    uint32_t pool_capacity;
+    uint32_t leaf_blocks;
+    uint64_t device_bytes;
+    uint64_t epoch;
+} rkf_scene_info;
+RKF_API rkf_status rkf_scene_info_get(rkf_ctx* ctx, rkf_scene_info* out);
+
+/* Download n_bricks of the device pool as reference VoxelSample words
+ * (inverse of rkf_pool_import_voxelsample; used to cross-check). */
+RKF_API rkf_status rkf_pool_export_voxelsample(rkf_ctx* ctx, uint32_t first_slot,
+                                       uint32_t n_bricks, uint32_t* words);
+/* Look up the slot (or sentinel) of brick (bx,by,bz) of object obj. */
+RKF_API rkf_status rkf_brick_lookup(rkf_ctx* ctx, uint32_t obj, const uint32_t* bxyz,
+                            uint32_t n, uint32_t* slots);
+
+/* ------------------------------------------------------------------------ */
+/* Seeded synthetic scenes built on the device                              */
+/* ------------------------------------------------------------------------ */
+
+/* One analytic primitive of a seeded synthetic scene (object-local metres).
+ * type: RKF_PRIM_SPHERE / BOX / CAPSULE.  rot is row-major R with
+ * local = R^T (p - centre).  params: sphere r; box hx,hy,hz; capsule r,h. */
+typedef struct rkf_prim {
+    uint32_t type;
+    uint32_t material;
+    float centre[3];
+    float params[3];
+    float rot[9];
+    float bound_radius;
+} rkf_prim;
+
+/* Band rule used to decide which bricks are allocated. */
+typedef enum rkf_band_rule {
+    RKF_BAND_VOXELS = 0,   /* any voxel |d| <= band_voxels*vs; deep interior  */
+                           /* bricks become INTERIOR_SLOT                     */
+    RKF_BAND_REFERENCE = 1 /* voxelize_object.rs:86-109: |d(centre)| < 1.8 *  */
+                           /* brick extent, everything else EMPTY_SLOT        */
+} rkf_band_rule;
+
+typedef struct rkf_voxelize_params {
+    float voxel_size;       /* metres                                         */
+    float smooth_k;         /* smooth-min radius (sdf.rs:48)                  */
+    float band_voxels;      /* narrow band half-width in voxels (3)           */
+    float cut_distance;     /* prims with |p-c|-bound >= cut are ignored      */
+    float aabb_min[3];      /* local-space AABB to voxelize                   */
+    float aabb_max[3];
+    uint32_t band_rule;     /* rkf_band_rule                                  */
+    uint32_t object_id;
+} rkf_voxelize_params;
+
+/* Voxelize the smooth union of prims into the device pool as one object
+ * (voxelize_sdf, crates/rkf-core/src/voxelize_object.rs:53-182), appending a
+ * GpuObject with identity transform.  Output slot order is the reference's
+ * z,y,x brick loop order starting at the pool's first free slot. */
+RKF_API rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, uint32_t n_prims,
+                              const rkf_voxelize_params* vp, uint32_t* out_object_index);
+
+/* Fetch object record i as the device holds it. */
+RKF_API rkf_status rkf_object_get(rkf_ctx* ctx, uint32_t i, rkf_gpu_object* out);
+
+/* ------------------------------------------------------------------------ */
+/* G-buffer march (replaces RayMarchPass::dispatch, ray_march.rs:96-118)     */
+/* ------------------------------------------------------------------------ */
+
+/* Per-ray flags written to rkf_gbuffer.flags */
+#define RKF_FLAG_HIT       0x1u
+#define RKF_FLAG_BISECTED  0x2u   /* hit found by the overstep bisection    */
+#define RKF_FLAG_STEPS_OUT 0x4u   /* ended by the near-step or hard budget  */
+
+/* SoA G-buffer.  Required planes: t, normal (3 floats per ray), slot,
+ * material, flags.  Optional reference-format planes (may be NULL):
+ * position = hit_pos.xyz + t (ray_march.wgsl:1091), packed_material
+ * (:1087-1090), motion = motion.xy, 1, sdf_at_hit (:1095-1105). */
+typedef struct rkf_gbuffer {
+    float* t;
+    float* normal;
+    uint32_t* slot;
+    uint16_t* material;
+    uint16_t* flags;
+    float* position;
+    uint32_t* packed_material;
+    float* motion;
+    uint32_t mem;            /* rkf_mem_kind of every pointer above          */
+    uint32_t _pad;
+} rkf_gbuffer;
+
+/* The B200 march: SoA distance plane at the context precision, two-level
+ * brick index with empty-brick read skipping, warp-compacted persistent
+ * kernel.  Bit-identical results to the reference algorithm in FP32. */
+RKF_API rkf_status rkf_march(rkf_ctx* ctx, const rkf_camera* cam, const rkf_march_params* p,
+                     uint32_t width, uint32_t height, rkf_gbuffer* out);
+
+/* The plain march: one launch, one thread per ray, reference AoS pool and
+ * the reference loop order.  The baseline the batched path is measured
+ * against. */
+RKF_API rkf_status rkf_march_plain(rkf_ctx* ctx, const rkf_camera* cam, const rkf_march_params* p,
+                           uint32_t width, uint32_t height, rkf_gbuffer* out);
+
+/* ------------------------------------------------------------------------ */
+/* Generic ray casts (secondary rays; shade_common_shading.wgsl:9-47)        */
+/* ------------------------------------------------------------------------ */
+typedef enum rkf_trace_mode {
+    RKF_TRACE_CLOSEST = 0,  /* full march: t, normal, material, slot          */
+    RKF_TRACE_ANY = 1,      /* any-hit: stop at the first surface (no bisect) */
+    RKF_TRACE_SHADOW = 2    /* soft_shadow (shade_common_shading.wgsl:9-33)   */
+} rkf_trace_mode;
+
+typedef struct rkf_hits {
+    float* t;          /* closest/any: hit t or MAX_FLOAT; shadow: factor    */
+    float* normal;     /* closest only (may be NULL)                         */
+    uint32_t* slot;    /* closest only (may be NULL)                         */
+    uint16_t* material;/* closest only (may be NULL)                         */
+    uint16_t* flags;   /* may be NULL                                        */
+    uint32_t mem;
+    uint32_t _pad;
+} rkf_hits;
+
+/* Rays: origins[3n], dirs[3n], tmax[n] (per-ray max_distance), mem kind of
+ * the inputs = in_mem. */
+RKF_API rkf_status rkf_trace_rays(rkf_ctx* ctx, const float* origins, const float* dirs,
+                          const float* tmax, uint32_t n, uint32_t mode,
+                          const rkf_march_params* p, uint32_t in_mem, rkf_hits* out);
+
+/* ------------------------------------------------------------------------ */
+/* Point queries: SdfQueryable::{evaluate, gradient}                         */
+/* (crates/rkf-physics/src/sdf_collision.rs:38-56)                          */
+/* ------------------------------------------------------------------------ */
+/* points[3n] -> dist[n] (min over objects, evaluate_object), grad[3n] (unit
+ * normal of the closest object, compute_normal_for_object; may be NULL),
+ * material[n] (may be NULL).  mem applies to all pointers. */
+RKF_API rkf_status rkf_query_points(rkf_ctx* ctx, const float* points, uint32_t n,
+                            float* dist, float* grad, uint16_t* material, uint32_t mem);
+
+/* ------------------------------------------------------------------------ */
+/* CSG edits (crates/rkf-edit/src/edit_op.rs:15, cpu_apply.rs:28-229)       */
+/* ------------------------------------------------------------------------ */
+typedef struct rkf_edit_op {
+    uint32_t object_index;   /* index into the object table                  */
+    uint32_t edit_type;      /* EditType: 0 union 1 subtract 2 intersect     */
+                             /* 3 smooth union 4 smooth subtract             */
+    uint32_t shape_type;     /* ShapeType: 0 sphere 1 box 2 capsule          */
+    uint32_t falloff;        /* FalloffCurve: 0 linear 1 smooth 2 sharp      */
+    float position[3];       /* object-local                                 */
+    float rotation[4];       /* quaternion x,y,z,w                           */
+    float dimensions[3];
+    float strength;
+    float blend_k;
+    uint32_t material_id;
+    uint32_t _pad[2];
+} rkf_edit_op;
+
+/* Apply one edit on the device: touched allocated bricks are rewritten into
+ * fresh slots (copy-on-write), EMPTY/INTERIOR bricks the brush reaches are
+ * allocated and filled, and a new index epoch is published.  Requests
+ * admitted before the call keep reading the previous epoch. */
+RKF_API rkf_status rkf_edit_csg(rkf_ctx* ctx, const rkf_edit_op* op, uint64_t* new_epoch);
+
+/* ------------------------------------------------------------------------ */
+/* Batched march: many views and ray batches in one persistent launch       */
+/* ------------------------------------------------------------------------ */
+typedef struct rkf_view {
+    rkf_camera camera;
+    uint32_t width, height;
+    rkf_gbuffer out;         /* device pointers only                         */
+} rkf_view;
+
+typedef struct rkf_ray_batch {
+    const float* origins;    /* device pointers only                         */
+    const float* dirs;
+    const float* tmax;
+    uint32_t n;
+    uint32_t mode;           /* rkf_trace_mode                               */
+    rkf_hits out;            /* device pointers only                         */
+} rkf_ray_batch;
+
+typedef struct rkf_batch_tuning {
+    uint32_t tile_w, tile_h;     /* ray-tile shape of a work item            */
+    uint32_t step_budget;        /* iterations before a ray is re-queued     */
+    uint32_t compact_interval;   /* iterations between warp compactions      */
+    uint32_t blocks_per_sm;
+    uint32_t threads_per_block;
+} rkf_batch_tuning;
+
+/* Run every view and ray batch in one persistent work-stealing launch.
+ * tuning may be NULL (autotuned defaults).  Blocks until complete. */
+RKF_API rkf_status rkf_march_batch(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views,
+                           const rkf_ray_batch* batches, uint32_t n_batches,
+                           const rkf_march_params* p, const rkf_batch_tuning* tuning);
+
+/* Search tile shape x step budget x compaction interval on a sample of the
+ * given work and store the winner in the context.  Writes it to *out. */
+RKF_API rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views,
+                        const rkf_ray_batch* batches, uint32_t n_batches,
+                        const rkf_march_params* p, rkf_batch_tuning* out);
+
+/* ------------------------------------------------------------------------ */
+/* Serving: resident request loop with continuous batching                  */
+/* ------------------------------------------------------------------------ */
+typedef enum rkf_request_kind {
+    RKF_REQ_RENDER = 0,   /* camera render -> G-buffer                       */
+    RKF_REQ_RAYS = 1,     /* ray batch -> hits                               */
+    RKF_REQ_POINTS = 2,   /* point queries -> distance/gradient/material     */
+    RKF_REQ_EDIT = 3      /* CSG edit (ordered w.r.t. later admissions)      */
+} rkf_request_kind;
+
+typedef struct rkf_request {
+    uint32_t kind;
+    uint32_t mode;             /* rays: rkf_trace_mode                        */
+    uint32_t width, height;    /* render                                      */
+    uint32_t n;                /* rays / points                               */
+    uint32_t _pad;
+    rkf_camera camera;         /* render                                      */
+    const float* in0;          /* rays: origins | points: xyz  (host)         */
+    const float* in1;          /* rays: dirs                    (host)        */
+    const float* in2;          /* rays: tmax                    (host)        */
+    rkf_edit_op edit;          /* edit                                        */
+    /* host outputs (caller-owned, must stay valid until the result is polled) */
+    float* out_t;              /* render/rays: t; points: dist                */
+    float* out_normal;         /* render/rays/points: 3 floats per item       */
+    uint32_t* out_slot;
+    uint16_t* out_material;
+    uint16_t* out_flags;
+} rkf_request;
+
+typedef uint64_t rkf_ticket;
+
+typedef struct rkf_result {
+    rkf_status status;
+    uint32_t kind;
+    uint64_t epoch;            /* index epoch the request read               */
+    double submit_us;          /* host clock at admission                    */
+    double start_us;           /* host clock when its work was issued        */
+    double done_us;            /* host clock when its result was complete    */
+    double device_ms;          /* device time of its share of the work       */
+} rkf_result;
+
+/* Start / stop the resident serving loop (a host thread + streams). */
+RKF_API rkf_status rkf_serve_start(rkf_ctx* ctx, const rkf_march_params* p);
+RKF_API rkf_status rkf_serve_stop(rkf_ctx* ctx);
+/* Admit a request.  RKF_BUSY when no slot or memory budget is free. */
+RKF_API rkf_status rkf_submit(rkf_ctx* ctx, const rkf_request* req, rkf_ticket* ticket);
+/* Wait up to timeout_us for a ticket.  RKF_NOT_READY if still running. */
+RKF_API rkf_status rkf_poll(rkf_ctx* ctx, rkf_ticket ticket, rkf_result* out, uint32_t timeout_us);
+RKF_API rkf_status rkf_cancel(rkf_ctx* ctx, rkf_ticket ticket);
+
+/* ------------------------------------------------------------------------ */
+/* FP64 rebasing (crates/rkf-core/src/world_position.rs:107-120)            */
+/* ------------------------------------------------------------------------ */
+typedef struct rkf_world_pos {
+    int32_t chunk[3];
+    float local[3];
+} rkf_world_pos;
+
+/* out = (float)(pos - origin) computed in FP64 (relative_to_f64). */
+RKF_API void rkf_world_relative(const rkf_world_pos* pos, const rkf_world_pos* origin,
+                        double out_f64[3], float out_f32[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RKF_CUDA_H */

@@ -1,0 +1,222 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg
+import this module, as the checker or as the timed CPU baseline.  The
+product package never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from rkifield_b200 import _abi as abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "liboracle_rkf.so")
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return LIB_PATH
+
+
+class orc_scene(C.Structure):
+    _fields_ = [("pool_words", C.c_void_p), ("dist_f16", C.c_void_p), ("dist_f32", C.c_void_p),
+                ("dist_u8", C.c_void_p), ("brick_scale", C.c_void_p), ("mat_plane", C.c_void_p),
+                ("blend_plane", C.c_void_p), ("precision", C.c_uint32),
+                ("brick_maps", C.c_void_p), ("top", C.c_void_p), ("leaves", C.c_void_p),
+                ("obj_top_info", C.c_void_p), ("objects", C.c_void_p),
+                ("num_objects", C.c_uint32)]
+
+
+class orc_stats(C.Structure):
+    _fields_ = [("sectors", C.c_uint64), ("index_sectors", C.c_uint64),
+                ("dist_sectors", C.c_uint64), ("mat_sectors", C.c_uint64),
+                ("steps", C.c_uint64), ("evals", C.c_uint64)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P, U32, I = C.c_void_p, C.c_uint32, C.c_int
+        L.orc_f16_from_f32.restype = C.c_uint16
+        L.orc_f16_from_f32.argtypes = [C.c_float]
+        L.orc_f16_to_f32.restype = C.c_float
+        L.orc_f16_to_f32.argtypes = [C.c_uint16]
+        L.orc_prim_sdf.restype = C.c_float
+        L.orc_prim_sdf.argtypes = [P, P]
+        L.orc_smin.restype = C.c_float
+        L.orc_smin.argtypes = [C.c_float, C.c_float, C.c_float]
+        L.orc_scene_eval.restype = C.c_float
+        L.orc_scene_eval.argtypes = [P, U32, C.c_float, C.c_float, P, P, P, P]
+        L.orc_voxelize.restype = P
+        L.orc_voxelize.argtypes = [P, U32, P, I]
+        L.orc_voxelized_info.argtypes = [P, P, P, P]
+        L.orc_voxelized_copy.argtypes = [P, P, P]
+        L.orc_voxelized_copy_f32.argtypes = [P, P]
+        L.orc_voxelized_free.argtypes = [P]
+        L.orc_voxelize_bricks.argtypes = [P, U32, P, P, U32, P, P, I]
+        L.orc_march.argtypes = [P, P, P, U32, U32, I, I, U32, U32] + [P] * 12 + [I, P]
+        L.orc_trace_rays.argtypes = [P, P, P, P, U32, U32, P, I, I] + [P] * 7
+        L.orc_query_points.argtypes = [P, P, U32, P, P, P, I]
+        L.orc_apply_edit_brick.restype = I
+        L.orc_apply_edit_brick.argtypes = [P, P, C.c_float, P]
+        L.orc_fill_brick_with_brush.argtypes = [P, P, C.c_float, P]
+        L.orc_evaluate_falloff.restype = C.c_float
+        L.orc_evaluate_falloff.argtypes = [U32, C.c_float, C.c_float]
+        L.orc_evaluate_shape.restype = C.c_float
+        L.orc_evaluate_shape.argtypes = [U32, P, P]
+        L.orc_sample_brick_trilinear.restype = C.c_float
+        L.orc_sample_brick_trilinear.argtypes = [P, P, C.c_float]
+        L.orc_march_params_default.argtypes = [P]
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def nthreads() -> int:
+    return max(1, os.cpu_count() or 1)
+
+
+class Voxelized:
+    """Oracle voxelization of a primitive list into a fresh pool + flat map."""
+
+    def __init__(self, prims: np.ndarray, vp: abi.rkf_voxelize_params, threads: int | None = None):
+        L = lib()
+        h = L.orc_voxelize(ptr(prims), len(prims), C.byref(vp), threads or nthreads())
+        dims = np.zeros(3, np.uint32)
+        nb = C.c_uint32()
+        ni = C.c_uint32()
+        L.orc_voxelized_info(h, ptr(dims), C.byref(nb), C.byref(ni))
+        self.dims = dims
+        self.n_bricks = nb.value
+        self.n_interior = ni.value
+        self.words = np.zeros(self.n_bricks * 1024, np.uint32)
+        self.map = np.zeros(int(dims.prod()), np.uint32)
+        L.orc_voxelized_copy(h, ptr(self.words), ptr(self.map))
+        self.dist_f32 = np.zeros(self.n_bricks * 512, np.float32)
+        L.orc_voxelized_copy_f32(h, ptr(self.dist_f32))
+        L.orc_voxelized_free(h)
+        self.voxel_size = vp.voxel_size
+
+    def gpu_object(self, object_id: int = 1) -> abi.rkf_gpu_object:
+        """The object's GpuObject (identity transform, unit scale) with the
+        tight AABB of allocated bricks (brick_ops.rs:225-262)."""
+        o = abi.rkf_gpu_object()
+        for i in range(4):
+            o.inverse_world[i * 4 + i] = 1.0
+        vs = np.float32(self.voxel_size)
+        be = vs * np.float32(8.0)
+        gs = self.dims.astype(np.float32) * be
+        for a in range(3):
+            o.aabb_min[a] = float(-gs[a] * np.float32(0.5))
+            o.aabb_max[a] = float(gs[a] * np.float32(0.5))
+        o.brick_map_offset = 0
+        for a in range(3):
+            o.brick_map_dims[a] = int(self.dims[a])
+        o.voxel_size = float(vs)
+        o.sdf_type = abi.RKF_SDF_VOXELIZED
+        o.accumulated_scale[0] = o.accumulated_scale[1] = o.accumulated_scale[2] = 1.0
+        o.object_id = object_id
+        # geometry AABB of allocated bricks
+        m = self.map.reshape(int(self.dims[2]), int(self.dims[1]), int(self.dims[0]))
+        alloc = m < abi.INTERIOR_SLOT
+        if alloc.any():
+            zz, yy, xx = np.nonzero(alloc)
+            lo = np.array([xx.min(), yy.min(), zz.min()], np.float32)
+            hi = np.array([xx.max() + 1, yy.max() + 1, zz.max() + 1], np.float32)
+            gmin = lo * be - gs * np.float32(0.5)
+            gmax = hi * be - gs * np.float32(0.5)
+            for a in range(3):
+                o.geometry_aabb_min[a] = float(gmin[a])
+                o.geometry_aabb_max[a] = float(gmax[a])
+        return o
+
+
+class Scene:
+    """Keeps the arrays behind an orc_scene alive."""
+
+    def __init__(self, objects, pool_words=None, brick_maps=None, top=None, leaves=None,
+                 obj_top_info=None, dist_f16=None, dist_f32=None, dist_u8=None,
+                 brick_scale=None, mat_plane=None, blend_plane=None,
+                 precision=abi.RKF_PRECISION_F16):
+        n = len(objects)
+        self.objects = (abi.rkf_gpu_object * n)(*objects)
+        self._keep = [pool_words, brick_maps, top, leaves, obj_top_info, dist_f16, dist_f32,
+                      dist_u8, brick_scale, mat_plane, blend_plane]
+        self.s = orc_scene(ptr(pool_words), ptr(dist_f16), ptr(dist_f32), ptr(dist_u8),
+                           ptr(brick_scale), ptr(mat_plane), ptr(blend_plane), precision,
+                           ptr(brick_maps), ptr(top), ptr(leaves), ptr(obj_top_info),
+                           C.addressof(self.objects), n)
+
+
+def march(scene: Scene, cam, params, w: int, h: int, fp64: bool = False, threads: int | None = None,
+          rows: tuple[int, int] | None = None, with_reference_planes: bool = False,
+          with_margin: bool = False, with_root: bool = False, count_sectors: bool = False):
+    n = w * h
+    out = {
+        "t": np.zeros(n, np.float32), "normal": np.zeros(3 * n, np.float32),
+        "slot": np.zeros(n, np.uint32), "material": np.zeros(n, np.uint16),
+        "flags": np.zeros(n, np.uint16),
+    }
+    if with_reference_planes:
+        out["position"] = np.zeros(4 * n, np.float32)
+        out["packed_material"] = np.zeros(n, np.uint32)
+        out["motion"] = np.zeros(4 * n, np.float32)
+    if fp64:
+        out["t64"] = np.zeros(n, np.float64)
+        out["normal64"] = np.zeros(3 * n, np.float64)
+    if with_margin:
+        out["margin"] = np.full(n, np.inf)
+    if with_root and fp64:
+        out["t_root"] = np.full(n, np.nan)
+    st = orc_stats()
+    r0, r1 = rows if rows else (0, 0)
+    lib().orc_march(C.byref(scene.s), C.byref(cam), C.byref(params), w, h, int(fp64),
+                    threads or nthreads(), r0, r1, ptr(out["t"]), ptr(out["normal"]),
+                    ptr(out["slot"]), ptr(out["material"]), ptr(out["flags"]),
+                    ptr(out.get("position")), ptr(out.get("packed_material")),
+                    ptr(out.get("motion")), ptr(out.get("t64")), ptr(out.get("normal64")),
+                    ptr(out.get("margin")), ptr(out.get("t_root")), int(count_sectors),
+                    C.byref(st))
+    out["stats"] = {k: getattr(st, k) for k, _ in orc_stats._fields_}
+    return out
+
+
+def trace(scene: Scene, origins, dirs, tmax, mode: int, params, fp64: bool = False,
+          threads: int | None = None, with_margin: bool = False):
+    n = len(tmax)
+    out = {"t": np.zeros(n, np.float32), "normal": np.zeros(3 * n, np.float32),
+           "slot": np.zeros(n, np.uint32), "material": np.zeros(n, np.uint16),
+           "flags": np.zeros(n, np.uint16)}
+    if fp64:
+        out["t64"] = np.zeros(n, np.float64)
+    if with_margin:
+        out["margin"] = np.full(n, np.inf)
+    lib().orc_trace_rays(C.byref(scene.s), ptr(origins), ptr(dirs), ptr(tmax), n, mode,
+                         C.byref(params), int(fp64), threads or nthreads(), ptr(out["t"]),
+                         ptr(out["normal"]), ptr(out["slot"]), ptr(out["material"]),
+                         ptr(out["flags"]), ptr(out.get("t64")), ptr(out.get("margin")))
+    return out
+
+
+def query_points(scene: Scene, points, threads: int | None = None):
+    n = len(points) // 3
+    d = np.zeros(n, np.float32)
+    g = np.zeros(3 * n, np.float32)
+    m = np.zeros(n, np.uint16)
+    lib().orc_query_points(C.byref(scene.s), ptr(points), n, ptr(d), ptr(g), ptr(m),
+                           threads or nthreads())
+    return d, g, m

@@ -1,0 +1,270 @@
+// api.cu — public march / trace / query / batch entry points.
+//
+// Host-pointer outputs are staged in a context-owned device buffer and copied
+// back on the context stream; device-pointer outputs are written in place.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "ctx.h"
+#include "march.h"
+
+using namespace rkf;
+
+namespace detail {
+
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+// Device staging for a G-buffer of n elements; fills dev with device pointers.
+rkf_status stage_gbuffer(Ctx* c, const rkf_gbuffer& host, uint64_t n, rkf_gbuffer* dev) {
+  const size_t sz[8] = {n * 4, n * 12, n * 4, n * 2, n * 2, host.position ? n * 16 : 0,
+                        host.packed_material ? n * 4 : 0, host.motion ? n * 16 : 0};
+  size_t total = 0;
+  for (size_t s : sz) total += align256(s);
+  rkf_status st = c->stage_bytes(total);
+  if (st != RKF_OK) return st;
+  char* b = c->stage.as<char>();
+  void* ptrs[8];
+  for (int i = 0; i < 8; ++i) {
+    ptrs[i] = sz[i] ? b : nullptr;
+    b += align256(sz[i]);
+  }
+  *dev = host;
+  dev->t = static_cast<float*>(ptrs[0]);
+  dev->normal = static_cast<float*>(ptrs[1]);
+  dev->slot = static_cast<uint32_t*>(ptrs[2]);
+  dev->material = static_cast<uint16_t*>(ptrs[3]);
+  dev->flags = static_cast<uint16_t*>(ptrs[4]);
+  dev->position = static_cast<float*>(ptrs[5]);
+  dev->packed_material = static_cast<uint32_t*>(ptrs[6]);
+  dev->motion = static_cast<float*>(ptrs[7]);
+  dev->mem = RKF_MEM_DEVICE;
+  return RKF_OK;
+}
+
+rkf_status copy_back_gbuffer(Ctx* c, const rkf_gbuffer& host, const rkf_gbuffer& dev, uint64_t n) {
+  auto cp = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+    if (!dst || !src || !bytes) return cudaSuccess;
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+  };
+  RKF_CUDA_TRY(cp(host.t, dev.t, n * 4));
+  RKF_CUDA_TRY(cp(host.normal, dev.normal, n * 12));
+  RKF_CUDA_TRY(cp(host.slot, dev.slot, n * 4));
+  RKF_CUDA_TRY(cp(host.material, dev.material, n * 2));
+  RKF_CUDA_TRY(cp(host.flags, dev.flags, n * 2));
+  RKF_CUDA_TRY(cp(host.position, dev.position, n * 16));
+  RKF_CUDA_TRY(cp(host.packed_material, dev.packed_material, n * 4));
+  RKF_CUDA_TRY(cp(host.motion, dev.motion, n * 16));
+  return RKF_OK;
+}
+
+rkf_status check_common(rkf_ctx* ctx, const void* a, const rkf_march_params* p, const char* fn) {
+  if (!ctx || !a || !p) return fail(RKF_INVALID_ARG, std::string(fn) + ": null argument");
+  if (p->hard_max_steps == 0 || p->hard_max_steps > (1u << 20))
+    return fail(RKF_INVALID_ARG, std::string(fn) + ": hard_max_steps out of range");
+  if (p->bisect_steps > 64) return fail(RKF_INVALID_ARG, std::string(fn) + ": bisect_steps out of range");
+  return RKF_OK;
+}
+
+rkf_status check_gbuffer(const rkf_gbuffer* out, const char* fn) {
+  if (!out || !out->t || !out->normal || !out->slot || !out->material || !out->flags)
+    return fail(RKF_INVALID_ARG, std::string(fn) + ": G-buffer plane missing");
+  if (out->mem > RKF_MEM_DEVICE) return fail(RKF_INVALID_ARG, std::string(fn) + ": bad mem kind");
+  return RKF_OK;
+}
+
+template <class F>
+rkf_status run_gbuffer(Ctx* c, const rkf_gbuffer* out, uint64_t n, F&& launch) {
+  if (out->mem == RKF_MEM_DEVICE) {
+    rkf_status st = launch(*out);
+    if (st != RKF_OK) return st;
+    RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return RKF_OK;
+  }
+  rkf_gbuffer dev;
+  rkf_status st = stage_gbuffer(c, *out, n, &dev);
+  if (st != RKF_OK) return st;
+  st = launch(dev);
+  if (st != RKF_OK) return st;
+  st = copy_back_gbuffer(c, *out, dev, n);
+  if (st != RKF_OK) return st;
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return RKF_OK;
+}
+
+}  // namespace detail
+
+using namespace detail;
+
+extern "C" {
+
+rkf_status rkf_march(rkf_ctx* ctx, const rkf_camera* cam, const rkf_march_params* p, uint32_t width,
+                     uint32_t height, rkf_gbuffer* out) {
+  rkf_status st = check_common(ctx, cam, p, "rkf_march");
+  if (st != RKF_OK) return st;
+  if ((st = check_gbuffer(out, "rkf_march")) != RKF_OK) return st;
+  if (width == 0 || height == 0 || static_cast<uint64_t>(width) * height > (1ull << 31))
+    return fail(RKF_INVALID_ARG, "rkf_march: bad resolution");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  const uint64_t n = static_cast<uint64_t>(width) * height;
+  return run_gbuffer(c, out, n, [&](const rkf_gbuffer& dev) {
+    const rkf_batch_tuning& tu = c->tuning;
+    std::vector<Segment> segs{view_segment(cam, width, height, tu.tile_w, tu.tile_h, dev)};
+    segs[0].first = 0;
+    return launch_persistent(c, segs, segs[0].n_ids, p, tu, c->stream, &c->seg_buf,
+                             c->counters.as<unsigned long long>());
+  });
+}
+
+rkf_status rkf_march_plain(rkf_ctx* ctx, const rkf_camera* cam, const rkf_march_params* p,
+                           uint32_t width, uint32_t height, rkf_gbuffer* out) {
+  rkf_status st = check_common(ctx, cam, p, "rkf_march_plain");
+  if (st != RKF_OK) return st;
+  if ((st = check_gbuffer(out, "rkf_march_plain")) != RKF_OK) return st;
+  if (width == 0 || height == 0 || static_cast<uint64_t>(width) * height > (1ull << 31))
+    return fail(RKF_INVALID_ARG, "rkf_march_plain: bad resolution");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  const uint64_t n = static_cast<uint64_t>(width) * height;
+  return run_gbuffer(c, out, n, [&](const rkf_gbuffer& dev) {
+    return launch_plain(c, cam, p, width, height, dev, c->stream);
+  });
+}
+
+rkf_status rkf_trace_rays(rkf_ctx* ctx, const float* origins, const float* dirs, const float* tmax,
+                          uint32_t n, uint32_t mode, const rkf_march_params* p, uint32_t in_mem,
+                          rkf_hits* out) {
+  rkf_status st = check_common(ctx, p, p, "rkf_trace_rays");
+  if (st != RKF_OK) return st;
+  if (!out || !out->t || (n && (!origins || !dirs || !tmax)))
+    return fail(RKF_INVALID_ARG, "rkf_trace_rays: null argument");
+  if (mode > RKF_TRACE_SHADOW) return fail(RKF_INVALID_ARG, "rkf_trace_rays: bad mode");
+  if (in_mem > RKF_MEM_DEVICE || out->mem > RKF_MEM_DEVICE)
+    return fail(RKF_INVALID_ARG, "rkf_trace_rays: bad mem kind");
+  if (n == 0) return RKF_OK;
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  // stage inputs and outputs as needed: [o 12n][d 12n][tmax 4n] + outputs
+  const size_t in_b = in_mem == RKF_MEM_HOST ? align256(12ull * n) * 2 + align256(4ull * n) : 0;
+  const size_t out_b = out->mem == RKF_MEM_HOST
+                           ? align256(4ull * n) + align256(12ull * n) + align256(4ull * n) +
+                                 align256(2ull * n) * 2
+                           : 0;
+  if ((st = c->stage_bytes(in_b + out_b)) != RKF_OK) return st;
+  char* b = c->stage.as<char>();
+  const float *d_o = origins, *d_d = dirs, *d_t = tmax;
+  if (in_mem == RKF_MEM_HOST) {
+    RKF_CUDA_TRY(cudaMemcpyAsync(b, origins, 12ull * n, cudaMemcpyHostToDevice, c->stream));
+    d_o = reinterpret_cast<float*>(b);
+    b += align256(12ull * n);
+    RKF_CUDA_TRY(cudaMemcpyAsync(b, dirs, 12ull * n, cudaMemcpyHostToDevice, c->stream));
+    d_d = reinterpret_cast<float*>(b);
+    b += align256(12ull * n);
+    RKF_CUDA_TRY(cudaMemcpyAsync(b, tmax, 4ull * n, cudaMemcpyHostToDevice, c->stream));
+    d_t = reinterpret_cast<float*>(b);
+    b += align256(4ull * n);
+  }
+  rkf_hits dev = *out;
+  if (out->mem == RKF_MEM_HOST) {
+    dev.t = reinterpret_cast<float*>(b);
+    b += align256(4ull * n);
+    dev.normal = out->normal ? reinterpret_cast<float*>(b) : nullptr;
+    b += align256(12ull * n);
+    dev.slot = out->slot ? reinterpret_cast<uint32_t*>(b) : nullptr;
+    b += align256(4ull * n);
+    dev.material = out->material ? reinterpret_cast<uint16_t*>(b) : nullptr;
+    b += align256(2ull * n);
+    dev.flags = out->flags ? reinterpret_cast<uint16_t*>(b) : nullptr;
+    dev.mem = RKF_MEM_DEVICE;
+  }
+  std::vector<Segment> segs{ray_segment(d_o, d_d, d_t, n, mode, dev)};
+  segs[0].first = 0;
+  st = launch_persistent(c, segs, n, p, c->tuning, c->stream, &c->seg_buf,
+                         c->counters.as<unsigned long long>());
+  if (st != RKF_OK) return st;
+  if (out->mem == RKF_MEM_HOST) {
+    RKF_CUDA_TRY(cudaMemcpyAsync(out->t, dev.t, 4ull * n, cudaMemcpyDeviceToHost, c->stream));
+    if (out->normal) RKF_CUDA_TRY(cudaMemcpyAsync(out->normal, dev.normal, 12ull * n, cudaMemcpyDeviceToHost, c->stream));
+    if (out->slot) RKF_CUDA_TRY(cudaMemcpyAsync(out->slot, dev.slot, 4ull * n, cudaMemcpyDeviceToHost, c->stream));
+    if (out->material) RKF_CUDA_TRY(cudaMemcpyAsync(out->material, dev.material, 2ull * n, cudaMemcpyDeviceToHost, c->stream));
+    if (out->flags) RKF_CUDA_TRY(cudaMemcpyAsync(out->flags, dev.flags, 2ull * n, cudaMemcpyDeviceToHost, c->stream));
+  }
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return RKF_OK;
+}
+
+rkf_status rkf_query_points(rkf_ctx* ctx, const float* points, uint32_t n, float* dist, float* grad,
+                            uint16_t* material, uint32_t mem) {
+  if (!ctx || (n && !points)) return fail(RKF_INVALID_ARG, "rkf_query_points: null argument");
+  if (mem > RKF_MEM_DEVICE) return fail(RKF_INVALID_ARG, "rkf_query_points: bad mem kind");
+  if (n == 0) return RKF_OK;
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  if (mem == RKF_MEM_DEVICE) {
+    rkf_status st = launch_query(c, points, n, dist, grad, material, c->stream);
+    if (st != RKF_OK) return st;
+    RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return RKF_OK;
+  }
+  const size_t b_in = align256(12ull * n), b_d = align256(4ull * n), b_g = align256(12ull * n),
+               b_m = align256(2ull * n);
+  rkf_status st = c->stage_bytes(b_in + b_d + b_g + b_m);
+  if (st != RKF_OK) return st;
+  char* b = c->stage.as<char>();
+  float* dp = reinterpret_cast<float*>(b);
+  float* dd = reinterpret_cast<float*>(b + b_in);
+  float* dg = reinterpret_cast<float*>(b + b_in + b_d);
+  uint16_t* dm = reinterpret_cast<uint16_t*>(b + b_in + b_d + b_g);
+  RKF_CUDA_TRY(cudaMemcpyAsync(dp, points, 12ull * n, cudaMemcpyHostToDevice, c->stream));
+  st = launch_query(c, dp, n, dist ? dd : nullptr, grad ? dg : nullptr, material ? dm : nullptr, c->stream);
+  if (st != RKF_OK) return st;
+  if (dist) RKF_CUDA_TRY(cudaMemcpyAsync(dist, dd, 4ull * n, cudaMemcpyDeviceToHost, c->stream));
+  if (grad) RKF_CUDA_TRY(cudaMemcpyAsync(grad, dg, 12ull * n, cudaMemcpyDeviceToHost, c->stream));
+  if (material) RKF_CUDA_TRY(cudaMemcpyAsync(material, dm, 2ull * n, cudaMemcpyDeviceToHost, c->stream));
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return RKF_OK;
+}
+
+rkf_status rkf_march_batch(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views,
+                           const rkf_ray_batch* batches, uint32_t n_batches,
+                           const rkf_march_params* p, const rkf_batch_tuning* tuning) {
+  if (!ctx || !p || (n_views && !views) || (n_batches && !batches))
+    return fail(RKF_INVALID_ARG, "rkf_march_batch: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  const rkf_batch_tuning tu = tuning ? *tuning : c->tuning;
+  if (tu.tile_w == 0 || tu.tile_h == 0 || tu.tile_w * tu.tile_h > 4096)
+    return fail(RKF_INVALID_ARG, "rkf_march_batch: bad tile shape");
+  std::vector<Segment> segs;
+  segs.reserve(n_views + n_batches);
+  uint64_t first = 0;
+  for (uint32_t i = 0; i < n_views; ++i) {
+    const rkf_view& v = views[i];
+    if (v.width == 0 || v.height == 0) continue;
+    if (v.out.mem != RKF_MEM_DEVICE || !v.out.t || !v.out.normal || !v.out.slot || !v.out.material || !v.out.flags)
+      return fail(RKF_INVALID_ARG, "rkf_march_batch: views need device G-buffers");
+    Segment sg = view_segment(&v.camera, v.width, v.height, tu.tile_w, tu.tile_h, v.out);
+    sg.first = first;
+    first += sg.n_ids;
+    segs.push_back(sg);
+  }
+  for (uint32_t i = 0; i < n_batches; ++i) {
+    const rkf_ray_batch& r = batches[i];
+    if (r.n == 0) continue;
+    if (r.out.mem != RKF_MEM_DEVICE || !r.out.t || !r.origins || !r.dirs || !r.tmax || r.mode > RKF_TRACE_SHADOW)
+      return fail(RKF_INVALID_ARG, "rkf_march_batch: bad ray batch");
+    Segment sg = ray_segment(r.origins, r.dirs, r.tmax, r.n, r.mode, r.out);
+    sg.first = first;
+    first += sg.n_ids;
+    segs.push_back(sg);
+  }
+  if (segs.empty()) return RKF_OK;
+  rkf_status st = launch_persistent(c, segs, first, p, tu, c->stream, &c->seg_buf,
+                                    c->counters.as<unsigned long long>());
+  if (st != RKF_OK) return st;
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return RKF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,482 @@
+// ctx.cu — context lifetime, scene import (the reference upload path), the
+// two-level brick index, and small query entry points.
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "ctx.h"
+
+namespace rkf {
+
+namespace {
+thread_local std::string t_last_error;
+cudaError_t default_alloc(void** p, size_t bytes) { return cudaMalloc(p, bytes); }
+}  // namespace
+
+alloc_hook_fn g_alloc_hook = default_alloc;
+
+void set_error(const std::string& msg) { t_last_error = msg; }
+rkf_status fail(rkf_status st, const std::string& msg) {
+  t_last_error = msg;
+  return st;
+}
+
+DevBuf::~DevBuf() { release(); }
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+rkf_status DevBuf::alloc(size_t n) {
+  release();
+  if (n == 0) return RKF_OK;
+  cudaError_t e = g_alloc_hook(&p, n);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? RKF_OOM : RKF_CUDA_ERROR,
+                std::string("device allocation of ") + std::to_string(n) +
+                    " bytes failed: " + cudaGetErrorString(e));
+  }
+  bytes = n;
+  return RKF_OK;
+}
+
+ObjDev make_objdev(const rkf_gpu_object& o, uint32_t top_off, uint32_t has_flat) {
+  ObjDev d;
+  std::memset(&d, 0, sizeof(d));
+  std::memcpy(d.m, o.inverse_world, sizeof(d.m));
+  // Every constant below is the value the shader recomputes per sample, in the
+  // same float operations (ray_march.wgsl:354-363, :621, :630).
+  d.vs = o.voxel_size;
+  d.be = d.vs * 8.0f;
+  d.be2 = d.be * 2.0f;
+  for (int a = 0; a < 3; ++a) {
+    d.gs[a] = static_cast<float>(o.brick_map_dims[a]) * d.be;
+    d.half_gs[a] = d.gs[a] * 0.5f;
+  }
+  d.lo = d.vs * 0.01f;
+  for (int a = 0; a < 3; ++a) d.hi[a] = d.gs[a] - d.lo;
+  d.vs16 = d.vs * 16.0f;
+  for (int a = 0; a < 3; ++a) {
+    d.gmin[a] = o.geometry_aabb_min[a];
+    d.gmax[a] = o.geometry_aabb_max[a];
+  }
+  d.has_geom = o.geometry_aabb_max[0] > o.geometry_aabb_min[0] ? 1u : 0u;
+  const float sx = o.accumulated_scale[0], sy = o.accumulated_scale[1],
+              sz = o.accumulated_scale[2];
+  const float myz = sz < sy ? sz : sy;
+  d.min_scale = myz < sx ? myz : sx;
+  for (int a = 0; a < 4; ++a) d.params[a] = o.sdf_params[a];
+  for (int a = 0; a < 3; ++a) {
+    d.tv[a] = static_cast<int>(o.brick_map_dims[a]) * 8;
+    d.bdims[a] = o.brick_map_dims[a];
+    d.tdim[a] = (o.brick_map_dims[a] + 7) / 8;
+  }
+  d.top_off = top_off;
+  d.map_off = o.brick_map_offset;
+  d.has_flat = has_flat;
+  d.sdf_type = o.sdf_type;
+  d.prim_type = o.primitive_type;
+  d.object_id = o.object_id;
+  d.material_id = o.material_id;
+  return d;
+}
+
+SceneDev Ctx::scene_dev() const {
+  SceneDev s;
+  s.dist_f16 = dist_f16.as<uint16_t>();
+  s.dist_f32 = dist_f32.as<float>();
+  s.dist_u8 = dist_u8.as<int8_t>();
+  s.brick_step = brick_step.as<float>();
+  s.mat = mat.as<uint16_t>();
+  s.blend = blend.as<uint8_t>();
+  s.aos = aos.as<uint2>();
+  s.top = top.as<uint32_t>();
+  s.leaves = leaves.as<uint32_t>();
+  s.flat_maps = flat_maps.as<uint32_t>();
+  s.objs = objdev.as<ObjDev>();
+  s.n_objs = obj_count();
+  s.precision = cfg.precision;
+  return s;
+}
+
+rkf_status Ctx::upload_objects() {
+  if (objdev_host.empty()) return RKF_OK;
+  const size_t bytes = objdev_host.size() * sizeof(ObjDev);
+  if (objdev.bytes < bytes) {
+    rkf_status st = objdev.alloc(bytes);
+    if (st != RKF_OK) return st;
+  }
+  RKF_CUDA_TRY(cudaMemcpyAsync(objdev.p, objdev_host.data(), bytes, cudaMemcpyHostToDevice, stream));
+  RKF_CUDA_TRY(cudaStreamSynchronize(stream));
+  return RKF_OK;
+}
+
+rkf_status Ctx::ensure_leaf_capacity(uint32_t need) {
+  if (need <= leaf_cap) return RKF_OK;
+  uint32_t cap = leaf_cap ? leaf_cap : 64;
+  while (cap < need) cap *= 2;
+  DevBuf nb;
+  rkf_status st = nb.alloc(static_cast<size_t>(cap) * 512 * 4);
+  if (st != RKF_OK) return st;
+  if (n_leaves)
+    RKF_CUDA_TRY(cudaMemcpyAsync(nb.p, leaves.p, static_cast<size_t>(n_leaves) * 2048,
+                                 cudaMemcpyDeviceToDevice, stream));
+  RKF_CUDA_TRY(cudaStreamSynchronize(stream));
+  std::swap(leaves.p, nb.p);
+  std::swap(leaves.bytes, nb.bytes);
+  leaf_cap = cap;
+  return RKF_OK;
+}
+
+rkf_status Ctx::stage_bytes(size_t bytes) {
+  if (stage.bytes >= bytes) return RKF_OK;
+  return stage.alloc(bytes + bytes / 4);
+}
+
+namespace detail {
+
+// VoxelSample words -> SoA planes (+ optional AoS copy).  One thread per voxel.
+__global__ void k_import_words(const uint2* __restrict__ words, uint64_t nvox, uint64_t first_vox,
+                               uint16_t* dist_f16, float* dist_f32, uint16_t* mat, uint8_t* blend,
+                               uint2* aos) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= nvox) return;
+  const uint2 w = words[i];
+  const uint64_t v = first_vox + i;
+  const uint16_t d = static_cast<uint16_t>(w.x & 0xFFFFu);
+  if (dist_f16) dist_f16[v] = d;
+  if (dist_f32) dist_f32[v] = __half2float(__ushort_as_half(d));
+  mat[v] = static_cast<uint16_t>(((w.x >> 16) & 0x3Fu) | (((w.x >> 22) & 0x3Fu) << 6));
+  blend[v] = static_cast<uint8_t>(w.y >> 24);
+  if (aos) aos[v] = w;
+}
+
+__global__ void k_lookup(SceneDev s, uint32_t obj, const uint32_t* bxyz, uint32_t n, uint32_t* out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const ObjDev& o = s.objs[obj];
+  const uint32_t bx = bxyz[3 * i], by = bxyz[3 * i + 1], bz = bxyz[3 * i + 2];
+  if (bx >= o.bdims[0] || by >= o.bdims[1] || bz >= o.bdims[2]) {
+    out[i] = RKF_EMPTY_SLOT;
+    return;
+  }
+  out[i] = lookup2(s, o, bx, by, bz);
+}
+
+}  // namespace detail
+
+// Band-normalised signed u8 code of one brick: step = range/127 with range the
+// largest finite |d| in the brick; |code| = min(floor(|d|/step), 127) so the
+// decoded |d| never exceeds the stored one (sphere tracing never overshoots).
+__global__ void k_encode_u8(const float* __restrict__ src_f32, const uint16_t* __restrict__ src_f16,
+                            uint32_t first_slot, uint32_t n_bricks, int8_t* code, float* step) {
+  const uint32_t b = blockIdx.x;
+  if (b >= n_bricks) return;
+  const uint64_t base = (static_cast<uint64_t>(first_slot) + b) * 512;
+  __shared__ float red[256];
+  float m = 0.0f;
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) {
+    const float d = src_f32 ? src_f32[base + i] : __half2float(__ushort_as_half(src_f16[base + i]));
+    const float a = fabsf(d);
+    if (a <= 3.0e38f && a > m) m = a;
+  }
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = fmaxf(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  const float range = fmaxf(red[0], 1e-6f);
+  const float st = __fdiv_rn(range, 127.0f);
+  if (threadIdx.x == 0) step[first_slot + b] = st;
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) {
+    const float d = src_f32 ? src_f32[base + i] : __half2float(__ushort_as_half(src_f16[base + i]));
+    const float q = floorf(__fdiv_rn(fabsf(d), st));
+    const int c = q >= 127.0f ? 127 : static_cast<int>(q);
+    code[base + i] = static_cast<int8_t>(d < 0.0f ? -c : c);
+  }
+}
+
+}  // namespace rkf
+
+using namespace rkf;
+
+extern "C" {
+
+const char* rkf_last_error(void) { return t_last_error.c_str(); }
+
+void rkf_march_params_default(rkf_march_params* p) {
+  if (!p) return;
+  p->scene.num_objects = 0;
+  p->scene.max_steps = 128;         // gpu_scene.rs:38
+  p->scene.max_distance = 100.0f;   // gpu_scene.rs:39
+  p->scene.hit_threshold = 0.001f;  // gpu_scene.rs:40
+  p->hard_max_steps = 1024;         // ray_march.wgsl:36
+  p->bisect_steps = 8;              // ray_march.wgsl:31
+  p->min_step = 0.0005f;            // ray_march.wgsl:30
+  p->near_surface_threshold = 0.02f;  // ray_march.wgsl:41
+}
+
+void rkf_config_default(rkf_config* cfg) {
+  if (!cfg) return;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->device = 0;
+  cfg->pool_capacity_bricks = 1u << 16;
+  cfg->precision = RKF_PRECISION_F16;
+  cfg->keep_reference_pool = 1;
+  cfg->max_inflight = 64;
+}
+
+rkf_status rkf_create(const rkf_config* cfg, rkf_ctx** out) {
+  if (!cfg || !out) return fail(RKF_INVALID_ARG, "rkf_create: null argument");
+  if (cfg->precision > RKF_PRECISION_U8) return fail(RKF_INVALID_ARG, "rkf_create: bad precision");
+  if (cfg->pool_capacity_bricks == 0 || cfg->pool_capacity_bricks > (RKF_INTERIOR_SLOT - 1))
+    return fail(RKF_INVALID_ARG, "rkf_create: pool_capacity_bricks out of range");
+  int ndev = 0;
+  RKF_CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (cfg->device < 0 || cfg->device >= ndev)
+    return fail(RKF_INVALID_ARG, "rkf_create: no CUDA device " + std::to_string(cfg->device));
+  RKF_CUDA_TRY(cudaSetDevice(cfg->device));
+  auto c = std::make_unique<Ctx>();
+  c->device = cfg->device;
+  c->cfg = *cfg;
+  if (c->cfg.max_inflight == 0) c->cfg.max_inflight = 64;
+  RKF_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  RKF_CUDA_TRY(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device));
+  const size_t cap = cfg->pool_capacity_bricks;
+  c->capacity = cfg->pool_capacity_bricks;
+  const size_t nv = cap * 512;
+  rkf_status st = RKF_OK;
+  switch (cfg->precision) {
+    case RKF_PRECISION_F32:
+      st = c->dist_f32.alloc(nv * 4);
+      break;
+    case RKF_PRECISION_U8:
+      if ((st = c->dist_u8.alloc(nv)) == RKF_OK) st = c->brick_step.alloc(cap * 4);
+      // the f16 plane stays the import staging source for the u8 encoder
+      if (st == RKF_OK) st = c->dist_f16.alloc(nv * 2);
+      break;
+    default:
+      st = c->dist_f16.alloc(nv * 2);
+  }
+  if (st == RKF_OK) st = c->mat.alloc(nv * 2);
+  if (st == RKF_OK) st = c->blend.alloc(nv);
+  if (st == RKF_OK && cfg->keep_reference_pool) st = c->aos.alloc(nv * 8);
+  if (st == RKF_OK) st = c->counters.alloc(4096);
+  if (st != RKF_OK) {
+    cudaStreamDestroy(c->stream);
+    return st;
+  }
+  c->free_slots.resize(cap);
+  for (size_t i = 0; i < cap; ++i) c->free_slots[i] = static_cast<uint32_t>(cap - 1 - i);
+  c->tuning = rkf_batch_tuning{8, 4, 0, 16, 0, 256};
+  *out = reinterpret_cast<rkf_ctx*>(c.release());
+  return RKF_OK;
+}
+
+rkf_status rkf_serve_stop(rkf_ctx* ctx);
+
+rkf_status rkf_destroy(rkf_ctx* ctx) {
+  if (!ctx) return fail(RKF_INVALID_ARG, "rkf_destroy: null ctx");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  cudaSetDevice(c->device);
+  if (c->serve) rkf_serve_stop(ctx);
+  cudaStreamSynchronize(c->stream);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return RKF_OK;
+}
+
+rkf_status rkf_pool_import_voxelsample(rkf_ctx* ctx, const uint32_t* words, uint32_t first_slot,
+                                       uint32_t n_bricks) {
+  if (!ctx || (!words && n_bricks)) return fail(RKF_INVALID_ARG, "rkf_pool_import_voxelsample: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (static_cast<uint64_t>(first_slot) + n_bricks > c->capacity)
+    return fail(RKF_INVALID_ARG, "rkf_pool_import_voxelsample: slots beyond pool capacity");
+  if (n_bricks == 0) return RKF_OK;
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  const uint64_t nvox = static_cast<uint64_t>(n_bricks) * 512;
+  rkf_status st = c->stage_bytes(nvox * 8);
+  if (st != RKF_OK) return st;
+  RKF_CUDA_TRY(cudaMemcpyAsync(c->stage.p, words, nvox * 8, cudaMemcpyHostToDevice, c->stream));
+  const uint64_t first_vox = static_cast<uint64_t>(first_slot) * 512;
+  const unsigned blocks = static_cast<unsigned>((nvox + 255) / 256);
+  detail::k_import_words<<<blocks, 256, 0, c->stream>>>(c->stage.as<uint2>(), nvox, first_vox,
+                                                c->dist_f16.as<uint16_t>(), c->dist_f32.as<float>(),
+                                                c->mat.as<uint16_t>(), c->blend.as<uint8_t>(),
+                                                c->aos.as<uint2>());
+  RKF_CUDA_TRY(cudaGetLastError());
+  if (c->cfg.precision == RKF_PRECISION_U8) {
+    k_encode_u8<<<n_bricks, 256, 0, c->stream>>>(nullptr, c->dist_f16.as<uint16_t>(), first_slot,
+                                                 n_bricks, c->dist_u8.as<int8_t>(),
+                                                 c->brick_step.as<float>());
+    RKF_CUDA_TRY(cudaGetLastError());
+  }
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  // mark imported slots used (remove them from the free list)
+  std::vector<uint32_t> keep;
+  keep.reserve(c->free_slots.size());
+  for (uint32_t s : c->free_slots)
+    if (s < first_slot || s >= first_slot + n_bricks) keep.push_back(s);
+  c->used_slots += static_cast<uint32_t>(c->free_slots.size() - keep.size());
+  c->free_slots.swap(keep);
+  return RKF_OK;
+}
+
+rkf_status rkf_pool_export_voxelsample(rkf_ctx* ctx, uint32_t first_slot, uint32_t n_bricks,
+                                       uint32_t* words) {
+  if (!ctx || !words) return fail(RKF_INVALID_ARG, "rkf_pool_export_voxelsample: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (!c->aos.p) return fail(RKF_UNSUPPORTED, "rkf_pool_export_voxelsample: context keeps no reference pool");
+  if (static_cast<uint64_t>(first_slot) + n_bricks > c->capacity)
+    return fail(RKF_INVALID_ARG, "rkf_pool_export_voxelsample: range beyond capacity");
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  RKF_CUDA_TRY(cudaMemcpyAsync(words, c->aos.as<uint2>() + static_cast<size_t>(first_slot) * 512,
+                               static_cast<size_t>(n_bricks) * 4096, cudaMemcpyDeviceToHost, c->stream));
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return RKF_OK;
+}
+
+rkf_status rkf_brickmap_import(rkf_ctx* ctx, const uint32_t* packed, uint64_t n) {
+  if (!ctx || (!packed && n)) return fail(RKF_INVALID_ARG, "rkf_brickmap_import: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  c->flat_host.assign(packed, packed + n);
+  rkf_status st = c->flat_maps.alloc(n * 4);
+  if (st != RKF_OK) return st;
+  if (n) RKF_CUDA_TRY(cudaMemcpy(c->flat_maps.p, packed, n * 4, cudaMemcpyHostToDevice));
+  c->flat_len = n;
+  return RKF_OK;
+}
+
+rkf_status rkf_objects_import(rkf_ctx* ctx, const rkf_gpu_object* objects, uint32_t n) {
+  if (!ctx || (!objects && n)) return fail(RKF_INVALID_ARG, "rkf_objects_import: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  // validate and build the two-level index of every voxelized object
+  std::vector<uint32_t> top;
+  std::vector<uint32_t> leaf_host;
+  std::vector<ObjDev> od;
+  for (uint32_t i = 0; i < n; ++i) {
+    const rkf_gpu_object& o = objects[i];
+    if (o.sdf_type > RKF_SDF_VOXELIZED) return fail(RKF_INVALID_ARG, "rkf_objects_import: bad sdf_type");
+    uint32_t top_off = static_cast<uint32_t>(top.size());
+    if (o.sdf_type == RKF_SDF_VOXELIZED) {
+      const uint64_t dx = o.brick_map_dims[0], dy = o.brick_map_dims[1], dz = o.brick_map_dims[2];
+      if (dx == 0 || dy == 0 || dz == 0 || !(o.voxel_size > 0.0f))
+        return fail(RKF_INVALID_ARG, "rkf_objects_import: voxelized object with empty grid");
+      if (o.brick_map_offset + dx * dy * dz > c->flat_host.size())
+        return fail(RKF_INVALID_ARG, "rkf_objects_import: brick map extends past the imported buffer");
+      const uint32_t tx = static_cast<uint32_t>((dx + 7) / 8), ty = static_cast<uint32_t>((dy + 7) / 8),
+                     tz = static_cast<uint32_t>((dz + 7) / 8);
+      top.resize(top.size() + static_cast<size_t>(tx) * ty * tz, RKF_EMPTY_SLOT);
+      for (uint32_t kz = 0; kz < tz; ++kz)
+        for (uint32_t ky = 0; ky < ty; ++ky)
+          for (uint32_t kx = 0; kx < tx; ++kx) {
+            bool any = false, all_int = true;
+            for (uint32_t l = 0; l < 512; ++l) {
+              const uint64_t bx = kx * 8 + (l & 7), by = ky * 8 + ((l >> 3) & 7), bz = kz * 8 + (l >> 6);
+              uint32_t s = RKF_EMPTY_SLOT;
+              if (bx < dx && by < dy && bz < dz)
+                s = c->flat_host[o.brick_map_offset + bx + by * dx + bz * dx * dy];
+              if (s != RKF_EMPTY_SLOT) any = true;
+              if (s != RKF_INTERIOR_SLOT) all_int = false;
+              if (s < RKF_INTERIOR_SLOT && s >= c->capacity)
+                return fail(RKF_INVALID_ARG, "rkf_objects_import: brick map names a slot beyond the pool");
+            }
+            uint32_t entry = RKF_EMPTY_SLOT;
+            if (all_int) {
+              entry = RKF_INTERIOR_SLOT;
+            } else if (any) {
+              entry = c->n_leaves + static_cast<uint32_t>(leaf_host.size() / 512);
+              for (uint32_t l = 0; l < 512; ++l) {
+                const uint64_t bx = kx * 8 + (l & 7), by = ky * 8 + ((l >> 3) & 7), bz = kz * 8 + (l >> 6);
+                uint32_t s = RKF_EMPTY_SLOT;
+                if (bx < dx && by < dy && bz < dz)
+                  s = c->flat_host[o.brick_map_offset + bx + by * dx + bz * dx * dy];
+                leaf_host.push_back(s);
+              }
+            }
+            top[top_off + kx + ky * tx + kz * tx * ty] = entry;
+          }
+    }
+    od.push_back(make_objdev(o, top_off, o.sdf_type == RKF_SDF_VOXELIZED ? 1u : 0u));
+  }
+  // replace the index wholesale
+  c->n_leaves = 0;
+  const uint32_t nl = static_cast<uint32_t>(leaf_host.size() / 512);
+  rkf_status st = c->ensure_leaf_capacity(nl ? nl : 1);
+  if (st != RKF_OK) return st;
+  if (nl)
+    RKF_CUDA_TRY(cudaMemcpy(c->leaves.p, leaf_host.data(), leaf_host.size() * 4, cudaMemcpyHostToDevice));
+  c->n_leaves = nl;
+  st = c->top.alloc(std::max<size_t>(top.size(), 1) * 4);
+  if (st != RKF_OK) return st;
+  if (!top.empty()) RKF_CUDA_TRY(cudaMemcpy(c->top.p, top.data(), top.size() * 4, cudaMemcpyHostToDevice));
+  c->top_len = top.size();
+  c->objects.assign(objects, objects + n);
+  c->objdev_host = od;
+  st = c->upload_objects();
+  if (st != RKF_OK) return st;
+  c->epoch++;
+  return RKF_OK;
+}
+
+rkf_status rkf_object_get(rkf_ctx* ctx, uint32_t i, rkf_gpu_object* out) {
+  if (!ctx || !out) return fail(RKF_INVALID_ARG, "rkf_object_get: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (i >= c->obj_count()) return fail(RKF_INVALID_ARG, "rkf_object_get: index out of range");
+  *out = c->objects[i];
+  return RKF_OK;
+}
+
+rkf_status rkf_scene_info_get(rkf_ctx* ctx, rkf_scene_info* out) {
+  if (!ctx || !out) return fail(RKF_INVALID_ARG, "rkf_scene_info_get: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  out->num_objects = c->obj_count();
+  out->pool_bricks_used = c->used_slots;
+  out->pool_capacity = c->capacity;
+  out->leaf_blocks = c->n_leaves;
+  out->device_bytes = c->dist_f16.bytes + c->dist_f32.bytes + c->dist_u8.bytes + c->brick_step.bytes +
+                      c->mat.bytes + c->blend.bytes + c->aos.bytes + c->top.bytes + c->leaves.bytes +
+                      c->flat_maps.bytes + c->objdev.bytes;
+  out->epoch = c->epoch;
+  return RKF_OK;
+}
+
+rkf_status rkf_brick_lookup(rkf_ctx* ctx, uint32_t obj, const uint32_t* bxyz, uint32_t n,
+                            uint32_t* slots) {
+  if (!ctx || ((!bxyz || !slots) && n)) return fail(RKF_INVALID_ARG, "rkf_brick_lookup: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (obj >= c->obj_count() || c->objects[obj].sdf_type != RKF_SDF_VOXELIZED)
+    return fail(RKF_INVALID_ARG, "rkf_brick_lookup: not a voxelized object");
+  if (n == 0) return RKF_OK;
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  DevBuf buf;
+  rkf_status st = buf.alloc(static_cast<size_t>(n) * 16);
+  if (st != RKF_OK) return st;
+  uint32_t* din = buf.as<uint32_t>();
+  uint32_t* dout = din + 3 * static_cast<size_t>(n);
+  RKF_CUDA_TRY(cudaMemcpyAsync(din, bxyz, static_cast<size_t>(n) * 12, cudaMemcpyHostToDevice, c->stream));
+  detail::k_lookup<<<(n + 255) / 256, 256, 0, c->stream>>>(c->scene_dev(), obj, din, n, dout);
+  RKF_CUDA_TRY(cudaGetLastError());
+  RKF_CUDA_TRY(cudaMemcpyAsync(slots, dout, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost, c->stream));
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return RKF_OK;
+}
+
+void rkf_world_relative(const rkf_world_pos* pos, const rkf_world_pos* origin, double out_f64[3],
+                        float out_f32[3]) {
+  // WorldPosition::relative_to_f64 (world_position.rs:107-120), CHUNK_SIZE 8 m
+  for (int a = 0; a < 3; ++a) {
+    const double chunk_m = static_cast<double>(pos->chunk[a] - origin->chunk[a]) * 8.0;
+    const double local = static_cast<double>(pos->local[a] - origin->local[a]);
+    const double v = chunk_m + local;
+    if (out_f64) out_f64[a] = v;
+    if (out_f32) out_f32[a] = static_cast<float>(v);
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// ctx.h — host-side state of an rkf_ctx (one device, one resident scene).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/rkf_cuda.h"
+#include "device_common.cuh"
+
+namespace rkf {
+
+// Thread-local message for rkf_last_error().
+void set_error(const std::string& msg);
+rkf_status fail(rkf_status st, const std::string& msg);
+
+#define RKF_CUDA_TRY(expr)                                                        \
+  do {                                                                            \
+    cudaError_t e_ = (expr);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      return ::rkf::fail(e_ == cudaErrorMemoryAllocation ? RKF_OOM : RKF_CUDA_ERROR, \
+                         std::string(#expr) + ": " + cudaGetErrorString(e_));    \
+    }                                                                             \
+  } while (0)
+
+// A device allocation owned by the context.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf();
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  rkf_status alloc(size_t n);  // frees any previous allocation
+  void release();
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+// Allocation hook used by every context allocation (tests replace it to
+// simulate an out-of-memory device without touching the GPU).
+using alloc_hook_fn = cudaError_t (*)(void** p, size_t bytes);
+extern alloc_hook_fn g_alloc_hook;
+
+struct ServeState;  // serve.cu
+
+struct Ctx {
+  int device = 0;
+  rkf_config cfg{};
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+
+  // pool planes
+  uint32_t capacity = 0;
+  DevBuf dist_f16, dist_f32, dist_u8, brick_step, mat, blend, aos;
+  std::vector<uint32_t> free_slots;  // LIFO, low slots on top (brick_pool.rs:37-42)
+  uint32_t used_slots = 0;
+
+  // reference flat maps (kept for the plain march when imported)
+  DevBuf flat_maps;
+  uint64_t flat_len = 0;
+  std::vector<uint32_t> flat_host;  // host copy used to build the index
+
+  // two-level index
+  DevBuf top;
+  uint64_t top_len = 0;
+  DevBuf leaves;
+  uint32_t n_leaves = 0, leaf_cap = 0;
+
+  // objects
+  std::vector<rkf_gpu_object> objects;
+  std::vector<ObjDev> objdev_host;
+  DevBuf objdev;
+
+  uint64_t epoch = 0;
+
+  // scratch reused by march calls (host-pointer outputs staged here)
+  DevBuf stage;
+  DevBuf counters;   // work counters of the persistent kernels
+  DevBuf seg_buf;    // segment table of the persistent kernel
+  DevBuf l2_flush;
+
+  // batching
+  rkf_batch_tuning tuning{};
+  bool tuned = false;
+
+  ServeState* serve = nullptr;  // owned; created by rkf_serve_start
+
+  SceneDev scene_dev() const;
+  uint32_t obj_count() const { return static_cast<uint32_t>(objects.size()); }
+  rkf_status upload_objects();
+  rkf_status ensure_leaf_capacity(uint32_t need);
+  rkf_status stage_bytes(size_t bytes);
+};
+
+// Builds ObjDev (precomputed per-object constants) from a GpuObject.
+ObjDev make_objdev(const rkf_gpu_object& o, uint32_t top_off, uint32_t has_flat);
+
+// Marches (march_fast.cu / march_plain.cu)
+struct Segment;
+rkf_status launch_plain(Ctx* c, const rkf_camera* cam, const rkf_march_params* p, uint32_t w,
+                        uint32_t h, const rkf_gbuffer& dev_out, cudaStream_t st);
+
+}  // namespace rkf

@@ -1,0 +1,44 @@
+// march.h — work segments of the persistent march and its launchers.
+#pragma once
+
+#include <vector>
+
+#include "ctx.h"
+
+namespace rkf {
+
+constexpr uint32_t kMaxObjectsFast = 64;
+
+// One unit of batched work: a view (kind 0, primary rays over w x h pixels
+// walked in tile order) or a ray batch (kind 1).  Device pointers only.
+struct Segment {
+  uint64_t first;     // first global work id of the segment
+  uint64_t n_ids;     // work ids the segment spans
+  uint32_t kind, mode;
+  uint32_t w, h, tiles_x, _pad;
+  float pos[3], fwd[3], right[3], up[3], jitter[2];
+  float prev_vp[16];
+  const float* origins;
+  const float* dirs;
+  const float* tmax;
+  float* t;
+  float* normal;
+  uint32_t* slot;
+  uint16_t* material;
+  uint16_t* flags;
+  float* position;
+  uint32_t* packed;
+  float* motion;
+};
+
+Segment view_segment(const rkf_camera* cam, uint32_t w, uint32_t h, uint32_t tile_w,
+                     uint32_t tile_h, const rkf_gbuffer& out);
+Segment ray_segment(const float* o, const float* d, const float* tmax, uint32_t n, uint32_t mode,
+                    const rkf_hits& out);
+rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs, uint64_t total,
+                             const rkf_march_params* p, const rkf_batch_tuning& tu,
+                             cudaStream_t st, DevBuf* seg_buf, unsigned long long* counter);
+rkf_status launch_query(Ctx* c, const float* pts, uint32_t n, float* d, float* g, uint16_t* m,
+                        cudaStream_t st);
+
+}  // namespace rkf

@@ -1,0 +1,226 @@
+"""Host-side mirror of the reference's march interfaces over the C ABI.
+
+The reference drives the march through ``GpuScene`` uploads
+(``crates/rkf-render/src/gpu_scene.rs:141-234``), ``RayMarchPass::dispatch``
+(``crates/rkf-render/src/ray_march.rs:96-118``) and physics point queries
+through ``trait SdfQueryable`` (``crates/rkf-physics/src/sdf_collision.rs:38-44``).
+This module offers the same operations, same names and argument meaning, on
+top of ``librkf_cuda.so``.  Every call goes to the CUDA library; there is no
+CPU path.  Errors raise :class:`RkfError` carrying the library status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi as abi
+from ._abi import RkfError, check  # noqa: F401  (re-exported)
+
+PRECISIONS = {"f16": abi.RKF_PRECISION_F16, "f32": abi.RKF_PRECISION_F32, "u8": abi.RKF_PRECISION_U8}
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def gbuffer_host(n: int, reference_planes: bool = False) -> dict:
+    out = {"t": np.zeros(n, np.float32), "normal": np.zeros(3 * n, np.float32),
+           "slot": np.zeros(n, np.uint32), "material": np.zeros(n, np.uint16),
+           "flags": np.zeros(n, np.uint16)}
+    if reference_planes:
+        out["position"] = np.zeros(4 * n, np.float32)
+        out["packed_material"] = np.zeros(n, np.uint32)
+        out["motion"] = np.zeros(4 * n, np.float32)
+    return out
+
+
+def _gb_struct(out: dict, mem: int = abi.RKF_MEM_HOST) -> abi.rkf_gbuffer:
+    g = abi.rkf_gbuffer()
+    for k in ("t", "normal", "slot", "material", "flags", "position", "packed_material", "motion"):
+        v = out.get(k)
+        setattr(g, k, None if v is None else (v if isinstance(v, int) else v.ctypes.data))
+    g.mem = mem
+    return g
+
+
+class Context:
+    """One device-resident scene (brick pool, brick index, object table)."""
+
+    def __init__(self, device: int = 0, pool_capacity: int = 1 << 16, precision: str = "f16",
+                 keep_reference_pool: bool = True, max_inflight: int = 64,
+                 mem_budget_bytes: int = 0):
+        self.lib = abi.load_library()
+        cfg = abi.rkf_config()
+        self.lib.rkf_config_default(C.byref(cfg))
+        cfg.device = device
+        cfg.pool_capacity_bricks = pool_capacity
+        cfg.precision = PRECISIONS[precision]
+        cfg.keep_reference_pool = int(keep_reference_pool)
+        cfg.max_inflight = max_inflight
+        cfg.mem_budget_bytes = mem_budget_bytes
+        h = C.c_void_p()
+        check(self.lib.rkf_create(C.byref(cfg), C.byref(h)), "rkf_create")
+        self.h = h
+        self.precision = precision
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if self.h:
+            check(self.lib.rkf_destroy(self.h), "rkf_destroy")
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- import (GpuScene::set_brick_pool / upload_brick_maps / upload_objects)
+    def set_brick_pool(self, words: np.ndarray, first_slot: int = 0):
+        words = np.ascontiguousarray(words, np.uint32)
+        assert words.size % 1024 == 0
+        check(self.lib.rkf_pool_import_voxelsample(self.h, _p(words), first_slot, words.size // 1024),
+              "rkf_pool_import_voxelsample")
+
+    def upload_brick_maps(self, packed: np.ndarray):
+        packed = np.ascontiguousarray(packed, np.uint32)
+        check(self.lib.rkf_brickmap_import(self.h, _p(packed), packed.size), "rkf_brickmap_import")
+
+    def upload_objects(self, objects):
+        arr = (abi.rkf_gpu_object * len(objects))(*objects)
+        check(self.lib.rkf_objects_import(self.h, arr, len(objects)), "rkf_objects_import")
+
+    def voxelize(self, prims: np.ndarray, vp: abi.rkf_voxelize_params) -> int:
+        prims = np.ascontiguousarray(prims)
+        idx = C.c_uint32()
+        check(self.lib.rkf_voxelize_prims(self.h, _p(prims), len(prims), C.byref(vp), C.byref(idx)),
+              "rkf_voxelize_prims")
+        return idx.value
+
+    def info(self) -> dict:
+        i = abi.rkf_scene_info()
+        check(self.lib.rkf_scene_info_get(self.h, C.byref(i)), "rkf_scene_info_get")
+        return {k: getattr(i, k) for k, _ in abi.rkf_scene_info._fields_}
+
+    def object(self, i: int) -> abi.rkf_gpu_object:
+        o = abi.rkf_gpu_object()
+        check(self.lib.rkf_object_get(self.h, i, C.byref(o)), "rkf_object_get")
+        return o
+
+    def export_pool(self, first_slot: int, n_bricks: int) -> np.ndarray:
+        w = np.zeros(n_bricks * 1024, np.uint32)
+        check(self.lib.rkf_pool_export_voxelsample(self.h, first_slot, n_bricks, _p(w)),
+              "rkf_pool_export_voxelsample")
+        return w
+
+    def brick_lookup(self, obj: int, bxyz: np.ndarray) -> np.ndarray:
+        bxyz = np.ascontiguousarray(bxyz, np.uint32)
+        n = bxyz.size // 3
+        out = np.zeros(n, np.uint32)
+        check(self.lib.rkf_brick_lookup(self.h, obj, _p(bxyz), n, _p(out)), "rkf_brick_lookup")
+        return out
+
+    # -- march (RayMarchPass::dispatch) ------------------------------------
+    def march(self, cam, params, width: int, height: int, reference_planes: bool = False,
+              out: dict | None = None, plain: bool = False) -> dict:
+        out = out if out is not None else gbuffer_host(width * height, reference_planes)
+        g = _gb_struct(out)
+        fn = self.lib.rkf_march_plain if plain else self.lib.rkf_march
+        check(fn(self.h, C.byref(cam), C.byref(params), width, height, C.byref(g)),
+              "rkf_march_plain" if plain else "rkf_march")
+        return out
+
+    def march_device(self, cam, params, width: int, height: int, dev_ptrs: dict, plain: bool = False):
+        g = _gb_struct(dev_ptrs, abi.RKF_MEM_DEVICE)
+        fn = self.lib.rkf_march_plain if plain else self.lib.rkf_march
+        check(fn(self.h, C.byref(cam), C.byref(params), width, height, C.byref(g)), "march")
+
+    # -- generic ray casts -------------------------------------------------
+    def trace(self, origins, dirs, tmax, mode: int, params, closest_planes: bool = True) -> dict:
+        origins = np.ascontiguousarray(origins, np.float32).ravel()
+        dirs = np.ascontiguousarray(dirs, np.float32).ravel()
+        tmax = np.ascontiguousarray(tmax, np.float32).ravel()
+        n = tmax.size
+        out = {"t": np.zeros(n, np.float32), "flags": np.zeros(n, np.uint16)}
+        if mode == abi.RKF_TRACE_CLOSEST and closest_planes:
+            out.update(normal=np.zeros(3 * n, np.float32), slot=np.zeros(n, np.uint32),
+                       material=np.zeros(n, np.uint16))
+        h = abi.rkf_hits()
+        h.t = _p(out["t"])
+        h.normal = _p(out.get("normal"))
+        h.slot = _p(out.get("slot"))
+        h.material = _p(out.get("material"))
+        h.flags = _p(out["flags"])
+        h.mem = abi.RKF_MEM_HOST
+        check(self.lib.rkf_trace_rays(self.h, _p(origins), _p(dirs), _p(tmax), n, mode,
+                                      C.byref(params), abi.RKF_MEM_HOST, C.byref(h)),
+              "rkf_trace_rays")
+        return out
+
+    # -- point queries (SdfQueryable) --------------------------------------
+    def query_points(self, points) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        pts = np.ascontiguousarray(points, np.float32).ravel()
+        n = pts.size // 3
+        d = np.zeros(n, np.float32)
+        g = np.zeros(3 * n, np.float32)
+        m = np.zeros(n, np.uint16)
+        check(self.lib.rkf_query_points(self.h, _p(pts), n, _p(d), _p(g), _p(m), abi.RKF_MEM_HOST),
+              "rkf_query_points")
+        return d, g, m
+
+    # -- edits ---------------------------------------------------------------
+    def edit(self, op: abi.rkf_edit_op) -> int:
+        ep = C.c_uint64()
+        check(self.lib.rkf_edit_csg(self.h, C.byref(op), C.byref(ep)), "rkf_edit_csg")
+        return ep.value
+
+
+class GpuScene:
+    """``GpuScene`` upload surface (gpu_scene.rs:141-234) on a :class:`Context`."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def set_brick_pool(self, words):
+        self.ctx.set_brick_pool(words)
+
+    def upload_brick_maps(self, packed):
+        self.ctx.upload_brick_maps(packed)
+
+    def upload_objects(self, objects):
+        self.ctx.upload_objects(objects)
+
+
+class RayMarchPass:
+    """``RayMarchPass`` (ray_march.rs:29-119): dispatch marches one view into
+    a G-buffer (SoA numpy planes)."""
+
+    DEFAULT_INTERNAL = (960, 540)  # ray_march.rs:24-26
+
+    def __init__(self, scene: GpuScene, width: int = 960, height: int = 540):
+        self.scene = scene
+        self.width, self.height = width, height
+
+    def dispatch(self, camera, params, reference_planes: bool = False) -> dict:
+        return self.scene.ctx.march(camera, params, self.width, self.height, reference_planes)
+
+
+class BrickPoolSdf:
+    """``SdfQueryable`` backed by the device brick pool: ``evaluate`` and
+    ``gradient`` of sdf_collision.rs:38-44, batched."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def evaluate(self, pos) -> np.ndarray:
+        return self.ctx.query_points(pos)[0]
+
+    def gradient(self, pos) -> np.ndarray:
+        return self.ctx.query_points(pos)[1].reshape(-1, 3)
