@@ -200,6 +200,14 @@ RKF_API rkf_status rkf_scene_info_get(rkf_ctx* ctx, rkf_scene_info* out);
  * (inverse of rkf_pool_import_voxelsample; used to cross-check). */
 RKF_API rkf_status rkf_pool_export_voxelsample(rkf_ctx* ctx, uint32_t first_slot,
                                        uint32_t n_bricks, uint32_t* words);
+/* Copy the device brick index out: the top grids (8^3-brick blocks: EMPTY,
+ * INTERIOR or a leaf number), the 512-entry leaves, and per object
+ * {top offset, top dims x, y, z}.  No reference counterpart (the reference
+ * keeps only flat maps); used to cross-check the device index.  Pass NULL
+ * arrays to query the sizes. */
+RKF_API rkf_status rkf_index_export(rkf_ctx* ctx, uint32_t* top, uint64_t* top_n,
+                                    uint32_t* leaves, uint64_t* leaf_entries,
+                                    uint32_t* obj_top_info, uint32_t* n_objects);
 /* Look up the slot (or sentinel) of brick (bx,by,bz) of object obj. */
 RKF_API rkf_status rkf_brick_lookup(rkf_ctx* ctx, uint32_t obj, const uint32_t* bxyz,
                             uint32_t n, uint32_t* slots);
@@ -286,6 +294,19 @@ RKF_API rkf_status rkf_march(rkf_ctx* ctx, const rkf_camera* cam, const rkf_marc
  * against. */
 RKF_API rkf_status rkf_march_plain(rkf_ctx* ctx, const rkf_camera* cam, const rkf_march_params* p,
                            uint32_t width, uint32_t height, rkf_gbuffer* out);
+
+/* Enqueue a march on a caller stream without waiting for it: the analogue
+ * of recording RayMarchPass::dispatch into a wgpu command encoder
+ * (ray_march.rs:96).  Device-pointer G-buffers only.  `stream` is a
+ * cudaStream_t of the context's device (NULL = the context stream).  Calls
+ * on one context share its launch scratch: issue them on one stream, or
+ * synchronise between streams. */
+RKF_API rkf_status rkf_march_async(rkf_ctx* ctx, const rkf_camera* cam, const rkf_march_params* p,
+                                   uint32_t width, uint32_t height, const rkf_gbuffer* out,
+                                   void* stream);
+RKF_API rkf_status rkf_march_plain_async(rkf_ctx* ctx, const rkf_camera* cam,
+                                         const rkf_march_params* p, uint32_t width,
+                                         uint32_t height, const rkf_gbuffer* out, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Generic ray casts (secondary rays; shade_common_shading.wgsl:9-47)        */

@@ -165,7 +165,8 @@ class Scene:
 def march(scene: Scene, cam, params, w: int, h: int, fp64: bool = False, threads: int | None = None,
           rows: tuple[int, int] | None = None, with_reference_planes: bool = False,
           with_margin: bool = False, with_root: bool = False, count_sectors: bool = False):
-    n = w * h
+    r0, r1 = rows if rows else (0, 0)
+    n = w * ((r1 - r0) if r1 > r0 else h)
     out = {
         "t": np.zeros(n, np.float32), "normal": np.zeros(3 * n, np.float32),
         "slot": np.zeros(n, np.uint32), "material": np.zeros(n, np.uint16),
@@ -183,7 +184,6 @@ def march(scene: Scene, cam, params, w: int, h: int, fp64: bool = False, threads
     if with_root and fp64:
         out["t_root"] = np.full(n, np.nan)
     st = orc_stats()
-    r0, r1 = rows if rows else (0, 0)
     lib().orc_march(C.byref(scene.s), C.byref(cam), C.byref(params), w, h, int(fp64),
                     threads or nthreads(), r0, r1, ptr(out["t"]), ptr(out["normal"]),
                     ptr(out["slot"]), ptr(out["material"]), ptr(out["flags"]),

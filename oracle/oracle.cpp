@@ -866,7 +866,7 @@ void march_view(const orc_scene* s, const rkf_camera* cam, const rkf_march_param
     Marcher<R> mc{s, &tr, out.margin ? &marg : nullptr};
     const uint32_t px = static_cast<uint32_t>(li % w);
     const uint32_t py = row0 + static_cast<uint32_t>(li / w);
-    const uint64_t i = static_cast<uint64_t>(py) * w + px;
+    const uint64_t i = li;  // outputs hold rows [row0, row1) only
     // ray generation (ray_march.wgsl:1046-1053)
     const R u = ((R(static_cast<float>(px)) + R(0.5)) + R(cam->jitter[0])) / R(static_cast<float>(w));
     const R v = ((R(static_cast<float>(py)) + R(0.5)) + R(cam->jitter[1])) / R(static_cast<float>(h));

@@ -102,7 +102,8 @@ typedef struct orc_stats {
  * rkf_gbuffer (host arrays; optional planes may be NULL).  margin (optional,
  * per ray) receives the smallest distance of any FP decision to its
  * threshold (for grazing flags); t_root (optional, fp64 only) the refined
- * trilinear surface crossing.  Rows [row0,row1) only when row1 > row0. */
+ * trilinear surface crossing.  When row1 > row0 only rows [row0,row1) are
+ * marched and the output arrays hold just those rows. */
 void orc_march(const orc_scene* s, const rkf_camera* cam, const rkf_march_params* p,
                uint32_t w, uint32_t h, int fp64, int threads, uint32_t row0, uint32_t row1,
                float* t, float* normal, uint32_t* slot, uint16_t* material, uint16_t* flags,

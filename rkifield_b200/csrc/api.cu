@@ -132,6 +132,36 @@ rkf_status rkf_march_plain(rkf_ctx* ctx, const rkf_camera* cam, const rkf_march_
   });
 }
 
+rkf_status rkf_march_async(rkf_ctx* ctx, const rkf_camera* cam, const rkf_march_params* p,
+                           uint32_t width, uint32_t height, const rkf_gbuffer* out, void* stream) {
+  rkf_status st = check_common(ctx, cam, p, "rkf_march_async");
+  if (st != RKF_OK) return st;
+  if ((st = check_gbuffer(out, "rkf_march_async")) != RKF_OK) return st;
+  if (out->mem != RKF_MEM_DEVICE) return fail(RKF_INVALID_ARG, "rkf_march_async: device G-buffer required");
+  if (width == 0 || height == 0 || static_cast<uint64_t>(width) * height > (1ull << 31))
+    return fail(RKF_INVALID_ARG, "rkf_march_async: bad resolution");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  const rkf_batch_tuning& tu = c->tuning;
+  std::vector<Segment> segs{view_segment(cam, width, height, tu.tile_w, tu.tile_h, *out)};
+  segs[0].first = 0;
+  return launch_persistent(c, segs, segs[0].n_ids, p, tu, s, &c->seg_buf, c->counters.as<unsigned long long>());
+}
+
+rkf_status rkf_march_plain_async(rkf_ctx* ctx, const rkf_camera* cam, const rkf_march_params* p,
+                                 uint32_t width, uint32_t height, const rkf_gbuffer* out, void* stream) {
+  rkf_status st = check_common(ctx, cam, p, "rkf_march_plain_async");
+  if (st != RKF_OK) return st;
+  if ((st = check_gbuffer(out, "rkf_march_plain_async")) != RKF_OK) return st;
+  if (out->mem != RKF_MEM_DEVICE) return fail(RKF_INVALID_ARG, "rkf_march_plain_async: device G-buffer required");
+  if (width == 0 || height == 0 || static_cast<uint64_t>(width) * height > (1ull << 31))
+    return fail(RKF_INVALID_ARG, "rkf_march_plain_async: bad resolution");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  return launch_plain(c, cam, p, width, height, *out, stream ? static_cast<cudaStream_t>(stream) : c->stream);
+}
+
 rkf_status rkf_trace_rays(rkf_ctx* ctx, const float* origins, const float* dirs, const float* tmax,
                           uint32_t n, uint32_t mode, const rkf_march_params* p, uint32_t in_mem,
                           rkf_hits* out) {

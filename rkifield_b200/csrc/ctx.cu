@@ -446,6 +446,27 @@ rkf_status rkf_scene_info_get(rkf_ctx* ctx, rkf_scene_info* out) {
   return RKF_OK;
 }
 
+rkf_status rkf_index_export(rkf_ctx* ctx, uint32_t* top, uint64_t* top_n, uint32_t* leaves,
+                            uint64_t* leaf_entries, uint32_t* obj_top_info, uint32_t* n_objects) {
+  if (!ctx || !top_n || !leaf_entries || !n_objects)
+    return fail(RKF_INVALID_ARG, "rkf_index_export: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  *top_n = c->top_len;
+  *leaf_entries = static_cast<uint64_t>(c->n_leaves) * 512;
+  *n_objects = c->obj_count();
+  if (top && c->top_len)
+    RKF_CUDA_TRY(cudaMemcpy(top, c->top.p, c->top_len * 4, cudaMemcpyDeviceToHost));
+  if (leaves && c->n_leaves)
+    RKF_CUDA_TRY(cudaMemcpy(leaves, c->leaves.p, static_cast<size_t>(c->n_leaves) * 2048, cudaMemcpyDeviceToHost));
+  if (obj_top_info)
+    for (uint32_t i = 0; i < c->obj_count(); ++i) {
+      obj_top_info[4 * i] = c->objdev_host[i].top_off;
+      for (int a = 0; a < 3; ++a) obj_top_info[4 * i + 1 + a] = c->objdev_host[i].tdim[a];
+    }
+  return RKF_OK;
+}
+
 rkf_status rkf_brick_lookup(rkf_ctx* ctx, uint32_t obj, const uint32_t* bxyz, uint32_t n,
                             uint32_t* slots) {
   if (!ctx || ((!bxyz || !slots) && n)) return fail(RKF_INVALID_ARG, "rkf_brick_lookup: null argument");

@@ -120,6 +120,26 @@ class Context:
               "rkf_pool_export_voxelsample")
         return w
 
+    def export_index(self) -> dict:
+        """Device brick index (top grids, leaves, per-object top info)."""
+        tn, ln, no = C.c_uint64(), C.c_uint64(), C.c_uint32()
+        check(self.lib.rkf_index_export(self.h, None, C.byref(tn), None, C.byref(ln), None, C.byref(no)),
+              "rkf_index_export")
+        top = np.zeros(max(1, tn.value), np.uint32)
+        leaves = np.zeros(max(1, ln.value), np.uint32)
+        info = np.zeros(4 * max(1, no.value), np.uint32)
+        check(self.lib.rkf_index_export(self.h, _p(top), C.byref(tn), _p(leaves), C.byref(ln), _p(info),
+                                        C.byref(no)), "rkf_index_export")
+        return {"top": top, "leaves": leaves, "obj_top_info": info}
+
+    def march_async(self, cam, params, width: int, height: int, dev_ptrs: dict, stream_ptr: int,
+                    plain: bool = False):
+        """Enqueue a march on a caller stream into device planes (no sync)."""
+        g = _gb_struct(dev_ptrs, abi.RKF_MEM_DEVICE)
+        fn = self.lib.rkf_march_plain_async if plain else self.lib.rkf_march_async
+        check(fn(self.h, C.byref(cam), C.byref(params), width, height, C.byref(g), stream_ptr),
+              "rkf_march_async")
+
     def brick_lookup(self, obj: int, bxyz: np.ndarray) -> np.ndarray:
         bxyz = np.ascontiguousarray(bxyz, np.uint32)
         n = bxyz.size // 3
