@@ -1,5 +1,6 @@
 // ctx.cu — context lifetime, scene import (the reference upload path), the
 // two-level brick index, and small query entry points.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -76,6 +77,15 @@ ObjDev make_objdev(const rkf_gpu_object& o, uint32_t top_off, uint32_t has_flat)
   d.top_off = top_off;
   d.map_off = o.brick_map_offset;
   d.has_flat = has_flat;
+  d.vs2 = d.vs * 2.0f;
+  d.rcp_vs = d.vs > 0.0f ? static_cast<float>(1.0 / static_cast<double>(d.vs)) : 0.0f;
+  d.div_ok = 0;  // set after the device check (verify_exact_div)
+  const float* m = o.inverse_world;
+  d.translate_only = (m[0] == 1.0f && m[1] == 0.0f && m[2] == 0.0f && m[3] == 0.0f && m[4] == 0.0f &&
+                      m[5] == 1.0f && m[6] == 0.0f && m[7] == 0.0f && m[8] == 0.0f && m[9] == 0.0f &&
+                      m[10] == 1.0f && m[11] == 0.0f && m[15] == 1.0f)
+                         ? 1u
+                         : 0u;
   d.sdf_type = o.sdf_type;
   d.prim_type = o.primitive_type;
   d.object_id = o.object_id;
@@ -101,8 +111,60 @@ SceneDev Ctx::scene_dev() const {
   return s;
 }
 
+namespace detail {
+// Counts the floats x in [b0, b0+n) (as bit patterns) whose exact_div_vs
+// differs from the IEEE quotient x/vs.
+__global__ void k_verify_div(float vs, float rcp, uint32_t b0, uint32_t n, unsigned int* bad) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  unsigned int local = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const float x = __uint_as_float(b0 + i);
+    if (__float_as_uint(exact_div_vs(x, vs, rcp)) != __float_as_uint(__fdiv_rn(x, vs))) ++local;
+  }
+  if (local) atomicAdd(bad, local);
+}
+}  // namespace detail
+
+// Decide ObjDev::div_ok for every voxelized object: exhaustively compare the
+// fast quotient with IEEE division over every float of the object's clamped
+// sampling domain [vs*0.01, max(grid size) - vs*0.01].
+rkf_status Ctx::verify_exact_div() {
+  for (ObjDev& d : objdev_host) {
+    if (d.sdf_type != RKF_SDF_VOXELIZED || d.div_ok) continue;
+    const float hi = std::max(d.hi[0], std::max(d.hi[1], d.hi[2]));
+    if (!(d.lo > 0.0f) || !(hi > d.lo)) continue;
+    uint32_t b0, b1;
+    std::memcpy(&b0, &d.lo, 4);
+    std::memcpy(&b1, &hi, 4);
+    uint32_t vsb;
+    std::memcpy(&vsb, &d.vs, 4);
+    auto it = div_checked.find(vsb);
+    if (it != div_checked.end() && it->second.first <= b0 && it->second.second >= b1) {
+      d.div_ok = 1;
+      continue;
+    }
+    DevBuf bad;
+    rkf_status st = bad.alloc(4);
+    if (st != RKF_OK) return st;
+    RKF_CUDA_TRY(cudaMemsetAsync(bad.p, 0, 4, stream));
+    detail::k_verify_div<<<sm_count * 8, 256, 0, stream>>>(d.vs, d.rcp_vs, b0, b1 - b0 + 1,
+                                                          bad.as<unsigned int>());
+    RKF_CUDA_TRY(cudaGetLastError());
+    unsigned int nbad = 0;
+    RKF_CUDA_TRY(cudaMemcpyAsync(&nbad, bad.p, 4, cudaMemcpyDeviceToHost, stream));
+    RKF_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (nbad == 0) {
+      d.div_ok = 1;
+      div_checked[vsb] = {b0, b1};
+    }
+  }
+  return RKF_OK;
+}
+
 rkf_status Ctx::upload_objects() {
   if (objdev_host.empty()) return RKF_OK;
+  rkf_status vst = verify_exact_div();
+  if (vst != RKF_OK) return vst;
   const size_t bytes = objdev_host.size() * sizeof(ObjDev);
   if (objdev.bytes < bytes) {
     rkf_status st = objdev.alloc(bytes);

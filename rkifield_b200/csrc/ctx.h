@@ -98,6 +98,8 @@ struct Ctx {
   SceneDev scene_dev() const;
   uint32_t obj_count() const { return static_cast<uint32_t>(objects.size()); }
   rkf_status upload_objects();
+  rkf_status verify_exact_div();
+  std::map<uint32_t, std::pair<uint32_t, uint32_t>> div_checked;  // vs bits -> verified bit range
   rkf_status ensure_leaf_capacity(uint32_t need);
   rkf_status stage_bytes(size_t bytes);
 };

@@ -50,7 +50,22 @@ struct ObjDev {
   uint32_t sdf_type, prim_type, object_id, material_id;
   uint32_t has_geom;
   uint32_t has_flat;    // brick map lives in the reference flat buffer
+  float rcp_vs;         // RN(1/vs), for the exact quotient below
+  uint32_t div_ok;      // 1: exact_div_vs == IEEE x/vs verified on [lo, max(hi)]
+  uint32_t translate_only;  // inverse_world is identity in its linear part
+  float vs2;            // vs * 2 (INTERIOR value of the stepping sampler)
 };
+
+// x / vs rounded to nearest even, by one Markstein correction step of the
+// product with the rounded reciprocal (q0 = x*r, e = x - q0*vs exactly by
+// FMA, q = q0 + e*r).  An object uses it only after every float of its
+// clamped sampling domain has been checked against the IEEE quotient on the
+// device (ObjDev::div_ok); otherwise the IEEE division is used.
+__device__ __forceinline__ float exact_div_vs(float x, float vs, float rcp) {
+  const float q0 = __fmul_rn(x, rcp);
+  const float e = __fmaf_rn(-q0, vs, x);
+  return __fmaf_rn(e, rcp, q0);
+}
 
 struct SceneDev {
   const uint16_t* __restrict__ dist_f16;

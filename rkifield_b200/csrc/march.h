@@ -7,7 +7,7 @@
 
 namespace rkf {
 
-constexpr uint32_t kMaxObjectsFast = 64;
+constexpr uint32_t kMaxObjectsFast = 32;
 
 // One unit of batched work: a view (kind 0, primary rays over w x h pixels
 // walked in tile order) or a ray batch (kind 1).  Device pointers only.

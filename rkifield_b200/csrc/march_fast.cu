@@ -7,14 +7,18 @@
 // (normals), :1036-1112 (ray generation and G-buffer), and
 // shade_common_shading.wgsl:9-33 (soft_shadow).
 //
-// Execution model.  Each lane owns one ray at a time and advances a small
-// state machine (MARCH -> BISECT -> NORMAL -> EPILOGUE, or SHADOW) by exactly
-// one SDF sample per loop iteration, so the warp stays convergent on the
-// sampler whatever state each lane is in.  A lane whose ray finishes takes a
-// new ray from a global work counter (warp-aggregated atomic), so divergent
-// ray lengths do not idle lanes.  Work ids walk views tile by tile so the
-// rays a warp holds are spatially coherent.  The material of the hit is read
-// once, at the end, from the position that decided it.
+// Execution model.  Each lane owns one ray at a time.  A warp alternates
+//   1. refill: idle lanes take the next work ids from a global counter
+//      (one warp-aggregated atomic); ids walk views tile by tile, so a warp's
+//      rays stay spatially coherent;
+//   2. march: up to K sphere-tracing iterations (K = the compaction interval)
+//      in a tight loop, leaving early once no lane is still marching;
+//   3. finish: lanes that hit run their bisection (8 samples) and central
+//      differences (6 samples) together, one sample per iteration;
+//   4. epilogue: finished lanes write their G-buffer entry and go idle.
+// So a ray that ends early frees its lane within K iterations instead of
+// idling it until the slowest ray of the warp finishes.  The hit material is
+// read once, from the position that decided it.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -27,16 +31,17 @@ namespace rkf {
 
 namespace detail {
 
-enum : uint32_t { ST_IDLE = 0, ST_MARCH, ST_BISECT, ST_NORMAL, ST_EPI, ST_SHADOW, ST_DONE };
+enum : uint32_t { ST_IDLE = 0, ST_MARCH, ST_BISECT, ST_NORMAL, ST_EPI, ST_SHADOW };
 
 constexpr uint32_t kFull = 0xFFFFFFFFu;
 
 struct KParams {
+  ObjDev objs[kMaxObjectsFast];  // object table in the constant parameter bank
   SceneDev s;
   const Segment* segs;
   uint32_t nseg;
   uint32_t tile_w, tile_h;
-  uint32_t refill_interval;
+  uint32_t interval;
   uint64_t total;
   unsigned long long* counter;
   rkf_march_params p;
@@ -51,11 +56,34 @@ __device__ __forceinline__ uint32_t find_segment(const Segment* segs, uint32_t n
   return lo;
 }
 
-template <int PREC>
-__global__ void __launch_bounds__(256, 2) k_march_persistent(KParams kp) {
-  extern __shared__ ObjDev sh_objs[];
-  for (uint32_t i = threadIdx.x; i < kp.s.n_objs; i += blockDim.x) sh_objs[i] = kp.s.objs[i];
-  __syncthreads();
+// Minimum over objects [ob, oe) of evaluate_object at world position q.
+// SINGLE: the scene is exactly one object (object 0).
+template <int PREC, bool SINGLE>
+__device__ __forceinline__ float eval_min(const SceneDev& s, const ObjDev* objs, uint32_t ob,
+                                          uint32_t oe, float qx, float qy, float qz, float& best_un,
+                                          uint32_t& best_i, LaneCache& lc) {
+  if (SINGLE) {
+    best_i = 0;
+    return eval_obj<PREC>(s, objs[0], qx, qy, qz, &best_un, lc);
+  }
+  float best = kMaxFloat;
+  best_un = kMaxFloat;
+  best_i = ob;
+  for (uint32_t oi = ob; oi < oe; ++oi) {
+    float du;
+    const float d = eval_obj<PREC>(s, objs[oi], qx, qy, qz, &du, lc);
+    if (d < best) {
+      best = d;
+      best_un = du;
+      best_i = oi;
+    }
+  }
+  return best;
+}
+
+template <int PREC, bool SINGLE>
+__global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_constant__ KParams kp) {
+  const ObjDev* sh_objs = kp.objs;
   const SceneDev& s = kp.s;
   const rkf_march_params& p = kp.p;
   const uint32_t lane = threadIdx.x & 31;
@@ -65,250 +93,189 @@ __global__ void __launch_bounds__(256, 2) k_march_persistent(KParams kp) {
   LaneCache lc;
   uint32_t state = ST_IDLE;
   uint32_t seg = 0, idx = 0, mode = RKF_TRACE_CLOSEST;
-  float ox = 0, oy = 0, oz = 0, dx = 0, dy = 0, dz = 0, sx = 0, sy = 0, sz = 0;
+  float ox = 0, oy = 0, oz = 0, rdx = 0, rdy = 0, rdz = 0;
   float t = 0, prev_t = 0, prev_dist = kMaxFloat, tmax = 0;
   uint32_t near = 0, step = 0, sub = 0, hit_obj = 0;
-  float lo = 0, hi = 0, mat_t = 0, shadow = 1.0f;
+  float lo = 0, hi = 0, mat_t = 0, shadow = 1.0f, gpos = 0;
   bool mat_ok = false, bisected = false, hit = false;
-  float lpx = 0, lpy = 0, lpz = 0, eps = 0, g0 = 0, g1 = 0, g2 = 0, gpos = 0;
   bool exhausted = false;
-  uint32_t it = 0;
 
   for (;;) {
-    // ---- refill idle lanes -------------------------------------------------
-    const bool idle = state == ST_IDLE;
-    const uint32_t need = __ballot_sync(kFull, idle);
-    const bool all_idle = need == kFull;
-    if (need && !exhausted && (all_idle || (it % kp.refill_interval) == 0)) {
-      const uint32_t leader = __ffs(need) - 1;
-      unsigned long long base = 0;
-      if (lane == leader) base = atomicAdd(kp.counter, static_cast<unsigned long long>(__popc(need)));
-      base = __shfl_sync(kFull, base, leader);
-      if (base + __popc(need) >= kp.total) exhausted = true;
-      if (idle) {
-        const uint64_t id = base + __popc(need & ((1u << lane) - 1u));
-        if (id < kp.total) {
-          seg = find_segment(kp.segs, kp.nseg, id);
-          const Segment& sg = kp.segs[seg];
-          const uint64_t local = id - sg.first;
-          bool valid = true;
-          if (sg.kind == 0) {  // view: tile-ordered pixel ids
-            const uint32_t per = kp.tile_w * kp.tile_h;
-            const uint32_t tile = static_cast<uint32_t>(local / per);
-            const uint32_t r = static_cast<uint32_t>(local % per);
-            const uint32_t px = (tile % sg.tiles_x) * kp.tile_w + r % kp.tile_w;
-            const uint32_t py = (tile / sg.tiles_x) * kp.tile_h + r / kp.tile_w;
-            valid = px < sg.w && py < sg.h;
+    // ---- 1. refill idle lanes ------------------------------------------------
+    {
+      const bool idle = state == ST_IDLE;
+      const uint32_t need = __ballot_sync(kFull, idle);
+      if (need && !exhausted) {
+        const uint32_t leader = __ffs(need) - 1;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(kp.counter, static_cast<unsigned long long>(__popc(need)));
+        base = __shfl_sync(kFull, base, leader);
+        if (base + __popc(need) >= kp.total) exhausted = true;
+        if (idle) {
+          const uint64_t id = base + __popc(need & ((1u << lane) - 1u));
+          if (id < kp.total) {
+            seg = find_segment(kp.segs, kp.nseg, id);
+            const Segment& sg = kp.segs[seg];
+            const uint64_t local = id - sg.first;
+            bool valid = true;
+            if (sg.kind == 0) {  // view: tile-ordered pixel ids
+              const uint32_t per = kp.tile_w * kp.tile_h;
+              const uint32_t tile = static_cast<uint32_t>(local / per);
+              const uint32_t r = static_cast<uint32_t>(local % per);
+              const uint32_t px = (tile % sg.tiles_x) * kp.tile_w + r % kp.tile_w;
+              const uint32_t py = (tile / sg.tiles_x) * kp.tile_h + r / kp.tile_w;
+              valid = px < sg.w && py < sg.h;
+              if (valid) {
+                idx = py * sg.w + px;
+                // ray generation (ray_march.wgsl:1046-1053)
+                const float u = __fdiv_rn(__fadd_rn(__fadd_rn(static_cast<float>(px), 0.5f), sg.jitter[0]),
+                                          static_cast<float>(sg.w));
+                const float v = __fdiv_rn(__fadd_rn(__fadd_rn(static_cast<float>(py), 0.5f), sg.jitter[1]),
+                                          static_cast<float>(sg.h));
+                const float nx = __fsub_rn(__fmul_rn(u, 2.0f), 1.0f);
+                const float ny = __fsub_rn(1.0f, __fmul_rn(v, 2.0f));
+                const float vx = __fadd_rn(__fadd_rn(sg.fwd[0], __fmul_rn(sg.right[0], nx)), __fmul_rn(sg.up[0], ny));
+                const float vy = __fadd_rn(__fadd_rn(sg.fwd[1], __fmul_rn(sg.right[1], nx)), __fmul_rn(sg.up[1], ny));
+                const float vz = __fadd_rn(__fadd_rn(sg.fwd[2], __fmul_rn(sg.right[2], nx)), __fmul_rn(sg.up[2], ny));
+                const float l = len3(vx, vy, vz);
+                rdx = __fdiv_rn(vx, l);
+                rdy = __fdiv_rn(vy, l);
+                rdz = __fdiv_rn(vz, l);
+                ox = sg.pos[0];
+                oy = sg.pos[1];
+                oz = sg.pos[2];
+                tmax = p.scene.max_distance;
+                mode = RKF_TRACE_CLOSEST;
+              }
+            } else {
+              idx = static_cast<uint32_t>(local);
+              const size_t i3 = 3 * static_cast<size_t>(idx);
+              ox = __ldg(sg.origins + i3);
+              oy = __ldg(sg.origins + i3 + 1);
+              oz = __ldg(sg.origins + i3 + 2);
+              rdx = __ldg(sg.dirs + i3);
+              rdy = __ldg(sg.dirs + i3 + 1);
+              rdz = __ldg(sg.dirs + i3 + 2);
+              tmax = __ldg(sg.tmax + idx);
+              mode = sg.mode;
+            }
             if (valid) {
-              idx = py * sg.w + px;
-              // ray generation (ray_march.wgsl:1046-1053)
-              const float u = __fdiv_rn(__fadd_rn(__fadd_rn(static_cast<float>(px), 0.5f), sg.jitter[0]),
-                                        static_cast<float>(sg.w));
-              const float v = __fdiv_rn(__fadd_rn(__fadd_rn(static_cast<float>(py), 0.5f), sg.jitter[1]),
-                                        static_cast<float>(sg.h));
-              const float nx = __fsub_rn(__fmul_rn(u, 2.0f), 1.0f);
-              const float ny = __fsub_rn(1.0f, __fmul_rn(v, 2.0f));
-              const float vx = __fadd_rn(__fadd_rn(sg.fwd[0], __fmul_rn(sg.right[0], nx)), __fmul_rn(sg.up[0], ny));
-              const float vy = __fadd_rn(__fadd_rn(sg.fwd[1], __fmul_rn(sg.right[1], nx)), __fmul_rn(sg.up[1], ny));
-              const float vz = __fadd_rn(__fadd_rn(sg.fwd[2], __fmul_rn(sg.right[2], nx)), __fmul_rn(sg.up[2], ny));
-              const float l = len3(vx, vy, vz);
-              dx = __fdiv_rn(vx, l);
-              dy = __fdiv_rn(vy, l);
-              dz = __fdiv_rn(vz, l);
-              ox = sg.pos[0];
-              oy = sg.pos[1];
-              oz = sg.pos[2];
-              tmax = p.scene.max_distance;
-              mode = RKF_TRACE_CLOSEST;
+              near = 0;
+              step = 0;
+              hit = bisected = mat_ok = false;
+              if (mode == RKF_TRACE_SHADOW) {
+                t = 0.005f;  // SHADOW_EPSILON (shade_common.wgsl:274)
+                shadow = 1.0f;
+                state = ST_SHADOW;
+              } else {
+                t = 0.0f;
+                prev_t = 0.0f;
+                prev_dist = kMaxFloat;
+                state = ST_MARCH;
+              }
+            }
+          }
+        }
+      }
+      if (__all_sync(kFull, state == ST_IDLE)) {
+        if (exhausted) break;
+        continue;
+      }
+    }
+    // the march steps along the safe direction (ray_march.wgsl:784); hit
+    // positions use the raw direction (:1068)
+    const float qdx = fabsf(rdx) < 1e-10f ? 1e-10f : rdx;
+    const float qdy = fabsf(rdy) < 1e-10f ? 1e-10f : rdy;
+    const float qdz = fabsf(rdz) < 1e-10f ? 1e-10f : rdz;
+
+    // ---- 2. tight march loop -------------------------------------------------
+#pragma unroll 1
+    for (uint32_t k = 0; k < kp.interval; ++k) {
+      if (state == ST_MARCH) {
+        if (step >= p.hard_max_steps || t > tmax || near >= p.scene.max_steps) {
+          hit = false;
+          state = ST_EPI;
+        } else {
+          float best_un;
+          uint32_t best_i;
+          const float best = eval_min<PREC, SINGLE>(s, sh_objs, 0, nobj, __fadd_rn(ox, __fmul_rn(qdx, t)),
+                                                    __fadd_rn(oy, __fmul_rn(qdy, t)),
+                                                    __fadd_rn(oz, __fmul_rn(qdz, t)), best_un, best_i, lc);
+          if (best < 0.0f && prev_dist > hit_thr) {  // overstep (ray_march.wgsl:816)
+            hit_obj = best_i;
+            hit = true;
+            if (mode == RKF_TRACE_ANY) {
+              state = ST_EPI;
+            } else {
+              lo = prev_t;
+              hi = t;
+              mat_t = t;
+              mat_ok = best_un < sh_objs[best_i].vs16;
+              sub = 0;
+              bisected = true;
+              state = ST_BISECT;
+            }
+          } else if (best < hit_thr) {  // :842
+            hit_obj = best_i;
+            hit = true;
+            if (mode == RKF_TRACE_ANY) {
+              state = ST_EPI;
+            } else {
+              // a direct hit: enter the finish phase with the bisection done
+              mat_t = t;
+              mat_ok = best_un < sh_objs[best_i].vs16;
+              sub = p.bisect_steps;
+              state = ST_BISECT;
             }
           } else {
-            idx = static_cast<uint32_t>(local);
-            ox = __ldg(sg.origins + 3 * static_cast<size_t>(idx));
-            oy = __ldg(sg.origins + 3 * static_cast<size_t>(idx) + 1);
-            oz = __ldg(sg.origins + 3 * static_cast<size_t>(idx) + 2);
-            dx = __ldg(sg.dirs + 3 * static_cast<size_t>(idx));
-            dy = __ldg(sg.dirs + 3 * static_cast<size_t>(idx) + 1);
-            dz = __ldg(sg.dirs + 3 * static_cast<size_t>(idx) + 2);
-            tmax = __ldg(sg.tmax + idx);
-            mode = sg.mode;
+            if (best < p.near_surface_threshold) near++;
+            prev_t = t;
+            prev_dist = best;
+            t = __fadd_rn(t, fmax_(best, p.min_step));
+            step++;
           }
-          if (valid) {
-            sx = fabsf(dx) < 1e-10f ? 1e-10f : dx;  // safe_dir (ray_march.wgsl:784)
-            sy = fabsf(dy) < 1e-10f ? 1e-10f : dy;
-            sz = fabsf(dz) < 1e-10f ? 1e-10f : dz;
-            near = 0;
-            step = 0;
-            sub = 0;
-            hit = bisected = mat_ok = false;
-            if (mode == RKF_TRACE_SHADOW) {
-              t = 0.005f;  // SHADOW_EPSILON (shade_common.wgsl:274)
-              shadow = 1.0f;
-              state = ST_SHADOW;
-            } else {
-              t = 0.0f;
-              prev_t = 0.0f;
-              prev_dist = kMaxFloat;
-              state = ST_MARCH;
+        }
+      } else if (state == ST_SHADOW) {
+        // soft_shadow (shade_common_shading.wgsl:9-33)
+        if (step >= 256u || near >= 32u || t > tmax) {
+          shadow = clampf(shadow, 0.0f, 1.0f);
+          hit = false;
+          state = ST_EPI;
+        } else {
+          float best_un;
+          uint32_t best_i;
+          const float best = eval_min<PREC, SINGLE>(s, sh_objs, 0, nobj, __fadd_rn(ox, __fmul_rn(rdx, t)),
+                                                    __fadd_rn(oy, __fmul_rn(rdy, t)),
+                                                    __fadd_rn(oz, __fmul_rn(rdz, t)), best_un, best_i, lc);
+          if (best < 0.005f) {
+            shadow = 0.0f;
+            hit = true;
+            state = ST_EPI;
+          } else {
+            if (best < 0.02f) {
+              shadow = fmin_(shadow, __fdiv_rn(__fmul_rn(16.0f, best), t));
+              near++;
             }
+            t = __fadd_rn(t, fmax_(best, 0.005f));
+            step++;
           }
         }
       }
-    }
-    if (__all_sync(kFull, state == ST_IDLE)) {
-      if (exhausted) break;
-      ++it;
-      continue;
-    }
-    ++it;
-
-    // ---- terminal checks at the top of a march / shadow iteration ----------
-    if (state == ST_MARCH) {
-      if (step >= p.hard_max_steps || t > tmax || near >= p.scene.max_steps) {
-        hit = false;
-        state = ST_EPI;
-      }
-    } else if (state == ST_SHADOW) {
-      if (step >= 256u || near >= 32u || t > tmax) {  // shade_common_shading.wgsl:17-20
-        shadow = clampf(shadow, 0.0f, 1.0f);
-        hit = false;
-        state = ST_EPI;
-      }
+      if ((k & 3u) == 3u && !__any_sync(kFull, state == ST_MARCH || state == ST_SHADOW)) break;
     }
 
-    // ---- phase A: what to sample -------------------------------------------
-    uint32_t ob = 0, oe = 0;
-    bool local_space = false, grad = false;
-    float qx = 0, qy = 0, qz = 0;
-    if (state == ST_MARCH || state == ST_SHADOW) {
-      ob = 0;
-      oe = nobj;
-      qx = __fadd_rn(ox, __fmul_rn(sx, t));
-      qy = __fadd_rn(oy, __fmul_rn(sy, t));
-      qz = __fadd_rn(oz, __fmul_rn(sz, t));
-    } else if (state == ST_BISECT) {
-      ob = hit_obj;
-      oe = hit_obj + 1;
-      const float mid = __fmul_rn(__fadd_rn(lo, hi), 0.5f);
-      gpos = mid;
-      qx = __fadd_rn(ox, __fmul_rn(sx, mid));
-      qy = __fadd_rn(oy, __fmul_rn(sy, mid));
-      qz = __fadd_rn(oz, __fmul_rn(sz, mid));
-    } else if (state == ST_NORMAL) {
-      ob = hit_obj;
-      oe = hit_obj + 1;
-      const uint32_t ax = sub >> 1;
-      qx = lpx;
-      qy = lpy;
-      qz = lpz;
-      if (ax == 0) qx = (sub & 1) ? __fsub_rn(lpx, eps) : __fadd_rn(lpx, eps);
-      if (ax == 1) qy = (sub & 1) ? __fsub_rn(lpy, eps) : __fadd_rn(lpy, eps);
-      if (ax == 2) qz = (sub & 1) ? __fsub_rn(lpz, eps) : __fadd_rn(lpz, eps);
-      local_space = sh_objs[hit_obj].sdf_type == RKF_SDF_VOXELIZED;
-      grad = true;
-    }
-
-    // ---- phase B: one SDF sample (min over the requested objects) ---------
-    float best = kMaxFloat, best_un = kMaxFloat;
-    uint32_t best_i = 0;
-    for (uint32_t oi = ob; oi < oe; ++oi) {
-      const ObjDev& o = sh_objs[oi];
-      float d, du;
-      if (local_space) {
-        d = sample_vox<PREC>(s, o, oi, qx, qy, qz, grad, lc);
-        du = d;
-      } else {
-        d = eval_obj<PREC>(s, o, oi, qx, qy, qz, &du, lc);
-      }
-      if (d < best) {
-        best = d;
-        best_un = du;
-        best_i = oi;
-      }
-    }
-
-    // ---- phase C: advance the state machine -------------------------------
-    bool to_normal = false;
-    if (state == ST_MARCH) {
-      if (best < 0.0f && prev_dist > hit_thr) {  // overstep (ray_march.wgsl:816)
-        hit_obj = best_i;
-        if (mode == RKF_TRACE_ANY) {
-          hit = true;
-          state = ST_EPI;
-        } else {
-          lo = prev_t;
-          hi = t;
-          mat_t = t;
-          mat_ok = best_un < sh_objs[best_i].vs16;
-          sub = 0;
-          bisected = true;
-          state = p.bisect_steps ? ST_BISECT : ST_NORMAL;
-          if (!p.bisect_steps) t = __fmul_rn(__fadd_rn(lo, hi), 0.5f);
-        }
-        if (state == ST_NORMAL) to_normal = true;
-      } else if (best < hit_thr) {  // :842
-        hit_obj = best_i;
-        if (mode == RKF_TRACE_ANY) {
-          hit = true;
-          state = ST_EPI;
-        } else {
-          mat_t = t;
-          mat_ok = best_un < sh_objs[best_i].vs16;
-          to_normal = true;
-        }
-      } else {
-        if (best < p.near_surface_threshold) near++;
-        prev_t = t;
-        prev_dist = best;
-        t = __fadd_rn(t, fmax_(best, p.min_step));
-        step++;
-      }
-    } else if (state == ST_BISECT) {
-      if (best < 0.0f) {
-        hi = gpos;
-      } else {
-        lo = gpos;
-        mat_t = gpos;
-        mat_ok = best_un < sh_objs[hit_obj].vs16;
-      }
-      if (++sub == p.bisect_steps) {
-        t = __fmul_rn(__fadd_rn(lo, hi), 0.5f);
-        to_normal = true;
-      }
-    } else if (state == ST_NORMAL) {
-      if (sub & 1) {
-        const float g = __fsub_rn(gpos, best);
-        if ((sub >> 1) == 0) g0 = g;
-        else if ((sub >> 1) == 1) g1 = g;
-        else g2 = g;
-      } else {
-        gpos = best;
-      }
-      if (++sub == 6) state = ST_EPI;
-    } else if (state == ST_SHADOW) {
-      // soft_shadow body (shade_common_shading.wgsl:21-31)
-      if (best < 0.005f) {
-        shadow = 0.0f;
-        hit = true;
-        state = ST_EPI;
-      } else {
-        if (best < 0.02f) {
-          shadow = fmin_(shadow, __fdiv_rn(__fmul_rn(16.0f, best), t));
-          near++;
-        }
-        t = __fadd_rn(t, fmax_(best, 0.005f));
-        step++;
-      }
-    }
-    if (to_normal) {
-      hit = true;
-      {
+    // ---- 3. finish: bisection and central differences -------------------------
+    float g0 = 0, g1 = 0, g2 = 0, lpx = 0, lpy = 0, lpz = 0, eps = 0;
+    while (__any_sync(kFull, state == ST_BISECT || state == ST_NORMAL)) {
+      if (state == ST_BISECT && sub >= p.bisect_steps) {
+        // bisection done (or a direct hit): t = (lo+hi)/2, set up the normal
+        if (bisected) t = __fmul_rn(__fadd_rn(lo, hi), 0.5f);
         const ObjDev& o = sh_objs[hit_obj];
-        // hit_pos = ray_origin + ray_dir * t (ray_march.wgsl:1068)
-        const float hx = __fadd_rn(ox, __fmul_rn(dx, t));
-        const float hy = __fadd_rn(oy, __fmul_rn(dy, t));
-        const float hz = __fadd_rn(oz, __fmul_rn(dz, t));
+        const float hx = __fadd_rn(ox, __fmul_rn(rdx, t));
+        const float hy = __fadd_rn(oy, __fmul_rn(rdy, t));
+        const float hz = __fadd_rn(oz, __fmul_rn(rdz, t));
         if (o.sdf_type == RKF_SDF_VOXELIZED) {
-          to_local(o, hx, hy, hz, lpx, lpy, lpz);
+          to_local_fast(o, hx, hy, hz, lpx, lpy, lpz);
           eps = __fmul_rn(o.vs, 2.0f);
         } else {
           lpx = hx;
@@ -316,15 +283,52 @@ __global__ void __launch_bounds__(256, 2) k_march_persistent(KParams kp) {
           lpz = hz;
           eps = __fmul_rn(hit_thr, 10.0f);
         }
+        sub = 0;
+        state = ST_NORMAL;
       }
-      sub = 0;
-      state = ST_NORMAL;
+      if (state == ST_BISECT) {
+        const float mid = __fmul_rn(__fadd_rn(lo, hi), 0.5f);
+        float du;
+        const float d = eval_obj<PREC>(s, sh_objs[hit_obj], __fadd_rn(ox, __fmul_rn(qdx, mid)),
+                                       __fadd_rn(oy, __fmul_rn(qdy, mid)), __fadd_rn(oz, __fmul_rn(qdz, mid)),
+                                       &du, lc);
+        if (d < 0.0f) {
+          hi = mid;
+        } else {
+          lo = mid;
+          mat_t = mid;
+          mat_ok = du < sh_objs[hit_obj].vs16;
+        }
+        ++sub;
+      } else if (state == ST_NORMAL) {
+        const ObjDev& o = sh_objs[hit_obj];
+        const uint32_t ax = sub >> 1;
+        float qx = lpx, qy = lpy, qz = lpz;
+        if (ax == 0) qx = (sub & 1) ? __fsub_rn(lpx, eps) : __fadd_rn(lpx, eps);
+        if (ax == 1) qy = (sub & 1) ? __fsub_rn(lpy, eps) : __fadd_rn(lpy, eps);
+        if (ax == 2) qz = (sub & 1) ? __fsub_rn(lpz, eps) : __fadd_rn(lpz, eps);
+        float d;
+        if (o.sdf_type == RKF_SDF_VOXELIZED) {
+          d = sample_vox<PREC>(s, o, qx, qy, qz, true, lc);
+        } else {
+          float du;
+          d = eval_obj<PREC>(s, o, qx, qy, qz, &du, lc);
+        }
+        if (sub & 1) {
+          const float g = __fsub_rn(gpos, d);
+          if (ax == 0) g0 = g;
+          else if (ax == 1) g1 = g;
+          else g2 = g;
+        } else {
+          gpos = d;
+        }
+        if (++sub == 6) state = ST_EPI;
+      }
     }
 
-    // ---- epilogue: outputs of a finished ray --------------------------------
+    // ---- 4. epilogue: outputs of finished rays -------------------------------
     if (state == ST_EPI) {
       const Segment& sg = kp.segs[seg];
-      uint16_t flags = 0;
       if (mode == RKF_TRACE_SHADOW) {
         sg.t[idx] = shadow;
         if (sg.flags) sg.flags[idx] = hit ? RKF_FLAG_HIT : 0;
@@ -334,6 +338,7 @@ __global__ void __launch_bounds__(256, 2) k_march_persistent(KParams kp) {
           sg.flags[idx] = hit ? RKF_FLAG_HIT
                               : ((step >= p.hard_max_steps || near >= p.scene.max_steps) ? RKF_FLAG_STEPS_OUT : 0);
       } else {
+        uint16_t flags = 0;
         float nx = 0, ny = 0, nz = 0;
         uint32_t slot = RKF_EMPTY_SLOT, mat = 0, sec = 0, blend = 0;
         float hx = 0, hy = 0, hz = 0, sdf_hit = 0;
@@ -341,9 +346,9 @@ __global__ void __launch_bounds__(256, 2) k_march_persistent(KParams kp) {
           flags |= RKF_FLAG_HIT;
           if (bisected) flags |= RKF_FLAG_BISECTED;
           const ObjDev& o = sh_objs[hit_obj];
-          hx = __fadd_rn(ox, __fmul_rn(dx, t));
-          hy = __fadd_rn(oy, __fmul_rn(dy, t));
-          hz = __fadd_rn(oz, __fmul_rn(dz, t));
+          hx = __fadd_rn(ox, __fmul_rn(rdx, t));
+          hy = __fadd_rn(oy, __fmul_rn(rdy, t));
+          hz = __fadd_rn(oz, __fmul_rn(rdz, t));
           if (o.sdf_type == RKF_SDF_VOXELIZED) {
             // world_grad = transpose(inverse_world) * (g, 0)  (:1014)
             const float wx = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(o.m[0], g0), __fmul_rn(o.m[1], g1)),
@@ -354,30 +359,25 @@ __global__ void __launch_bounds__(256, 2) k_march_persistent(KParams kp) {
                                                  __fmul_rn(o.m[10], g2)), __fmul_rn(o.m[11], 0.0f));
             const float l = len3(wx, wy, wz);
             if (l < 1e-10f) {
-              nx = 0.0f; ny = 1.0f; nz = 0.0f;
+              ny = 1.0f;
             } else {
               nx = __fdiv_rn(wx, l); ny = __fdiv_rn(wy, l); nz = __fdiv_rn(wz, l);
             }
-            float lx, ly, lz;
-            to_local(o, hx, hy, hz, lx, ly, lz);
             uint32_t vi = 0;
-            slot = nearest_slot(s, o, hit_obj, lx, ly, lz, vi, lc);
+            slot = nearest_slot(s, o, lpx, lpy, lpz, vi, lc);
             if (slot < RKF_INTERIOR_SLOT) {
               const size_t v = static_cast<size_t>(slot) * 512 + vi;
               sec = (__ldg(s.mat + v) >> 6) & 0x3Fu;
               blend = __ldg(s.blend + v);
             }
-            if (sg.motion) sdf_hit = sample_vox<PREC>(s, o, hit_obj, lx, ly, lz, false, lc);
+            if (sg.motion) sdf_hit = sample_vox<PREC>(s, o, lpx, lpy, lpz, false, lc);
           } else {
             const float l = len3(g0, g1, g2);
             nx = __fdiv_rn(g0, l); ny = __fdiv_rn(g1, l); nz = __fdiv_rn(g2, l);
           }
-          if (mat_ok || o.sdf_type == RKF_SDF_ANALYTICAL) {
-            const float mx = __fadd_rn(ox, __fmul_rn(sx, mat_t));
-            const float my = __fadd_rn(oy, __fmul_rn(sy, mat_t));
-            const float mz = __fadd_rn(oz, __fmul_rn(sz, mat_t));
-            mat = material_at(s, o, hit_obj, mx, my, mz, lc);
-          }
+          if (mat_ok || o.sdf_type == RKF_SDF_ANALYTICAL)
+            mat = material_at(s, o, __fadd_rn(ox, __fmul_rn(qdx, mat_t)), __fadd_rn(oy, __fmul_rn(qdy, mat_t)),
+                              __fadd_rn(oz, __fmul_rn(qdz, mat_t)), lc);
         } else if (step >= p.hard_max_steps || near >= p.scene.max_steps) {
           flags |= RKF_FLAG_STEPS_OUT;
         }
@@ -391,12 +391,11 @@ __global__ void __launch_bounds__(256, 2) k_march_persistent(KParams kp) {
         if (sg.material) sg.material[idx] = static_cast<uint16_t>(mat);
         if (sg.flags) sg.flags[idx] = flags;
         if (sg.position) {
-          float4 pv = hit ? make_float4(hx, hy, hz, t) : make_float4(0.f, 0.f, 0.f, kMaxFloat);
+          const float4 pv = hit ? make_float4(hx, hy, hz, t) : make_float4(0.f, 0.f, 0.f, kMaxFloat);
           reinterpret_cast<float4*>(sg.position)[idx] = pv;
         }
         if (sg.packed)
-          sg.packed[idx] = hit ? ((mat & 0x3Fu) | (sec << 6) | (blend << 12) |
-                                  (sh_objs[hit_obj].object_id << 24))
+          sg.packed[idx] = hit ? ((mat & 0x3Fu) | (sec << 6) | (blend << 12) | (sh_objs[hit_obj].object_id << 24))
                                : 0u;
         if (sg.motion) {
           float4 mv = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -441,23 +440,15 @@ __global__ void k_query_points(SceneDev s, const float* __restrict__ pts, uint32
   LaneCache lc;
   const float px = pts[3 * static_cast<size_t>(i)], py = pts[3 * static_cast<size_t>(i) + 1],
               pz = pts[3 * static_cast<size_t>(i) + 2];
-  float best = kMaxFloat, best_un = kMaxFloat;
+  float best_un = kMaxFloat;
   uint32_t bi = 0;
-  for (uint32_t oi = 0; oi < s.n_objs; ++oi) {
-    float du;
-    const float d = eval_obj<PREC>(s, sh_objs[oi], oi, px, py, pz, &du, lc);
-    if (d < best) {
-      best = d;
-      best_un = du;
-      bi = oi;
-    }
-  }
+  const float best = eval_min<PREC, false>(s, sh_objs, 0, s.n_objs, px, py, pz, best_un, bi, lc);
   if (dist) dist[i] = best;
   if (material) {
     uint32_t m = 0;
     if (s.n_objs) {
       const ObjDev& o = sh_objs[bi];
-      if (o.sdf_type == RKF_SDF_ANALYTICAL || best_un < o.vs16) m = material_at(s, o, bi, px, py, pz, lc);
+      if (o.sdf_type == RKF_SDF_ANALYTICAL || best_un < o.vs16) m = material_at(s, o, px, py, pz, lc);
     }
     material[i] = static_cast<uint16_t>(m);
   }
@@ -467,14 +458,14 @@ __global__ void k_query_points(SceneDev s, const float* __restrict__ pts, uint32
       const ObjDev& o = sh_objs[bi];
       if (o.sdf_type == RKF_SDF_VOXELIZED) {
         float lx, ly, lz;
-        to_local(o, px, py, pz, lx, ly, lz);
+        to_local_fast(o, px, py, pz, lx, ly, lz);
         const float e = __fmul_rn(o.vs, 2.0f);
-        const float g0 = __fsub_rn(sample_vox<PREC>(s, o, bi, __fadd_rn(lx, e), ly, lz, true, lc),
-                                   sample_vox<PREC>(s, o, bi, __fsub_rn(lx, e), ly, lz, true, lc));
-        const float g1 = __fsub_rn(sample_vox<PREC>(s, o, bi, lx, __fadd_rn(ly, e), lz, true, lc),
-                                   sample_vox<PREC>(s, o, bi, lx, __fsub_rn(ly, e), lz, true, lc));
-        const float g2 = __fsub_rn(sample_vox<PREC>(s, o, bi, lx, ly, __fadd_rn(lz, e), true, lc),
-                                   sample_vox<PREC>(s, o, bi, lx, ly, __fsub_rn(lz, e), true, lc));
+        const float g0 = __fsub_rn(sample_vox<PREC>(s, o, __fadd_rn(lx, e), ly, lz, true, lc),
+                                   sample_vox<PREC>(s, o, __fsub_rn(lx, e), ly, lz, true, lc));
+        const float g1 = __fsub_rn(sample_vox<PREC>(s, o, lx, __fadd_rn(ly, e), lz, true, lc),
+                                   sample_vox<PREC>(s, o, lx, __fsub_rn(ly, e), lz, true, lc));
+        const float g2 = __fsub_rn(sample_vox<PREC>(s, o, lx, ly, __fadd_rn(lz, e), true, lc),
+                                   sample_vox<PREC>(s, o, lx, ly, __fsub_rn(lz, e), true, lc));
         const float wx = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(o.m[0], g0), __fmul_rn(o.m[1], g1)),
                                              __fmul_rn(o.m[2], g2)), __fmul_rn(o.m[3], 0.0f));
         const float wy = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(o.m[4], g0), __fmul_rn(o.m[5], g1)),
@@ -489,12 +480,12 @@ __global__ void k_query_points(SceneDev s, const float* __restrict__ pts, uint32
         // analytic: central differences with eps = 10 * hit_threshold(0.001)
         const float e = __fmul_rn(0.001f, 10.0f);
         float du;
-        const float a = __fsub_rn(eval_obj<PREC>(s, o, bi, __fadd_rn(px, e), py, pz, &du, lc),
-                                  eval_obj<PREC>(s, o, bi, __fsub_rn(px, e), py, pz, &du, lc));
-        const float b = __fsub_rn(eval_obj<PREC>(s, o, bi, px, __fadd_rn(py, e), pz, &du, lc),
-                                  eval_obj<PREC>(s, o, bi, px, __fsub_rn(py, e), pz, &du, lc));
-        const float c = __fsub_rn(eval_obj<PREC>(s, o, bi, px, py, __fadd_rn(pz, e), &du, lc),
-                                  eval_obj<PREC>(s, o, bi, px, py, __fsub_rn(pz, e), &du, lc));
+        const float a = __fsub_rn(eval_obj<PREC>(s, o, __fadd_rn(px, e), py, pz, &du, lc),
+                                  eval_obj<PREC>(s, o, __fsub_rn(px, e), py, pz, &du, lc));
+        const float b = __fsub_rn(eval_obj<PREC>(s, o, px, __fadd_rn(py, e), pz, &du, lc),
+                                  eval_obj<PREC>(s, o, px, __fsub_rn(py, e), pz, &du, lc));
+        const float c = __fsub_rn(eval_obj<PREC>(s, o, px, py, __fadd_rn(pz, e), &du, lc),
+                                  eval_obj<PREC>(s, o, px, py, __fsub_rn(pz, e), &du, lc));
         const float l = len3(a, b, c);
         nx = __fdiv_rn(a, l); ny = __fdiv_rn(b, l); nz = __fdiv_rn(c, l);
       }
@@ -505,6 +496,11 @@ __global__ void k_query_points(SceneDev s, const float* __restrict__ pts, uint32
   }
 }
 
+template <int PREC, bool SINGLE>
+const void* persistent_fn() {
+  return reinterpret_cast<const void*>(&k_march_persistent<PREC, SINGLE>);
+}
+
 }  // namespace detail
 
 rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint64_t total,
@@ -512,6 +508,7 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
                              cudaStream_t st, DevBuf* seg_buf, unsigned long long* counter) {
   if (c->obj_count() > kMaxObjectsFast)
     return fail(RKF_UNSUPPORTED, "march: more objects than the persistent kernel holds");
+  if (c->obj_count() == 0) return fail(RKF_INVALID_ARG, "march: the scene has no objects");
   const size_t sb = segs_host.size() * sizeof(Segment);
   if (seg_buf->bytes < sb) {
     rkf_status s2 = seg_buf->alloc(sb);
@@ -520,48 +517,46 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   RKF_CUDA_TRY(cudaMemcpyAsync(seg_buf->p, segs_host.data(), sb, cudaMemcpyHostToDevice, st));
   RKF_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
   detail::KParams kp;
+  std::memset(&kp, 0, sizeof(kp));
+  std::memcpy(kp.objs, c->objdev_host.data(), sizeof(ObjDev) * c->obj_count());
   kp.s = c->scene_dev();
   kp.segs = seg_buf->as<Segment>();
   kp.nseg = static_cast<uint32_t>(segs_host.size());
   kp.tile_w = tu.tile_w ? tu.tile_w : 8;
   kp.tile_h = tu.tile_h ? tu.tile_h : 4;
-  kp.refill_interval = tu.compact_interval ? tu.compact_interval : 1;
+  kp.interval = tu.compact_interval ? tu.compact_interval : 16;
   kp.total = total;
   kp.counter = counter;
   kp.p = *p;
   kp.p.scene.num_objects = c->obj_count();
+  const bool single = c->obj_count() == 1;
+  const void* fn = nullptr;
+  switch (c->cfg.precision) {
+    case RKF_PRECISION_F32:
+      fn = single ? detail::persistent_fn<RKF_PRECISION_F32, true>() : detail::persistent_fn<RKF_PRECISION_F32, false>();
+      break;
+    case RKF_PRECISION_U8:
+      fn = single ? detail::persistent_fn<RKF_PRECISION_U8, true>() : detail::persistent_fn<RKF_PRECISION_U8, false>();
+      break;
+    default:
+      fn = single ? detail::persistent_fn<RKF_PRECISION_F16, true>() : detail::persistent_fn<RKF_PRECISION_F16, false>();
+  }
   const uint32_t threads = tu.threads_per_block ? tu.threads_per_block : 256;
+  if (threads > 256 || threads % 32)
+    return fail(RKF_INVALID_ARG, "march: threads_per_block must be a multiple of 32 <= 256");
+  const size_t smem = 0;
   uint32_t bps = tu.blocks_per_sm;
-  const size_t smem = sizeof(ObjDev) * std::max<uint32_t>(1, c->obj_count());
   if (bps == 0) {
     int occ = 0;
-    switch (c->cfg.precision) {
-      case RKF_PRECISION_F32:
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, detail::k_march_persistent<RKF_PRECISION_F32>, threads, smem);
-        break;
-      case RKF_PRECISION_U8:
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, detail::k_march_persistent<RKF_PRECISION_U8>, threads, smem);
-        break;
-      default:
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, detail::k_march_persistent<RKF_PRECISION_F16>, threads, smem);
-    }
+    RKF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem));
     bps = occ > 0 ? static_cast<uint32_t>(occ) : 1;
   }
   // never launch more lanes than work items
   uint64_t blocks = static_cast<uint64_t>(c->sm_count) * bps;
   const uint64_t need_blocks = (total + threads - 1) / threads;
   if (blocks > need_blocks) blocks = need_blocks ? need_blocks : 1;
-  switch (c->cfg.precision) {
-    case RKF_PRECISION_F32:
-      detail::k_march_persistent<RKF_PRECISION_F32><<<static_cast<unsigned>(blocks), threads, smem, st>>>(kp);
-      break;
-    case RKF_PRECISION_U8:
-      detail::k_march_persistent<RKF_PRECISION_U8><<<static_cast<unsigned>(blocks), threads, smem, st>>>(kp);
-      break;
-    default:
-      detail::k_march_persistent<RKF_PRECISION_F16><<<static_cast<unsigned>(blocks), threads, smem, st>>>(kp);
-  }
-  RKF_CUDA_TRY(cudaGetLastError());
+  void* args[] = {&kp};
+  RKF_CUDA_TRY(cudaLaunchKernel(fn, dim3(static_cast<unsigned>(blocks)), dim3(threads), args, smem, st));
   return RKF_OK;
 }
 
@@ -592,6 +587,8 @@ Segment view_segment(const rkf_camera* cam, uint32_t w, uint32_t h, uint32_t til
   sg.mode = RKF_TRACE_CLOSEST;
   sg.w = w;
   sg.h = h;
+  if (!tile_w) tile_w = 8;
+  if (!tile_h) tile_h = 4;
   sg.tiles_x = (w + tile_w - 1) / tile_w;
   const uint32_t tiles_y = (h + tile_h - 1) / tile_h;
   sg.n_ids = static_cast<uint64_t>(sg.tiles_x) * tiles_y * tile_w * tile_h;
@@ -604,7 +601,7 @@ Segment view_segment(const rkf_camera* cam, uint32_t w, uint32_t h, uint32_t til
   sg.jitter[0] = cam->jitter[0];
   sg.jitter[1] = cam->jitter[1];
   std::memcpy(sg.prev_vp, cam->prev_vp, sizeof(sg.prev_vp));
-  sg.t = static_cast<float*>(out.t ? out.t : nullptr);
+  sg.t = out.t;
   sg.normal = out.normal;
   sg.slot = out.slot;
   sg.material = out.material;
