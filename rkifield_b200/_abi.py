@@ -201,6 +201,8 @@ SIGNATURES = {
     "rkf_edit_csg": (_I, [_P, C.POINTER(rkf_edit_op), C.POINTER(_U64)]),
     "rkf_march_batch": (_I, [_P, C.POINTER(rkf_view), _U32, C.POINTER(rkf_ray_batch), _U32,
                              C.POINTER(rkf_march_params), C.POINTER(rkf_batch_tuning)]),
+    "rkf_march_batch_noalloc": (_I, [_P, C.POINTER(rkf_view), _U32, C.POINTER(rkf_ray_batch), _U32,
+                                     C.POINTER(rkf_march_params), C.POINTER(rkf_batch_tuning), _P]),
     "rkf_autotune": (_I, [_P, C.POINTER(rkf_view), _U32, C.POINTER(rkf_ray_batch), _U32,
                           C.POINTER(rkf_march_params), C.POINTER(rkf_batch_tuning)]),
     "rkf_serve_start": (_I, [_P, C.POINTER(rkf_march_params)]),

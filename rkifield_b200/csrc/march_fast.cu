@@ -560,6 +560,56 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   return RKF_OK;
 }
 
+rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t nseg, uint64_t total,
+                                     const rkf_march_params* p, const rkf_batch_tuning& tu,
+                                     cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter) {
+  if (c->obj_count() > kMaxObjectsFast)
+    return fail(RKF_UNSUPPORTED, "march: more objects than the persistent kernel holds");
+  if (c->obj_count() == 0) return fail(RKF_INVALID_ARG, "march: the scene has no objects");
+  RKF_CUDA_TRY(cudaMemcpyAsync(dev_segs, segs_host, sizeof(Segment) * nseg, cudaMemcpyHostToDevice, st));
+  RKF_CUDA_TRY(cudaMemsetAsync(dev_counter, 0, sizeof(unsigned long long), st));
+  detail::KParams kp;
+  std::memset(&kp, 0, sizeof(kp));
+  std::memcpy(kp.objs, c->objdev_host.data(), sizeof(ObjDev) * c->obj_count());
+  kp.s = c->scene_dev();
+  kp.segs = dev_segs;
+  kp.nseg = nseg;
+  kp.tile_w = tu.tile_w ? tu.tile_w : 8;
+  kp.tile_h = tu.tile_h ? tu.tile_h : 4;
+  kp.interval = tu.compact_interval ? tu.compact_interval : 16;
+  kp.total = total;
+  kp.counter = dev_counter;
+  kp.p = *p;
+  kp.p.scene.num_objects = c->obj_count();
+  const bool single = c->obj_count() == 1;
+  const void* fn = nullptr;
+  switch (c->cfg.precision) {
+    case RKF_PRECISION_F32:
+      fn = single ? detail::persistent_fn<RKF_PRECISION_F32, true>() : detail::persistent_fn<RKF_PRECISION_F32, false>();
+      break;
+    case RKF_PRECISION_U8:
+      fn = single ? detail::persistent_fn<RKF_PRECISION_U8, true>() : detail::persistent_fn<RKF_PRECISION_U8, false>();
+      break;
+    default:
+      fn = single ? detail::persistent_fn<RKF_PRECISION_F16, true>() : detail::persistent_fn<RKF_PRECISION_F16, false>();
+  }
+  const uint32_t threads = tu.threads_per_block ? tu.threads_per_block : 256;
+  if (threads > 256 || threads % 32)
+    return fail(RKF_INVALID_ARG, "march: threads_per_block must be a multiple of 32 <= 256");
+  uint32_t bps = tu.blocks_per_sm;
+  if (bps == 0) {
+    int occ = 0;
+    RKF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, 0));
+    bps = occ > 0 ? static_cast<uint32_t>(occ) : 1;
+  }
+  uint64_t blocks = static_cast<uint64_t>(c->sm_count) * bps;
+  const uint64_t need_blocks = (total + threads - 1) / threads;
+  if (blocks > need_blocks) blocks = need_blocks ? need_blocks : 1;
+  void* args[] = {&kp};
+  RKF_CUDA_TRY(cudaLaunchKernel(fn, dim3(static_cast<unsigned>(blocks)), dim3(threads), args, 0, st));
+  return RKF_OK;
+}
+
 rkf_status launch_query(Ctx* c, const float* pts, uint32_t n, float* d, float* g, uint16_t* m,
                         cudaStream_t st) {
   if (n == 0) return RKF_OK;
