@@ -1,0 +1,122 @@
+"""GPU parity of ray casts, point queries and the batched march.
+
+Ray casts in the three modes (closest hit = the full march of
+ray_march.wgsl:776-858 with normals and material; any hit; soft shadow of
+shade_common_shading.wgsl:9-33) and point queries (SdfQueryable over the
+pool, sdf_collision.rs:38-56) are compared bit for bit with the FP32 oracle.
+The batched launch must return exactly what separate calls return.
+"""
+import numpy as np
+import pytest
+
+from conftest import assert_bits_equal
+
+pytestmark = pytest.mark.gpu
+
+
+def _rays(n, seed, box=18.0, zero_components=True):
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(-box, box, (n, 3)).astype(np.float32)
+    d = rng.standard_normal((n, 3)).astype(np.float32)
+    if zero_components:  # axis-aligned rays exercise the 1e-10 safe direction
+        d[: n // 16, 1] = 0.0
+        d[n // 16: n // 8, 0] = 0.0
+        d[n // 8: n // 8 + 8] = np.float32([0, 0, 1])
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    tmax = rng.uniform(1.0, 60.0, n).astype(np.float32)
+    return o, d, tmax
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2], ids=["closest", "any", "shadow"])
+def test_trace_rays_bit_exact(oracle, small_scene, small_ctx, mode):
+    from rkifield_b200 import scenes
+    spec = small_scene["spec"]
+    v = small_scene["vox"]
+    sc = oracle.Scene([small_scene["obj"]], pool_words=v.words, brick_maps=v.map)
+    o, d, tmax = _rays(20000, seed=mode + 1)
+    p = scenes.march_params(spec)
+    ref = oracle.trace(sc, o.ravel(), d.ravel(), tmax, mode, p)
+    got = small_ctx.trace(o, d, tmax, mode, p)
+    assert_bits_equal(got["t"], ref["t"], "t")
+    assert_bits_equal(got["flags"], ref["flags"], "flags")
+    if mode == 0:
+        for k in ("normal", "slot", "material"):
+            assert_bits_equal(got[k], ref[k], k)
+    hits = int((ref["flags"] & 1).sum())
+    assert 100 < hits < 20000
+
+
+def test_trace_zero_rays(small_ctx):
+    from rkifield_b200 import scenes
+    out = small_ctx.trace(np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32),
+                          np.zeros(0, np.float32), 0, scenes.march_params(scenes.SCENE_SMALL))
+    assert out["t"].size == 0
+
+
+def test_query_points_bit_exact(oracle, small_scene, small_ctx):
+    v = small_scene["vox"]
+    sc = oracle.Scene([small_scene["obj"]], pool_words=v.words, brick_maps=v.map)
+    rng = np.random.default_rng(9)
+    pts = rng.uniform(-20, 20, (50000, 3)).astype(np.float32)
+    # also points right on the band around surfaces: march hits
+    d_ref, g_ref, m_ref = oracle.query_points(sc, pts.ravel())
+    d, g, m = small_ctx.query_points(pts)
+    assert_bits_equal(d, d_ref, "distance")
+    assert_bits_equal(g, g_ref, "gradient")
+    assert_bits_equal(m, m_ref, "material")
+    assert (np.abs(d) < 0.5).sum() > 10
+
+
+def test_batch_equals_separate_calls(small_scene, small_ctx):
+    """Several uneven views and ray batches in one persistent launch give the
+    same bits as separate calls."""
+    import ctypes as C
+
+    from rkifield_b200 import _abi as abi
+    from rkifield_b200 import cudart, scenes
+    spec = small_scene["spec"]
+    p = scenes.march_params(spec)
+    sizes = [(128, 72), (31, 200), (256, 256)]
+    views = (abi.rkf_view * len(sizes))()
+    gb = []
+    refs = []
+    for i, (w, h) in enumerate(sizes):
+        cam = scenes.seeded_camera(spec, w, h, seed=60 + i)
+        refs.append(small_ctx.march(cam, p, w, h))
+        g = cudart.device_gbuffer(w * h)
+        gb.append(g)
+        views[i].camera = cam
+        views[i].width, views[i].height = w, h
+        for k, a in g.items():
+            setattr(views[i].out, k, a.ptr)
+        views[i].out.mem = abi.RKF_MEM_DEVICE
+    o, d, tmax = _rays(5000, seed=77)
+    ray_ref = [small_ctx.trace(o, d, tmax, m, p) for m in (0, 2)]
+    ins = [cudart.DeviceArray(o.size, np.float32).upload(o.ravel()),
+           cudart.DeviceArray(d.size, np.float32).upload(d.ravel()),
+           cudart.DeviceArray(tmax.size, np.float32).upload(tmax)]
+    batches = (abi.rkf_ray_batch * 2)()
+    hb = []
+    for j, m in enumerate((0, 2)):
+        h = {"t": cudart.DeviceArray(5000, np.float32), "flags": cudart.DeviceArray(5000, np.uint16)}
+        if m == 0:
+            h.update(normal=cudart.DeviceArray(15000, np.float32), slot=cudart.DeviceArray(5000, np.uint32),
+                     material=cudart.DeviceArray(5000, np.uint16))
+        hb.append(h)
+        batches[j].origins, batches[j].dirs, batches[j].tmax = ins[0].ptr, ins[1].ptr, ins[2].ptr
+        batches[j].n, batches[j].mode = 5000, m
+        for k, a in h.items():
+            setattr(batches[j].out, k, a.ptr)
+        batches[j].out.mem = abi.RKF_MEM_DEVICE
+    for tu in (None, (16, 2, 0, 4, 0, 128), (4, 8, 0, 64, 1, 256)):
+        tuning = None
+        if tu is not None:
+            tuning = abi.rkf_batch_tuning(*tu)
+        abi.check(small_ctx.lib.rkf_march_batch(small_ctx.h, views, len(sizes), batches, 2, C.byref(p),
+                                                None if tuning is None else C.byref(tuning)), "batch")
+        for g, r in zip(gb, refs):
+            for k in r:
+                assert_bits_equal(g[k].download(), r[k], f"view {k} tuning {tu}")
+        for h, r in zip(hb, ray_ref):
+            for k in h:
+                assert_bits_equal(h[k].download(), r[k], f"rays {k} tuning {tu}")
