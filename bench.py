@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-sectors", action="store_true")
+    ap.add_argument("--cb-views", type=int, default=64, help="views in the batching workload (0 = skip)")
+    ap.add_argument("--cb-steps", type=int, default=3)
     return ap.parse_args()
 
 
@@ -243,6 +245,120 @@ def run_reference(args, world, rank, dist):
     }), flush=True)
 
 
+def build_batching(ctx, spec, prims, p, n_views, seed):
+    """Views of uneven size plus their shadow / AO ray batches, on the device."""
+    import ctypes as C
+
+    from rkifield_b200 import cudart, workloads
+    views = workloads.make_views(spec, prims, n_views, seed)
+    vs = (abi.rkf_view * len(views))()
+    keep = []
+    n_primary = 0
+    for i, v in enumerate(views):
+        g = cudart.device_gbuffer(v.width * v.height)
+        keep.append(g)
+        vs[i].camera = v.cam
+        vs[i].width, vs[i].height = v.width, v.height
+        for k, a in g.items():
+            setattr(vs[i].out, k, a.ptr)
+        vs[i].out.mem = abi.RKF_MEM_DEVICE
+        n_primary += v.width * v.height
+    abi.check(ctx.lib.rkf_march_batch(ctx.h, vs, len(views), None, 0, C.byref(p), None), "batch primaries")
+    rng = np.random.default_rng(seed + 1)
+    batches = (abi.rkf_ray_batch * (2 * len(views)))()
+    n_live = 0
+    n_slots = 0
+    for i, v in enumerate(views):
+        npx = v.width * v.height
+        g = keep[i]
+        target = np.array(v.cam.position[:3], np.float64) + 8.0 * np.array(v.cam.forward[:3], np.float64)
+        lights = (target[None] + rng.uniform(-10, 10, (4, 3)) + np.array([0.0, 8.0, 0.0])).astype(np.float32)
+        arrs = [cudart.DeviceArray(3 * 4 * npx, np.float32), cudart.DeviceArray(3 * 4 * npx, np.float32),
+                cudart.DeviceArray(4 * npx, np.float32), cudart.DeviceArray(3 * 8 * npx, np.float32),
+                cudart.DeviceArray(3 * 8 * npx, np.float32), cudart.DeviceArray(8 * npx, np.float32)]
+        keep.append(arrs)
+        hits = C.c_uint32()
+        gbs = abi.rkf_gbuffer()
+        gbs.t, gbs.normal, gbs.flags, gbs.mem = g["t"].ptr, g["normal"].ptr, g["flags"].ptr, abi.RKF_MEM_DEVICE
+        abi.check(ctx.lib.rkf_secondary_rays(ctx.h, C.byref(v.cam), v.width, v.height, C.byref(gbs),
+                                             lights.ctypes.data, 4, 8, 1.0, seed * 1000 + i,
+                                             *[a.ptr for a in arrs], C.byref(hits), None), "secondary rays")
+        n_live += hits.value * 12
+        for j, (o, d, t, nper, mode) in enumerate(((arrs[0], arrs[1], arrs[2], 4, abi.RKF_TRACE_SHADOW),
+                                                   (arrs[3], arrs[4], arrs[5], 8, abi.RKF_TRACE_ANY))):
+            out = {"t": cudart.DeviceArray(nper * npx, np.float32), "flags": cudart.DeviceArray(nper * npx, np.uint16)}
+            keep.append(out)
+            b = batches[2 * i + j]
+            b.origins, b.dirs, b.tmax, b.n, b.mode = o.ptr, d.ptr, t.ptr, nper * npx, mode
+            b.out.t, b.out.flags, b.out.mem = out["t"].ptr, out["flags"].ptr, abi.RKF_MEM_DEVICE
+            n_slots += nper * npx
+    return {"views": views, "vs": vs, "batches": batches, "keep": keep, "n_primary": n_primary,
+            "n_secondary_live": n_live, "n_secondary_slots": n_slots}
+
+
+def run_batching(ctx, spec, prims, p, args, stream):
+    import ctypes as C
+
+    from rkifield_b200 import cudart
+    wl = build_batching(ctx, spec, prims, p, args.cb_views, seed=300)
+    nv = len(wl["views"])
+    vs, bs = wl["vs"], wl["batches"]
+    # autotune on a sample: the first quarter of the views and their secondaries
+    ns = max(1, nv // 4)
+    tu = abi.rkf_batch_tuning()
+    t0 = time.perf_counter()
+    abi.check(ctx.lib.rkf_autotune(ctx.h, vs, ns, bs, 2 * ns, C.byref(p), C.byref(tu)), "autotune")
+    tune_s = time.perf_counter() - t0
+
+    def timed(fn, steps):
+        fn()
+        stream.synchronize()
+        ms = []
+        for _ in range(steps):
+            a, b = cudart.Event(), cudart.Event()
+            a.record(stream)
+            fn()
+            b.record(stream)
+            stream.synchronize()
+            ms.append(a.elapsed_ms(b))
+        return ms
+
+    def batched():
+        abi.check(ctx.lib.rkf_march_batch_async(ctx.h, vs, nv, bs, 2 * nv, C.byref(p), None, stream.ptr), "batch")
+
+    def per_request(plain):
+        for i in range(nv):
+            v = vs[i]
+            fn = ctx.lib.rkf_march_plain_async if plain else ctx.lib.rkf_march_async
+            abi.check(fn(ctx.h, C.byref(v.camera), C.byref(p), v.width, v.height, C.byref(v.out), stream.ptr),
+                      "view")
+        for j in range(2 * nv):
+            b = bs[j]
+            if plain:
+                abi.check(ctx.lib.rkf_trace_rays_plain_async(ctx.h, b.origins, b.dirs, b.tmax, b.n, b.mode,
+                                                             C.byref(p), C.byref(b.out), stream.ptr), "rays")
+            else:
+                abi.check(ctx.lib.rkf_march_batch_async(ctx.h, None, 0, C.byref(b), 1, C.byref(p), None,
+                                                        stream.ptr), "rays")
+
+    steps = args.cb_steps
+    mb = timed(batched, steps)
+    mp = timed(lambda: per_request(True), max(1, steps - 1))
+    mf = timed(lambda: per_request(False), max(1, steps - 1))
+    rays = wl["n_primary"] + wl["n_secondary_live"]
+    val = lambda ms: rays / (np.mean(ms) / 1e3) / 1e6  # noqa: E731
+    return {"views": nv, "primary_rays": wl["n_primary"], "secondary_rays_live": wl["n_secondary_live"],
+            "secondary_ray_slots": wl["n_secondary_slots"],
+            "tuning": {"tile": [tu.tile_w, tu.tile_h], "compact_interval": tu.compact_interval,
+                       "threads_per_block": tu.threads_per_block, "tune_s": tune_s},
+            "batched": {"value": val(mb), "unit": "Mrays/s", "ms": float(np.mean(mb)), "launches": 1},
+            "plain_per_request": {"value": val(mp), "unit": "Mrays/s", "ms": float(np.mean(mp)),
+                                  "launches": 3 * nv},
+            "b200_per_request": {"value": val(mf), "unit": "Mrays/s", "ms": float(np.mean(mf)),
+                                 "launches": 3 * nv},
+            "vs_plain": val(mb) / val(mp)}
+
+
 def run_b200(args, world, rank, local, dist):
     from rkifield_b200 import cudart
     from rkifield_b200.engine import Context, gbuffer_host
@@ -317,6 +433,10 @@ def run_b200(args, world, rank, local, dist):
     d2h = sum(v.nbytes for v in host_out.values())
     h2d = 144 + 32  # camera uniforms + march parameters
 
+    batching = None
+    if args.cb_views > 0:
+        batching = run_batching(ctx, spec, prims, p, args, stream)
+
     out = None
     if rank == 0:
         hits = int((host_out["flags"] & 1).sum())
@@ -368,6 +488,7 @@ def run_b200(args, world, rank, local, dist):
             "vs_plain": (value / plain["value"]) if plain else None,
             "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roof,
+            "batching": batching,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": args.steps,

@@ -333,6 +333,23 @@ RKF_API rkf_status rkf_trace_rays(rkf_ctx* ctx, const float* origins, const floa
                           const float* tmax, uint32_t n, uint32_t mode,
                           const rkf_march_params* p, uint32_t in_mem, rkf_hits* out);
 
+/* Shadow and ambient-occlusion rays for the hit pixels of a view, as the
+ * reference's shading pass queries them (shade_common_shading.wgsl:9-47):
+ * per pixel n_lights (<= 16) soft-shadow rays towards the point lights
+ * (origin = hit + normal*0.08, tmax = distance to the light) and ao_per_hit
+ * cosine-weighted hemisphere any-hit rays (origin = hit + normal*0.02,
+ * tmax = ao_radius).  Pixel p owns ray slots [p*n, p*n+n); pixels that missed
+ * get tmax = -1 (the ray ends on its first iteration).  gb: the view's device
+ * G-buffer; lights: host, 3 floats each; outputs: device arrays sized for
+ * w*h*n_lights / w*h*ao_per_hit rays.  *hit_pixels (host) receives the
+ * number of hit pixels.  Waits for completion. */
+RKF_API rkf_status rkf_secondary_rays(rkf_ctx* ctx, const rkf_camera* cam, uint32_t w, uint32_t h,
+                                      const rkf_gbuffer* gb, const float* lights,
+                                      uint32_t n_lights, uint32_t ao_per_hit, float ao_radius,
+                                      uint32_t seed, float* shadow_o, float* shadow_d,
+                                      float* shadow_tmax, float* ao_o, float* ao_d,
+                                      float* ao_tmax, uint32_t* hit_pixels, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Point queries: SdfQueryable::{evaluate, gradient}                         */
 /* (crates/rkf-physics/src/sdf_collision.rs:38-56)                          */
@@ -398,6 +415,23 @@ typedef struct rkf_batch_tuning {
 RKF_API rkf_status rkf_march_batch(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views,
                            const rkf_ray_batch* batches, uint32_t n_batches,
                            const rkf_march_params* p, const rkf_batch_tuning* tuning);
+
+/* rkf_march_batch enqueued on a caller stream (cudaStream_t, NULL = context
+ * stream) without waiting.  Shares the context's launch scratch with the
+ * other context launches: issue them on one stream or synchronise. */
+RKF_API rkf_status rkf_march_batch_async(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views,
+                                         const rkf_ray_batch* batches, uint32_t n_batches,
+                                         const rkf_march_params* p,
+                                         const rkf_batch_tuning* tuning, void* stream);
+
+/* Plain ray casts: one launch per request, one thread per ray, reference
+ * AoS pool and flat maps, the reference loop (ray_march.wgsl:776-858,
+ * shade_common_shading.wgsl:9-33).  The per-request baseline of the
+ * batched path.  Device pointers; enqueued on `stream` without waiting. */
+RKF_API rkf_status rkf_trace_rays_plain_async(rkf_ctx* ctx, const float* origins,
+                                              const float* dirs, const float* tmax, uint32_t n,
+                                              uint32_t mode, const rkf_march_params* p,
+                                              const rkf_hits* out, void* stream);
 
 /* rkf_march_batch for callers that cannot allocate device memory when they
  * call: callers on a fixed per-frame time budget (cudaMalloc synchronises

@@ -197,10 +197,16 @@ SIGNATURES = {
                                    _U32, C.POINTER(rkf_gbuffer), _P]),
     "rkf_trace_rays": (_I, [_P, _P, _P, _P, _U32, _U32, C.POINTER(rkf_march_params), _U32,
                             C.POINTER(rkf_hits)]),
+    "rkf_secondary_rays": (_I, [_P, C.POINTER(rkf_camera), _U32, _U32, C.POINTER(rkf_gbuffer), _P, _U32,
+                                _U32, C.c_float, _U32, _P, _P, _P, _P, _P, _P, C.POINTER(_U32), _P]),
     "rkf_query_points": (_I, [_P, _P, _U32, _P, _P, _P, _U32]),
     "rkf_edit_csg": (_I, [_P, C.POINTER(rkf_edit_op), C.POINTER(_U64)]),
     "rkf_march_batch": (_I, [_P, C.POINTER(rkf_view), _U32, C.POINTER(rkf_ray_batch), _U32,
                              C.POINTER(rkf_march_params), C.POINTER(rkf_batch_tuning)]),
+    "rkf_march_batch_async": (_I, [_P, C.POINTER(rkf_view), _U32, C.POINTER(rkf_ray_batch), _U32,
+                                   C.POINTER(rkf_march_params), C.POINTER(rkf_batch_tuning), _P]),
+    "rkf_trace_rays_plain_async": (_I, [_P, _P, _P, _P, _U32, _U32, C.POINTER(rkf_march_params),
+                                        C.POINTER(rkf_hits), _P]),
     "rkf_march_batch_noalloc": (_I, [_P, C.POINTER(rkf_view), _U32, C.POINTER(rkf_ray_batch), _U32,
                                      C.POINTER(rkf_march_params), C.POINTER(rkf_batch_tuning), _P]),
     "rkf_autotune": (_I, [_P, C.POINTER(rkf_view), _U32, C.POINTER(rkf_ray_batch), _U32,

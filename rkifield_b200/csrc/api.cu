@@ -259,10 +259,36 @@ rkf_status rkf_query_points(rkf_ctx* ctx, const float* points, uint32_t n, float
 rkf_status rkf_march_batch(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views,
                            const rkf_ray_batch* batches, uint32_t n_batches,
                            const rkf_march_params* p, const rkf_batch_tuning* tuning) {
+  rkf_status st = rkf_march_batch_async(ctx, views, n_views, batches, n_batches, p, tuning, nullptr);
+  if (st != RKF_OK) return st;
+  RKF_CUDA_TRY(cudaStreamSynchronize(reinterpret_cast<Ctx*>(ctx)->stream));
+  return RKF_OK;
+}
+
+rkf_status rkf_trace_rays_plain_async(rkf_ctx* ctx, const float* origins, const float* dirs,
+                                      const float* tmax, uint32_t n, uint32_t mode,
+                                      const rkf_march_params* p, const rkf_hits* out, void* stream) {
+  rkf_status st = check_common(ctx, p, p, "rkf_trace_rays_plain_async");
+  if (st != RKF_OK) return st;
+  if (!out || !out->t || (n && (!origins || !dirs || !tmax)))
+    return fail(RKF_INVALID_ARG, "rkf_trace_rays_plain_async: null argument");
+  if (mode > RKF_TRACE_SHADOW || out->mem != RKF_MEM_DEVICE)
+    return fail(RKF_INVALID_ARG, "rkf_trace_rays_plain_async: bad mode or host outputs");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  return launch_trace_plain(c, origins, dirs, tmax, n, mode, p, *out,
+                            stream ? static_cast<cudaStream_t>(stream) : c->stream);
+}
+
+rkf_status rkf_march_batch_async(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views,
+                                 const rkf_ray_batch* batches, uint32_t n_batches,
+                                 const rkf_march_params* p, const rkf_batch_tuning* tuning,
+                                 void* stream) {
   if (!ctx || !p || (n_views && !views) || (n_batches && !batches))
     return fail(RKF_INVALID_ARG, "rkf_march_batch: null argument");
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   RKF_CUDA_TRY(cudaSetDevice(c->device));
+  const cudaStream_t strm = stream ? static_cast<cudaStream_t>(stream) : c->stream;
   const rkf_batch_tuning tu = tuning ? *tuning : c->tuning;
   if (tu.tile_w == 0 || tu.tile_h == 0 || tu.tile_w * tu.tile_h > 4096)
     return fail(RKF_INVALID_ARG, "rkf_march_batch: bad tile shape");
@@ -290,11 +316,7 @@ rkf_status rkf_march_batch(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views
     segs.push_back(sg);
   }
   if (segs.empty()) return RKF_OK;
-  rkf_status st = launch_persistent(c, segs, first, p, tu, c->stream, &c->seg_buf,
-                                    c->counters.as<unsigned long long>());
-  if (st != RKF_OK) return st;
-  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  return RKF_OK;
+  return launch_persistent(c, segs, first, p, tu, strm, &c->seg_buf, c->counters.as<unsigned long long>());
 }
 
 }  // extern "C"

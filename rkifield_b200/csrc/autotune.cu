@@ -1,0 +1,73 @@
+// autotune.cu — pick the persistent march's launch tuning for a workload.
+//
+// The batched march has three knobs that change speed but never results:
+// the ray-tile shape that orders a view's work ids (the spatial coherence of
+// the rays a warp holds), the compaction interval (march iterations between
+// lane refills) and the block size / blocks per SM.  rkf_autotune times every
+// candidate on the caller's sample of the work with CUDA events and keeps
+// the fastest in the context, where rkf_march and rkf_march_batch use it.
+#include <cfloat>
+#include <cstring>
+#include <vector>
+
+#include "ctx.h"
+#include "march.h"
+
+using namespace rkf;
+
+extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views,
+                                   const rkf_ray_batch* batches, uint32_t n_batches,
+                                   const rkf_march_params* p, rkf_batch_tuning* out) {
+  if (!ctx || !p || (n_views && !views) || (n_batches && !batches))
+    return fail(RKF_INVALID_ARG, "rkf_autotune: null argument");
+  if (n_views + n_batches == 0) return fail(RKF_INVALID_ARG, "rkf_autotune: no work to tune on");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  static const uint32_t tiles[][2] = {{8, 4}, {4, 8}, {16, 2}, {32, 1}, {16, 4}, {8, 8}};
+  static const uint32_t intervals[] = {4, 8, 16, 32, 64};
+  static const uint32_t threads[] = {128, 256};
+  cudaEvent_t e0, e1;
+  RKF_CUDA_TRY(cudaEventCreate(&e0));
+  RKF_CUDA_TRY(cudaEventCreate(&e1));
+  rkf_batch_tuning best = c->tuning;
+  float best_ms = FLT_MAX;
+  rkf_status st = RKF_OK;
+  for (const auto& tl : tiles) {
+    for (uint32_t iv : intervals) {
+      for (uint32_t th : threads) {
+        rkf_batch_tuning tu{tl[0], tl[1], 0, iv, 0, th};
+        // one untimed launch, then the best of two timed ones
+        st = rkf_march_batch_async(ctx, views, n_views, batches, n_batches, p, &tu, nullptr);
+        if (st != RKF_OK) break;
+        float ms = FLT_MAX;
+        for (int r = 0; r < 2; ++r) {
+          cudaEventRecord(e0, c->stream);
+          st = rkf_march_batch_async(ctx, views, n_views, batches, n_batches, p, &tu, nullptr);
+          if (st != RKF_OK) break;
+          cudaEventRecord(e1, c->stream);
+          if (cudaEventSynchronize(e1) != cudaSuccess) {
+            st = fail(RKF_CUDA_ERROR, "rkf_autotune: launch failed");
+            break;
+          }
+          float m = 0.0f;
+          cudaEventElapsedTime(&m, e0, e1);
+          if (m < ms) ms = m;
+        }
+        if (st != RKF_OK) break;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = tu;
+        }
+      }
+      if (st != RKF_OK) break;
+    }
+    if (st != RKF_OK) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != RKF_OK) return st;
+  c->tuning = best;
+  c->tuned = true;
+  if (out) *out = best;
+  return RKF_OK;
+}

@@ -43,6 +43,9 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs, uint64_t 
 rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t nseg, uint64_t total,
                                      const rkf_march_params* p, const rkf_batch_tuning& tu,
                                      cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter);
+rkf_status launch_trace_plain(Ctx* c, const float* o, const float* d, const float* tmax, uint32_t n,
+                              uint32_t mode, const rkf_march_params* p, const rkf_hits& out,
+                              cudaStream_t st);
 rkf_status launch_query(Ctx* c, const float* pts, uint32_t n, float* d, float* g, uint16_t* m,
                         cudaStream_t st);
 

@@ -35,6 +35,14 @@ enum : uint32_t { ST_IDLE = 0, ST_MARCH, ST_BISECT, ST_NORMAL, ST_EPI, ST_SHADOW
 
 constexpr uint32_t kFull = 0xFFFFFFFFu;
 
+// Per-lane ray state that is read or written only when a ray starts, hits
+// or ends.
+struct ColdState {
+  uint32_t seg, idx, hit_obj, sub;
+  float lo, hi, mat_t, gpos, shadow;
+  bool hit, bisected, mat_ok;
+};
+
 struct KParams {
   ObjDev objs[kMaxObjectsFast];  // object table in the constant parameter bank
   SceneDev s;
@@ -82,7 +90,7 @@ __device__ __forceinline__ float eval_min(const SceneDev& s, const ObjDev* objs,
 }
 
 template <int PREC, bool SINGLE>
-__global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_constant__ KParams kp) {
+__global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_constant__ KParams kp) {
   const ObjDev* sh_objs = kp.objs;
   const SceneDev& s = kp.s;
   const rkf_march_params& p = kp.p;
@@ -92,12 +100,14 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
 
   LaneCache lc;
   uint32_t state = ST_IDLE;
-  uint32_t seg = 0, idx = 0, mode = RKF_TRACE_CLOSEST;
+  uint32_t mode = RKF_TRACE_CLOSEST;
+  // state a lane touches only when a ray starts, hits or ends lives in shared
+  // memory, which keeps the march loop's register footprint small
+  __shared__ ColdState cold_all[256];
+  ColdState& cs = cold_all[threadIdx.x];
   float ox = 0, oy = 0, oz = 0, rdx = 0, rdy = 0, rdz = 0;
   float t = 0, prev_t = 0, prev_dist = kMaxFloat, tmax = 0;
-  uint32_t near = 0, step = 0, sub = 0, hit_obj = 0;
-  float lo = 0, hi = 0, mat_t = 0, shadow = 1.0f, gpos = 0;
-  bool mat_ok = false, bisected = false, hit = false;
+  uint32_t near = 0, step = 0;
   bool exhausted = false;
 
   for (;;) {
@@ -114,8 +124,8 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
         if (idle) {
           const uint64_t id = base + __popc(need & ((1u << lane) - 1u));
           if (id < kp.total) {
-            seg = find_segment(kp.segs, kp.nseg, id);
-            const Segment& sg = kp.segs[seg];
+            cs.seg = find_segment(kp.segs, kp.nseg, id);
+            const Segment& sg = kp.segs[cs.seg];
             const uint64_t local = id - sg.first;
             bool valid = true;
             if (sg.kind == 0) {  // view: tile-ordered pixel ids
@@ -126,7 +136,7 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
               const uint32_t py = (tile / sg.tiles_x) * kp.tile_h + r / kp.tile_w;
               valid = px < sg.w && py < sg.h;
               if (valid) {
-                idx = py * sg.w + px;
+                cs.idx = py * sg.w + px;
                 // ray generation (ray_march.wgsl:1046-1053)
                 const float u = __fdiv_rn(__fadd_rn(__fadd_rn(static_cast<float>(px), 0.5f), sg.jitter[0]),
                                           static_cast<float>(sg.w));
@@ -148,24 +158,24 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
                 mode = RKF_TRACE_CLOSEST;
               }
             } else {
-              idx = static_cast<uint32_t>(local);
-              const size_t i3 = 3 * static_cast<size_t>(idx);
+              cs.idx = static_cast<uint32_t>(local);
+              const size_t i3 = 3 * static_cast<size_t>(cs.idx);
               ox = __ldg(sg.origins + i3);
               oy = __ldg(sg.origins + i3 + 1);
               oz = __ldg(sg.origins + i3 + 2);
               rdx = __ldg(sg.dirs + i3);
               rdy = __ldg(sg.dirs + i3 + 1);
               rdz = __ldg(sg.dirs + i3 + 2);
-              tmax = __ldg(sg.tmax + idx);
+              tmax = __ldg(sg.tmax + cs.idx);
               mode = sg.mode;
             }
             if (valid) {
               near = 0;
               step = 0;
-              hit = bisected = mat_ok = false;
+              cs.hit = cs.bisected = cs.mat_ok = false;
               if (mode == RKF_TRACE_SHADOW) {
                 t = 0.005f;  // SHADOW_EPSILON (shade_common.wgsl:274)
-                shadow = 1.0f;
+                cs.shadow = 1.0f;
                 state = ST_SHADOW;
               } else {
                 t = 0.0f;
@@ -182,7 +192,7 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
         continue;
       }
     }
-    // the march steps along the safe direction (ray_march.wgsl:784); hit
+    // the march steps along the safe direction (ray_march.wgsl:784); cs.hit
     // positions use the raw direction (:1068)
     const float qdx = fabsf(rdx) < 1e-10f ? 1e-10f : rdx;
     const float qdy = fabsf(rdy) < 1e-10f ? 1e-10f : rdy;
@@ -193,7 +203,7 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
     for (uint32_t k = 0; k < kp.interval; ++k) {
       if (state == ST_MARCH) {
         if (step >= p.hard_max_steps || t > tmax || near >= p.scene.max_steps) {
-          hit = false;
+          cs.hit = false;
           state = ST_EPI;
         } else {
           float best_un;
@@ -202,29 +212,29 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
                                                     __fadd_rn(oy, __fmul_rn(qdy, t)),
                                                     __fadd_rn(oz, __fmul_rn(qdz, t)), best_un, best_i, lc);
           if (best < 0.0f && prev_dist > hit_thr) {  // overstep (ray_march.wgsl:816)
-            hit_obj = best_i;
-            hit = true;
+            cs.hit_obj = best_i;
+            cs.hit = true;
             if (mode == RKF_TRACE_ANY) {
               state = ST_EPI;
             } else {
-              lo = prev_t;
-              hi = t;
-              mat_t = t;
-              mat_ok = best_un < sh_objs[best_i].vs16;
-              sub = 0;
-              bisected = true;
+              cs.lo = prev_t;
+              cs.hi = t;
+              cs.mat_t = t;
+              cs.mat_ok = best_un < sh_objs[best_i].vs16;
+              cs.sub = 0;
+              cs.bisected = true;
               state = ST_BISECT;
             }
           } else if (best < hit_thr) {  // :842
-            hit_obj = best_i;
-            hit = true;
+            cs.hit_obj = best_i;
+            cs.hit = true;
             if (mode == RKF_TRACE_ANY) {
               state = ST_EPI;
             } else {
-              // a direct hit: enter the finish phase with the bisection done
-              mat_t = t;
-              mat_ok = best_un < sh_objs[best_i].vs16;
-              sub = p.bisect_steps;
+              // a direct cs.hit: enter the finish phase with the bisection done
+              cs.mat_t = t;
+              cs.mat_ok = best_un < sh_objs[best_i].vs16;
+              cs.sub = p.bisect_steps;
               state = ST_BISECT;
             }
           } else {
@@ -238,8 +248,8 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
       } else if (state == ST_SHADOW) {
         // soft_shadow (shade_common_shading.wgsl:9-33)
         if (step >= 256u || near >= 32u || t > tmax) {
-          shadow = clampf(shadow, 0.0f, 1.0f);
-          hit = false;
+          cs.shadow = clampf(cs.shadow, 0.0f, 1.0f);
+          cs.hit = false;
           state = ST_EPI;
         } else {
           float best_un;
@@ -248,12 +258,12 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
                                                     __fadd_rn(oy, __fmul_rn(rdy, t)),
                                                     __fadd_rn(oz, __fmul_rn(rdz, t)), best_un, best_i, lc);
           if (best < 0.005f) {
-            shadow = 0.0f;
-            hit = true;
+            cs.shadow = 0.0f;
+            cs.hit = true;
             state = ST_EPI;
           } else {
             if (best < 0.02f) {
-              shadow = fmin_(shadow, __fdiv_rn(__fmul_rn(16.0f, best), t));
+              cs.shadow = fmin_(cs.shadow, __fdiv_rn(__fmul_rn(16.0f, best), t));
               near++;
             }
             t = __fadd_rn(t, fmax_(best, 0.005f));
@@ -267,10 +277,10 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
     // ---- 3. finish: bisection and central differences -------------------------
     float g0 = 0, g1 = 0, g2 = 0, lpx = 0, lpy = 0, lpz = 0, eps = 0;
     while (__any_sync(kFull, state == ST_BISECT || state == ST_NORMAL)) {
-      if (state == ST_BISECT && sub >= p.bisect_steps) {
-        // bisection done (or a direct hit): t = (lo+hi)/2, set up the normal
-        if (bisected) t = __fmul_rn(__fadd_rn(lo, hi), 0.5f);
-        const ObjDev& o = sh_objs[hit_obj];
+      if (state == ST_BISECT && cs.sub >= p.bisect_steps) {
+        // bisection done (or a direct cs.hit): t = (cs.lo+cs.hi)/2, set up the normal
+        if (cs.bisected) t = __fmul_rn(__fadd_rn(cs.lo, cs.hi), 0.5f);
+        const ObjDev& o = sh_objs[cs.hit_obj];
         const float hx = __fadd_rn(ox, __fmul_rn(rdx, t));
         const float hy = __fadd_rn(oy, __fmul_rn(rdy, t));
         const float hz = __fadd_rn(oz, __fmul_rn(rdz, t));
@@ -283,30 +293,30 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
           lpz = hz;
           eps = __fmul_rn(hit_thr, 10.0f);
         }
-        sub = 0;
+        cs.sub = 0;
         state = ST_NORMAL;
       }
       if (state == ST_BISECT) {
-        const float mid = __fmul_rn(__fadd_rn(lo, hi), 0.5f);
+        const float mid = __fmul_rn(__fadd_rn(cs.lo, cs.hi), 0.5f);
         float du;
-        const float d = eval_obj<PREC>(s, sh_objs[hit_obj], __fadd_rn(ox, __fmul_rn(qdx, mid)),
+        const float d = eval_obj<PREC>(s, sh_objs[cs.hit_obj], __fadd_rn(ox, __fmul_rn(qdx, mid)),
                                        __fadd_rn(oy, __fmul_rn(qdy, mid)), __fadd_rn(oz, __fmul_rn(qdz, mid)),
                                        &du, lc);
         if (d < 0.0f) {
-          hi = mid;
+          cs.hi = mid;
         } else {
-          lo = mid;
-          mat_t = mid;
-          mat_ok = du < sh_objs[hit_obj].vs16;
+          cs.lo = mid;
+          cs.mat_t = mid;
+          cs.mat_ok = du < sh_objs[cs.hit_obj].vs16;
         }
-        ++sub;
+        ++cs.sub;
       } else if (state == ST_NORMAL) {
-        const ObjDev& o = sh_objs[hit_obj];
-        const uint32_t ax = sub >> 1;
+        const ObjDev& o = sh_objs[cs.hit_obj];
+        const uint32_t ax = cs.sub >> 1;
         float qx = lpx, qy = lpy, qz = lpz;
-        if (ax == 0) qx = (sub & 1) ? __fsub_rn(lpx, eps) : __fadd_rn(lpx, eps);
-        if (ax == 1) qy = (sub & 1) ? __fsub_rn(lpy, eps) : __fadd_rn(lpy, eps);
-        if (ax == 2) qz = (sub & 1) ? __fsub_rn(lpz, eps) : __fadd_rn(lpz, eps);
+        if (ax == 0) qx = (cs.sub & 1) ? __fsub_rn(lpx, eps) : __fadd_rn(lpx, eps);
+        if (ax == 1) qy = (cs.sub & 1) ? __fsub_rn(lpy, eps) : __fadd_rn(lpy, eps);
+        if (ax == 2) qz = (cs.sub & 1) ? __fsub_rn(lpz, eps) : __fadd_rn(lpz, eps);
         float d;
         if (o.sdf_type == RKF_SDF_VOXELIZED) {
           d = sample_vox<PREC>(s, o, qx, qy, qz, true, lc);
@@ -314,38 +324,38 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
           float du;
           d = eval_obj<PREC>(s, o, qx, qy, qz, &du, lc);
         }
-        if (sub & 1) {
-          const float g = __fsub_rn(gpos, d);
+        if (cs.sub & 1) {
+          const float g = __fsub_rn(cs.gpos, d);
           if (ax == 0) g0 = g;
           else if (ax == 1) g1 = g;
           else g2 = g;
         } else {
-          gpos = d;
+          cs.gpos = d;
         }
-        if (++sub == 6) state = ST_EPI;
+        if (++cs.sub == 6) state = ST_EPI;
       }
     }
 
     // ---- 4. epilogue: outputs of finished rays -------------------------------
     if (state == ST_EPI) {
-      const Segment& sg = kp.segs[seg];
+      const Segment& sg = kp.segs[cs.seg];
       if (mode == RKF_TRACE_SHADOW) {
-        sg.t[idx] = shadow;
-        if (sg.flags) sg.flags[idx] = hit ? RKF_FLAG_HIT : 0;
+        sg.t[cs.idx] = cs.shadow;
+        if (sg.flags) sg.flags[cs.idx] = cs.hit ? RKF_FLAG_HIT : 0;
       } else if (mode == RKF_TRACE_ANY) {
-        sg.t[idx] = hit ? t : kMaxFloat;
+        sg.t[cs.idx] = cs.hit ? t : kMaxFloat;
         if (sg.flags)
-          sg.flags[idx] = hit ? RKF_FLAG_HIT
+          sg.flags[cs.idx] = cs.hit ? RKF_FLAG_HIT
                               : ((step >= p.hard_max_steps || near >= p.scene.max_steps) ? RKF_FLAG_STEPS_OUT : 0);
       } else {
         uint16_t flags = 0;
         float nx = 0, ny = 0, nz = 0;
         uint32_t slot = RKF_EMPTY_SLOT, mat = 0, sec = 0, blend = 0;
         float hx = 0, hy = 0, hz = 0, sdf_hit = 0;
-        if (hit) {
+        if (cs.hit) {
           flags |= RKF_FLAG_HIT;
-          if (bisected) flags |= RKF_FLAG_BISECTED;
-          const ObjDev& o = sh_objs[hit_obj];
+          if (cs.bisected) flags |= RKF_FLAG_BISECTED;
+          const ObjDev& o = sh_objs[cs.hit_obj];
           hx = __fadd_rn(ox, __fmul_rn(rdx, t));
           hy = __fadd_rn(oy, __fmul_rn(rdy, t));
           hz = __fadd_rn(oz, __fmul_rn(rdz, t));
@@ -375,31 +385,31 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
             const float l = len3(g0, g1, g2);
             nx = __fdiv_rn(g0, l); ny = __fdiv_rn(g1, l); nz = __fdiv_rn(g2, l);
           }
-          if (mat_ok || o.sdf_type == RKF_SDF_ANALYTICAL)
-            mat = material_at(s, o, __fadd_rn(ox, __fmul_rn(qdx, mat_t)), __fadd_rn(oy, __fmul_rn(qdy, mat_t)),
-                              __fadd_rn(oz, __fmul_rn(qdz, mat_t)), lc);
+          if (cs.mat_ok || o.sdf_type == RKF_SDF_ANALYTICAL)
+            mat = material_at(s, o, __fadd_rn(ox, __fmul_rn(qdx, cs.mat_t)), __fadd_rn(oy, __fmul_rn(qdy, cs.mat_t)),
+                              __fadd_rn(oz, __fmul_rn(qdz, cs.mat_t)), lc);
         } else if (step >= p.hard_max_steps || near >= p.scene.max_steps) {
           flags |= RKF_FLAG_STEPS_OUT;
         }
-        sg.t[idx] = hit ? t : kMaxFloat;
+        sg.t[cs.idx] = cs.hit ? t : kMaxFloat;
         if (sg.normal) {
-          sg.normal[3 * static_cast<size_t>(idx)] = nx;
-          sg.normal[3 * static_cast<size_t>(idx) + 1] = ny;
-          sg.normal[3 * static_cast<size_t>(idx) + 2] = nz;
+          sg.normal[3 * static_cast<size_t>(cs.idx)] = nx;
+          sg.normal[3 * static_cast<size_t>(cs.idx) + 1] = ny;
+          sg.normal[3 * static_cast<size_t>(cs.idx) + 2] = nz;
         }
-        if (sg.slot) sg.slot[idx] = slot;
-        if (sg.material) sg.material[idx] = static_cast<uint16_t>(mat);
-        if (sg.flags) sg.flags[idx] = flags;
+        if (sg.slot) sg.slot[cs.idx] = slot;
+        if (sg.material) sg.material[cs.idx] = static_cast<uint16_t>(mat);
+        if (sg.flags) sg.flags[cs.idx] = flags;
         if (sg.position) {
-          const float4 pv = hit ? make_float4(hx, hy, hz, t) : make_float4(0.f, 0.f, 0.f, kMaxFloat);
-          reinterpret_cast<float4*>(sg.position)[idx] = pv;
+          const float4 pv = cs.hit ? make_float4(hx, hy, hz, t) : make_float4(0.f, 0.f, 0.f, kMaxFloat);
+          reinterpret_cast<float4*>(sg.position)[cs.idx] = pv;
         }
         if (sg.packed)
-          sg.packed[idx] = hit ? ((mat & 0x3Fu) | (sec << 6) | (blend << 12) | (sh_objs[hit_obj].object_id << 24))
+          sg.packed[cs.idx] = cs.hit ? ((mat & 0x3Fu) | (sec << 6) | (blend << 12) | (sh_objs[cs.hit_obj].object_id << 24))
                                : 0u;
         if (sg.motion) {
           float4 mv = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (hit) {
+          if (cs.hit) {
             const float* m = sg.prev_vp;  // ray_march.wgsl:1094-1105
             const float cx = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[0], hx), __fmul_rn(m[4], hy)),
                                                  __fmul_rn(m[8], hz)), __fmul_rn(m[12], 1.0f));
@@ -412,7 +422,7 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
               const float ndx = __fdiv_rn(cx, cw), ndy = __fdiv_rn(cy, cw);
               const float pu = __fadd_rn(__fmul_rn(ndx, 0.5f), 0.5f);
               const float pv = __fsub_rn(0.5f, __fmul_rn(ndy, 0.5f));
-              const uint32_t px = idx % sg.w, py = idx / sg.w;
+              const uint32_t px = cs.idx % sg.w, py = cs.idx / sg.w;
               const float cu = __fdiv_rn(__fadd_rn(static_cast<float>(px), 0.5f), static_cast<float>(sg.w));
               const float cv = __fdiv_rn(__fadd_rn(static_cast<float>(py), 0.5f), static_cast<float>(sg.h));
               mox = __fsub_rn(cu, pu);
@@ -420,7 +430,7 @@ __global__ void __launch_bounds__(256, 3) k_march_persistent(const __grid_consta
             }
             mv = make_float4(mox, moy, 1.0f, sdf_hit);
           }
-          reinterpret_cast<float4*>(sg.motion)[idx] = mv;
+          reinterpret_cast<float4*>(sg.motion)[cs.idx] = mv;
         }
       }
       state = ST_IDLE;

@@ -5,6 +5,8 @@
 // (brick_maps[offset + bx + by*dx + bz*dx*dy]).  Every step performs the
 // shader's 8 map reads and 8 pool reads and its material lookup.  This is the
 // one-launch-per-request baseline the batched march is measured against.
+#include <cstring>
+
 #include "ctx.h"
 #include "march.h"
 
@@ -281,7 +283,197 @@ __global__ void __launch_bounds__(64) k_march_plain(PlainParams kp) {
   }
 }
 
+struct PlainRays {
+  PlainParams kp;  // scene, parameters (view fields unused)
+  const float* o;
+  const float* d;
+  const float* tmax;
+  uint32_t n, mode;
+};
+
+// One thread per ray: the same reference loop for generic ray casts
+// (closest hit, any hit, soft shadow of shade_common_shading.wgsl:9-33).
+__global__ void __launch_bounds__(128) k_trace_plain(PlainRays r) {
+  extern __shared__ ObjDev objs[];
+  for (uint32_t i = threadIdx.x; i < r.kp.s.n_objs; i += blockDim.x) objs[i] = r.kp.s.objs[i];
+  __syncthreads();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r.n) return;
+  const PlainParams& kp = r.kp;
+  const rkf_march_params& p = kp.p;
+  const float ox = r.o[3 * static_cast<size_t>(i)], oy = r.o[3 * static_cast<size_t>(i) + 1],
+              oz = r.o[3 * static_cast<size_t>(i) + 2];
+  const float dx = r.d[3 * static_cast<size_t>(i)], dy = r.d[3 * static_cast<size_t>(i) + 1],
+              dz = r.d[3 * static_cast<size_t>(i) + 2];
+  const float tmax = r.tmax[i];
+  if (r.mode == RKF_TRACE_SHADOW) {
+    float shadow = 1.0f, t = 0.005f;
+    uint32_t near = 0, it = 0;
+    bool occluded = false;
+    for (; it < 256u; ++it) {
+      if (near >= 32u || t > tmax) break;
+      const float qx = __fadd_rn(ox, __fmul_rn(dx, t)), qy = __fadd_rn(oy, __fmul_rn(dy, t)),
+                  qz = __fadd_rn(oz, __fmul_rn(dz, t));
+      float d = kMaxFloat;
+      for (uint32_t k = 0; k < kp.s.n_objs; ++k) {
+        uint32_t m;
+        d = fmin_(d, plain_eval(kp, objs[k], qx, qy, qz, &m));
+      }
+      if (d < 0.005f) {
+        occluded = true;
+        break;
+      }
+      if (d < 0.02f) {
+        shadow = fmin_(shadow, __fdiv_rn(__fmul_rn(16.0f, d), t));
+        near++;
+      }
+      t = __fadd_rn(t, fmax_(d, 0.005f));
+    }
+    kp.t[i] = occluded ? 0.0f : clampf(shadow, 0.0f, 1.0f);
+    if (kp.flags) kp.flags[i] = occluded ? RKF_FLAG_HIT : 0;
+    return;
+  }
+  const float sx = fabsf(dx) < 1e-10f ? 1e-10f : dx, sy = fabsf(dy) < 1e-10f ? 1e-10f : dy,
+              sz = fabsf(dz) < 1e-10f ? 1e-10f : dz;
+  float t = 0.0f, prev_t = 0.0f, prev_dist = kMaxFloat, rt = kMaxFloat;
+  uint32_t near = 0, step = 0, rmat = 0, robj = 0;
+  bool hit = false, bisected = false;
+  for (; step < p.hard_max_steps; ++step) {
+    if (t > tmax || near >= p.scene.max_steps) break;
+    const float qx = __fadd_rn(ox, __fmul_rn(sx, t)), qy = __fadd_rn(oy, __fmul_rn(sy, t)),
+                qz = __fadd_rn(oz, __fmul_rn(sz, t));
+    float md = kMaxFloat;
+    uint32_t bm = 0, bi = 0;
+    for (uint32_t k = 0; k < kp.s.n_objs; ++k) {
+      uint32_t m;
+      const float d = plain_eval(kp, objs[k], qx, qy, qz, &m);
+      if (d < md) {
+        md = d;
+        bm = m;
+        bi = k;
+      }
+    }
+    if (md < 0.0f && prev_dist > p.scene.hit_threshold) {
+      if (r.mode == RKF_TRACE_ANY) {
+        rt = t;
+        hit = true;
+        robj = bi;
+        break;
+      }
+      float lo = prev_t, hi = t;
+      uint32_t bmat = bm;
+      for (uint32_t b = 0; b < p.bisect_steps; ++b) {
+        const float mid = __fmul_rn(__fadd_rn(lo, hi), 0.5f);
+        uint32_t m;
+        const float d = plain_eval(kp, objs[bi], __fadd_rn(ox, __fmul_rn(sx, mid)),
+                                   __fadd_rn(oy, __fmul_rn(sy, mid)), __fadd_rn(oz, __fmul_rn(sz, mid)), &m);
+        if (d < 0.0f) {
+          hi = mid;
+        } else {
+          lo = mid;
+          bmat = m;
+        }
+      }
+      rt = __fmul_rn(__fadd_rn(lo, hi), 0.5f);
+      hit = bisected = true;
+      rmat = bmat;
+      robj = bi;
+      break;
+    }
+    if (md < p.scene.hit_threshold) {
+      rt = t;
+      hit = true;
+      rmat = bm;
+      robj = bi;
+      break;
+    }
+    if (md < p.near_surface_threshold) near++;
+    prev_t = t;
+    prev_dist = md;
+    t = __fadd_rn(t, fmax_(md, p.min_step));
+  }
+  const bool steps_out = !hit && (step >= p.hard_max_steps || near >= p.scene.max_steps);
+  kp.t[i] = hit ? rt : kMaxFloat;
+  if (r.mode == RKF_TRACE_ANY) {
+    if (kp.flags) kp.flags[i] = hit ? RKF_FLAG_HIT : (steps_out ? RKF_FLAG_STEPS_OUT : 0);
+    return;
+  }
+  uint16_t flags = hit ? static_cast<uint16_t>(RKF_FLAG_HIT | (bisected ? RKF_FLAG_BISECTED : 0))
+                       : static_cast<uint16_t>(steps_out ? RKF_FLAG_STEPS_OUT : 0);
+  float nxo = 0, nyo = 0, nzo = 0;
+  uint32_t slot = RKF_EMPTY_SLOT;
+  if (hit) {
+    const ObjDev& o = objs[robj];
+    const float hx = __fadd_rn(ox, __fmul_rn(dx, rt)), hy = __fadd_rn(oy, __fmul_rn(dy, rt)),
+                hz = __fadd_rn(oz, __fmul_rn(dz, rt));
+    if (o.sdf_type == RKF_SDF_VOXELIZED) {
+      float lx, ly, lz;
+      to_local(o, hx, hy, hz, lx, ly, lz);
+      const float e = __fmul_rn(o.vs, 2.0f);
+      const float g0 = __fsub_rn(plain_sample(kp, o, __fadd_rn(lx, e), ly, lz, true),
+                                 plain_sample(kp, o, __fsub_rn(lx, e), ly, lz, true));
+      const float g1 = __fsub_rn(plain_sample(kp, o, lx, __fadd_rn(ly, e), lz, true),
+                                 plain_sample(kp, o, lx, __fsub_rn(ly, e), lz, true));
+      const float g2 = __fsub_rn(plain_sample(kp, o, lx, ly, __fadd_rn(lz, e), true),
+                                 plain_sample(kp, o, lx, ly, __fsub_rn(lz, e), true));
+      const float wx = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(o.m[0], g0), __fmul_rn(o.m[1], g1)), __fmul_rn(o.m[2], g2)), __fmul_rn(o.m[3], 0.0f));
+      const float wy = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(o.m[4], g0), __fmul_rn(o.m[5], g1)), __fmul_rn(o.m[6], g2)), __fmul_rn(o.m[7], 0.0f));
+      const float wz = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(o.m[8], g0), __fmul_rn(o.m[9], g1)), __fmul_rn(o.m[10], g2)), __fmul_rn(o.m[11], 0.0f));
+      const float l = len3(wx, wy, wz);
+      if (l < 1e-10f) {
+        nyo = 1.0f;
+      } else {
+        nxo = __fdiv_rn(wx, l); nyo = __fdiv_rn(wy, l); nzo = __fdiv_rn(wz, l);
+      }
+      size_t vi;
+      slot = plain_nearest(kp, o, lx, ly, lz, &vi);
+    } else {
+      const float e = __fmul_rn(p.scene.hit_threshold, 10.0f);
+      uint32_t m;
+      const float a = __fsub_rn(plain_eval(kp, o, __fadd_rn(hx, e), hy, hz, &m), plain_eval(kp, o, __fsub_rn(hx, e), hy, hz, &m));
+      const float b = __fsub_rn(plain_eval(kp, o, hx, __fadd_rn(hy, e), hz, &m), plain_eval(kp, o, hx, __fsub_rn(hy, e), hz, &m));
+      const float c = __fsub_rn(plain_eval(kp, o, hx, hy, __fadd_rn(hz, e), &m), plain_eval(kp, o, hx, hy, __fsub_rn(hz, e), &m));
+      const float l = len3(a, b, c);
+      nxo = __fdiv_rn(a, l); nyo = __fdiv_rn(b, l); nzo = __fdiv_rn(c, l);
+    }
+  }
+  if (kp.normal) {
+    kp.normal[3 * static_cast<size_t>(i)] = nxo;
+    kp.normal[3 * static_cast<size_t>(i) + 1] = nyo;
+    kp.normal[3 * static_cast<size_t>(i) + 2] = nzo;
+  }
+  if (kp.slot) kp.slot[i] = slot;
+  if (kp.material) kp.material[i] = static_cast<uint16_t>(hit ? rmat : 0u);
+  if (kp.flags) kp.flags[i] = flags;
+}
+
 }  // namespace detail
+
+rkf_status launch_trace_plain(Ctx* c, const float* o, const float* d, const float* tmax, uint32_t n,
+                              uint32_t mode, const rkf_march_params* p, const rkf_hits& out,
+                              cudaStream_t st) {
+  if (!c->aos.p) return fail(RKF_UNSUPPORTED, "rkf_trace_rays_plain: context keeps no reference (AoS) pool");
+  if (n == 0) return RKF_OK;
+  detail::PlainRays r;
+  std::memset(&r, 0, sizeof(r));
+  r.kp.s = c->scene_dev();
+  r.kp.p = *p;
+  r.kp.p.scene.num_objects = c->obj_count();
+  r.kp.t = out.t;
+  r.kp.normal = out.normal;
+  r.kp.slot = out.slot;
+  r.kp.material = out.material;
+  r.kp.flags = out.flags;
+  r.o = o;
+  r.d = d;
+  r.tmax = tmax;
+  r.n = n;
+  r.mode = mode;
+  const size_t smem = sizeof(ObjDev) * (c->obj_count() ? c->obj_count() : 1);
+  detail::k_trace_plain<<<(n + 127) / 128, 128, smem, st>>>(r);
+  RKF_CUDA_TRY(cudaGetLastError());
+  return RKF_OK;
+}
 
 rkf_status launch_plain(Ctx* c, const rkf_camera* cam, const rkf_march_params* p, uint32_t w,
                         uint32_t h, const rkf_gbuffer& out, cudaStream_t st) {

@@ -107,9 +107,12 @@ __device__ __forceinline__ float sample_vox(const SceneDev& s, const ObjDev& o, 
   const float fx = floorf(vcx), fy = floorf(vcy), fz = floorf(vcz);
   const float tx = __fsub_rn(vcx, fx), ty = __fsub_rn(vcy, fy), tz = __fsub_rn(vcz, fz);
   const int x0 = static_cast<int>(fx), y0 = static_cast<int>(fy), z0 = static_cast<int>(fz);
-  const int cx0 = clampi(x0, 0, o.tv[0] - 1), cx1 = clampi(x0 + 1, 0, o.tv[0] - 1);
-  const int cy0 = clampi(y0, 0, o.tv[1] - 1), cy1 = clampi(y0 + 1, 0, o.tv[1] - 1);
-  const int cz0 = clampi(z0, 0, o.tv[2] - 1), cz1 = clampi(z0 + 1, 0, o.tv[2] - 1);
+  // cl lies in [vs*0.01, grid - vs*0.01] (never NaN: the clamp maps NaN to a
+  // bound), so the lower corner x0 is in [-1, tv-1]: clamping x0 from below
+  // and x0+1 from above is the shader's two-sided clamp of both
+  const int cx0 = max(x0, 0), cx1 = min(x0 + 1, o.tv[0] - 1);
+  const int cy0 = max(y0, 0), cy1 = min(y0 + 1, o.tv[1] - 1);
+  const int cz0 = max(z0, 0), cz1 = min(z0 + 1, o.tv[2] - 1);
   // ---- blocks (8^3 bricks = 64 voxels per axis) holding the corners --------
   const uint32_t kx0 = cx0 >> 6, ky0 = cy0 >> 6, kz0 = cz0 >> 6;
   const uint32_t txy = o.tdim[0] * o.tdim[1];
