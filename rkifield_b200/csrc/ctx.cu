@@ -6,6 +6,7 @@
 #include <string>
 
 #include "ctx.h"
+#include "edit.h"
 
 namespace rkf {
 
@@ -228,6 +229,14 @@ __global__ void k_lookup(SceneDev s, uint32_t obj, const uint32_t* bxyz, uint32_
 }
 
 }  // namespace detail
+
+rkf_status lookup_bricks(Ctx* c, uint32_t obj, const uint32_t* d_bxyz, uint32_t n, uint32_t* d_out,
+                         cudaStream_t st) {
+  if (n == 0) return RKF_OK;
+  detail::k_lookup<<<(n + 255) / 256, 256, 0, st>>>(c->scene_dev(), obj, d_bxyz, n, d_out);
+  RKF_CUDA_TRY(cudaGetLastError());
+  return RKF_OK;
+}
 
 // Band-normalised signed u8 code of one brick: step = range/127 with range the
 // largest finite |d| in the brick; |code| = min(floor(|d|/step), 127) so the

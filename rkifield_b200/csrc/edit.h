@@ -1,0 +1,26 @@
+// edit.h — device CSG edits (edit.cu) and the brick lookup they use.
+#pragma once
+
+#include <vector>
+
+#include "ctx.h"
+
+namespace rkf {
+
+struct EditOutcome {
+  uint32_t changed_bricks = 0;
+  DevBuf new_top;                 // top grid of the new epoch (empty: no change)
+  std::vector<uint32_t> retired;  // slots the new epoch no longer references
+};
+
+// Applies one edit; on success with changed bricks, out->new_top holds the
+// new epoch's top grid (the caller publishes it) and out->retired the slots
+// to free once no work reads the previous epoch.  Synchronises `st`.
+rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcome* out);
+
+// Slots (or sentinels) of n bricks (bxyz: 3 u32 each, device) of object obj
+// through the current index, into d_out (device).  Enqueued on st.
+rkf_status lookup_bricks(Ctx* c, uint32_t obj, const uint32_t* d_bxyz, uint32_t n, uint32_t* d_out,
+                         cudaStream_t st);
+
+}  // namespace rkf

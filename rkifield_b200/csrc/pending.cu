@@ -2,7 +2,6 @@
 #include "ctx.h"
 using namespace rkf;
 extern "C" {
-rkf_status rkf_edit_csg(rkf_ctx*, const rkf_edit_op*, uint64_t*) { return fail(RKF_UNSUPPORTED, "rkf_edit_csg: not built"); }
 rkf_status rkf_serve_start(rkf_ctx*, const rkf_march_params*) { return fail(RKF_UNSUPPORTED, "serve: not built"); }
 rkf_status rkf_serve_stop(rkf_ctx*) { return RKF_OK; }
 rkf_status rkf_submit(rkf_ctx*, const rkf_request*, rkf_ticket*) { return fail(RKF_UNSUPPORTED, "serve: not built"); }
