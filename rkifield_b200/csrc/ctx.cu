@@ -178,6 +178,8 @@ rkf_status Ctx::upload_objects() {
 
 rkf_status Ctx::ensure_leaf_capacity(uint32_t need) {
   if (need <= leaf_cap) return RKF_OK;
+  // while serving, in-flight launches hold the leaf buffer's address
+  if (leaves_frozen) return fail(RKF_OOM, "index leaf capacity reserved for the serving session is exhausted");
   uint32_t cap = leaf_cap ? leaf_cap : 64;
   while (cap < need) cap *= 2;
   DevBuf nb;

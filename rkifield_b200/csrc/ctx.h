@@ -75,6 +75,7 @@ struct Ctx {
   uint64_t top_len = 0;
   DevBuf leaves;
   uint32_t n_leaves = 0, leaf_cap = 0;
+  bool leaves_frozen = false;  // set while serving: the leaf buffer must not move
 
   // objects
   std::vector<rkf_gpu_object> objects;

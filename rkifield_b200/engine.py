@@ -202,6 +202,94 @@ class Context:
         return ep.value
 
 
+class Server:
+    """The resident request loop of a :class:`Context` (rkf_serve_start).
+
+    submit_* admit one request and return its ticket; the arrays passed in
+    (inputs and the output arrays the result is written to) must stay alive
+    until poll returns the ticket.  Page-locked arrays let the loop copy
+    asynchronously.  A refused admission raises RkfError(RKF_BUSY)."""
+
+    def __init__(self, ctx: Context, params):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.params = params
+        check(self.lib.rkf_serve_start(ctx.h, C.byref(params)), "rkf_serve_start")
+        self._keep = {}
+
+    def _submit(self, req, keep):
+        t = C.c_uint64()
+        check(self.lib.rkf_submit(self.ctx.h, C.byref(req), C.byref(t)), "rkf_submit")
+        self._keep[t.value] = (req, keep)
+        return t.value
+
+    def submit_render(self, cam, width: int, height: int, out: dict) -> int:
+        r = abi.rkf_request()
+        r.kind = abi.RKF_REQ_RENDER
+        r.width, r.height, r.n = width, height, width * height
+        r.camera = cam
+        r.out_t, r.out_normal = _p(out["t"]), _p(out["normal"])
+        r.out_slot, r.out_material, r.out_flags = _p(out["slot"]), _p(out["material"]), _p(out["flags"])
+        return self._submit(r, out)
+
+    def submit_rays(self, o, d, tmax, mode: int, out: dict) -> int:
+        r = abi.rkf_request()
+        r.kind = abi.RKF_REQ_RAYS
+        r.mode = mode
+        r.n = tmax.size
+        r.in0, r.in1, r.in2 = _p(o), _p(d), _p(tmax)
+        r.out_t, r.out_flags = _p(out["t"]), _p(out["flags"])
+        r.out_normal, r.out_slot, r.out_material = _p(out.get("normal")), _p(out.get("slot")), _p(out.get("material"))
+        return self._submit(r, (o, d, tmax, out))
+
+    def submit_points(self, pts, out: dict) -> int:
+        r = abi.rkf_request()
+        r.kind = abi.RKF_REQ_POINTS
+        r.n = pts.size // 3
+        r.in0 = _p(pts)
+        r.out_t, r.out_normal, r.out_material = _p(out["dist"]), _p(out["grad"]), _p(out["material"])
+        return self._submit(r, (pts, out))
+
+    def submit_edit(self, op) -> int:
+        r = abi.rkf_request()
+        r.kind = abi.RKF_REQ_EDIT
+        r.edit = op
+        return self._submit(r, None)
+
+    def poll(self, ticket: int, timeout_us: int = 0):
+        """Returns the rkf_result as a dict, or None if not complete."""
+        res = abi.rkf_result()
+        st = self.lib.rkf_poll(self.ctx.h, ticket, C.byref(res), timeout_us)
+        if st in (abi.RKF_NOT_READY, abi.RKF_TIMEOUT):
+            return None
+        check(st, "rkf_poll")
+        self._keep.pop(ticket, None)
+        return {k: getattr(res, k) for k, _ in abi.rkf_result._fields_}
+
+    def cancel(self, ticket: int):
+        check(self.lib.rkf_cancel(self.ctx.h, ticket), "rkf_cancel")
+
+    def stop(self):
+        check(self.lib.rkf_serve_stop(self.ctx.h), "rkf_serve_stop")
+
+
+def render_out(n: int) -> dict:
+    return gbuffer_host(n)
+
+
+def rays_out(n: int, mode: int) -> dict:
+    out = {"t": np.zeros(n, np.float32), "flags": np.zeros(n, np.uint16)}
+    if mode == abi.RKF_TRACE_CLOSEST:
+        out.update(normal=np.zeros(3 * n, np.float32), slot=np.zeros(n, np.uint32),
+                   material=np.zeros(n, np.uint16))
+    return out
+
+
+def points_out(n: int) -> dict:
+    return {"dist": np.zeros(n, np.float32), "grad": np.zeros(3 * n, np.float32),
+            "material": np.zeros(n, np.uint16)}
+
+
 class GpuScene:
     """``GpuScene`` upload surface (gpu_scene.rs:141-234) on a :class:`Context`."""
 
