@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--no-sectors", action="store_true")
     ap.add_argument("--cb-views", type=int, default=64, help="views in the batching workload (0 = skip)")
     ap.add_argument("--cb-steps", type=int, default=3)
+    ap.add_argument("--cs-requests", type=int, default=600, help="requests in the serving run (0 = skip)")
+    ap.add_argument("--cs-rate", type=float, default=2000.0)
+    ap.add_argument("--cs-budget", type=int, default=8192, help="serving memory budget, MiB")
     return ap.parse_args()
 
 
@@ -359,6 +362,145 @@ def run_batching(ctx, spec, prims, p, args, stream):
             "vs_plain": val(mb) / val(mp)}
 
 
+def _pinned_copy(arrs, keep):
+    """Copies of the given arrays in one page-locked block (async copies)."""
+    from rkifield_b200 import cudart
+    total = sum(a.nbytes for a in arrs) + 256 * len(arrs)
+    blk = cudart.PinnedArray(total, np.uint8)
+    keep.append(blk)
+    out, off = [], 0
+    for a in arrs:
+        v = blk.array[off:off + a.nbytes].view(a.dtype)
+        v[:] = a.ravel()
+        out.append(v)
+        off += (a.nbytes + 255) // 256 * 256
+    return out
+
+
+def run_serving(args, spec, prims, p, local):
+    """Poisson request stream through the serving loop vs plain per-request
+    launches of the same requests."""
+    import ctypes as C
+
+    from rkifield_b200 import cudart, engine, workloads
+    from rkifield_b200.engine import Context, RkfError, Server
+    reqs = workloads.make_request_stream(spec, prims, args.cs_requests, seed=500, rate_hz=args.cs_rate)
+    keep = []
+    # page-locked inputs and outputs for every request
+    bufs = []
+    for r in reqs:
+        if r.kind == 0:
+            o = engine.render_out(r.width * r.height)
+            names = list(o)
+            pin = _pinned_copy([o[k] for k in names], keep)
+            bufs.append((None, dict(zip(names, pin))))
+        elif r.kind == 1:
+            ins = _pinned_copy([r.o, r.d, r.tmax], keep)
+            o = engine.rays_out(r.n, 0)
+            names = list(o)
+            bufs.append((ins, dict(zip(names, _pinned_copy([o[k] for k in names], keep)))))
+        elif r.kind == 2:
+            ins = _pinned_copy([r.points], keep)
+            o = engine.points_out(r.n)
+            names = list(o)
+            bufs.append((ins, dict(zip(names, _pinned_copy([o[k] for k in names], keep)))))
+        else:
+            bufs.append((None, None))
+    rays_of = lambda r: r.n if r.kind in (0, 1) else 0  # noqa: E731
+    total_rays = sum(rays_of(r) for r in reqs)
+    total_pts = sum(r.n for r in reqs if r.kind == 2)
+
+    # ---- served ----------------------------------------------------------------
+    ctx = Context(device=local, pool_capacity=LARGE_POOL, mem_budget_bytes=args.cs_budget << 20,
+                  max_inflight=256)
+    ctx.voxelize(prims, scenes.voxelize_params(spec, prims))
+    srv = Server(ctx, p)
+    t0 = time.perf_counter()
+    i, live, res, busy = 0, {}, [None] * len(reqs), 0
+    submit_wall = [0.0] * len(reqs)
+    while i < len(reqs) or live:
+        now = time.perf_counter() - t0
+        while i < len(reqs) and reqs[i].arrival_s <= now:
+            r = reqs[i]
+            ins, out = bufs[i]
+            try:
+                if r.kind == 0:
+                    tk = srv.submit_render(r.cam, r.width, r.height, out)
+                elif r.kind == 1:
+                    tk = srv.submit_rays(ins[0], ins[1], ins[2], 0, out)
+                elif r.kind == 2:
+                    tk = srv.submit_points(ins[0], out)
+                else:
+                    tk = srv.submit_edit(r.edit)
+            except RkfError as e:
+                if e.status != abi.RKF_BUSY:
+                    raise
+                busy += 1
+                break  # admission refused: retry this request on the next pass
+            submit_wall[i] = time.perf_counter() - t0
+            live[tk] = i
+            i += 1
+        for tk in list(live):
+            rr = srv.poll(tk, 0)
+            if rr is not None:
+                res[live.pop(tk)] = rr
+        if live and (i >= len(reqs) or reqs[i].arrival_s > time.perf_counter() - t0):
+            time.sleep(20e-6)
+    wall = time.perf_counter() - t0
+    srv.stop()
+    ctx.close()
+    # latency = admission delay (arrival -> accepted) + loop latency (accepted -> done)
+    lat = np.array([(submit_wall[k] - reqs[k].arrival_s) * 1e3 + (res[k]["done_us"] - res[k]["submit_us"]) / 1e3
+                    for k in range(len(reqs))])
+    served = {"value": total_rays / wall / 1e6, "unit": "Mrays/s", "points_per_s": total_pts / wall,
+              "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+              "busy_retries": busy, "wall_s": wall}
+
+    # ---- plain: one launch per request, in arrival order, one at a time --------
+    ctx = Context(device=local, pool_capacity=LARGE_POOL)
+    ctx.voxelize(prims, scenes.voxelize_params(spec, prims))
+    stream = cudart.Stream()
+    service = []
+    for k, r in enumerate(reqs):
+        ins, out = bufs[k]
+        a = time.perf_counter()
+        if r.kind == 0:
+            ctx.march(r.cam, p, r.width, r.height, out=out, plain=True)
+        elif r.kind == 1:
+            n = r.n
+            dev = [cudart.DeviceArray(3 * n, np.float32).upload(ins[0]), cudart.DeviceArray(3 * n, np.float32).upload(ins[1]),
+                   cudart.DeviceArray(n, np.float32).upload(ins[2])]
+            ho = {kk: cudart.DeviceArray(v.size, v.dtype) for kk, v in out.items()}
+            h = abi.rkf_hits()
+            for kk, v in ho.items():
+                setattr(h, kk, v.ptr)
+            h.mem = abi.RKF_MEM_DEVICE
+            abi.check(ctx.lib.rkf_trace_rays_plain_async(ctx.h, dev[0].ptr, dev[1].ptr, dev[2].ptr, n, 0, C.byref(p),
+                                                         C.byref(h), stream.ptr), "plain rays")
+            stream.synchronize()
+            for kk, v in ho.items():
+                out[kk][:] = v.download()
+        elif r.kind == 2:
+            d, g, m = ctx.query_points(ins[0])
+            out["dist"][:], out["grad"][:], out["material"][:] = d, g, m
+        else:
+            ctx.edit(r.edit)
+        service.append(time.perf_counter() - a)
+    ctx.close()
+    # FIFO single server fed by the same arrivals
+    done, lat_p = 0.0, []
+    for r, s in zip(reqs, service):
+        start = max(done, r.arrival_s)
+        done = start + s
+        lat_p.append((done - r.arrival_s) * 1e3)
+    plain_wall = sum(service)
+    plain = {"value": total_rays / plain_wall / 1e6, "unit": "Mrays/s", "points_per_s": total_pts / plain_wall,
+             "latency_ms": {"p50": float(np.percentile(lat_p, 50)), "p99": float(np.percentile(lat_p, 99))}}
+    return {"requests": len(reqs), "rate_hz": args.cs_rate, "rays": total_rays, "points": total_pts,
+            "edits": sum(1 for r in reqs if r.kind == 3), "served": served, "plain_per_request": plain,
+            "vs_plain": served["value"] / plain["value"]}
+
+
 def run_b200(args, world, rank, local, dist):
     from rkifield_b200 import cudart
     from rkifield_b200.engine import Context, gbuffer_host
@@ -436,6 +578,9 @@ def run_b200(args, world, rank, local, dist):
     batching = None
     if args.cb_views > 0:
         batching = run_batching(ctx, spec, prims, p, args, stream)
+    serving = None
+    if args.cs_requests > 0 and rank == 0:
+        serving = run_serving(args, spec, prims, p, local)
 
     out = None
     if rank == 0:
@@ -489,6 +634,7 @@ def run_b200(args, world, rank, local, dist):
             "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roof,
             "batching": batching,
+            "serving": serving,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": args.steps,

@@ -294,6 +294,10 @@ void classify_brick(const rkf_prim* prims, uint32_t n, const rkf_voxelize_params
                                           k, cut, px, py, pz, &mat, &sec, &blend);
         const uint32_t idx = vx + vy * 8 + vz * 64;
         r.dist[idx] = d;
+        if (vp->band_rule == RKF_BAND_REFERENCE) {  // VoxelSample::new(d, mat, 0) (:180)
+          sec = 0;
+          blend = 0;
+        }
         r.words[2 * idx] = pack_word0(d, mat, sec);
         r.words[2 * idx + 1] = blend << 24;
         if (std::fabs(d) <= band) any_band = true;

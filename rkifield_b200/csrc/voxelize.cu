@@ -190,7 +190,8 @@ __global__ void __launch_bounds__(512) k_populate(VoxArgs a, const uint64_t* __r
   const float py = __fadd_rn(my, __fadd_rn(__fmul_rn(static_cast<float>(vy), g.vs), hv));
   const float pz = __fadd_rn(mz, __fadd_rn(__fmul_rn(static_cast<float>(vz), g.vs), hv));
   uint32_t m, s, b;
-  const float d = scene_eval_dev(a, px, py, pz, &m, &s, &b);
+  float d = scene_eval_dev(a, px, py, pz, &m, &s, &b);
+  if (g.rule == RKF_BAND_REFERENCE) s = b = 0;  // VoxelSample::new(d, mat, 0) (voxelize_object.rs:180)
   const size_t o = ci * 512 + v;
   dist[o] = d;
   mat[o] = static_cast<uint16_t>((m & 0x3Fu) | ((s & 0x3Fu) << 6));
