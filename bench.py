@@ -60,6 +60,11 @@ def parse():
     ap.add_argument("--cs-requests", type=int, default=600, help="requests in the serving run (0 = skip)")
     ap.add_argument("--cs-rate", type=float, default=2000.0)
     ap.add_argument("--cs-budget", type=int, default=8192, help="serving memory budget, MiB")
+    ap.add_argument("--pool-bricks", type=int, default=0, help="brick slots to reserve (0 = default)")
+    ap.add_argument("--no-reference-pool", action="store_true",
+                    help="keep no AoS reference pool (implies --no-plain; smaller device footprint)")
+    ap.add_argument("--report", default="", choices=["", "precision"],
+                    help="print a study instead of the benchmark line")
     return ap.parse_args()
 
 
@@ -91,7 +96,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except FileNotFoundError:
@@ -306,8 +311,8 @@ def run_batching(ctx, spec, prims, p, args, stream):
     wl = build_batching(ctx, spec, prims, p, args.cb_views, seed=300)
     nv = len(wl["views"])
     vs, bs = wl["vs"], wl["batches"]
-    # autotune on a sample: the first quarter of the views and their secondaries
-    ns = max(1, nv // 4)
+    # autotune on a sample: the first eighth of the views and their secondaries
+    ns = max(1, nv // 8)
     tu = abi.rkf_batch_tuning()
     t0 = time.perf_counter()
     abi.check(ctx.lib.rkf_autotune(ctx.h, vs, ns, bs, 2 * ns, C.byref(p), C.byref(tu)), "autotune")
@@ -501,6 +506,93 @@ def run_serving(args, spec, prims, p, local):
             "vs_plain": served["value"] / plain["value"]}
 
 
+def run_precision_report(args):
+    """Storage precision study on the small scene: per-ray error of the march
+    over f32 / f16 / u8 planes against the FP64 march over the analytic
+    voxel values (same control flow), 1920x1080 primary rays plus AO rays."""
+    import ctypes as C
+
+    from oracle import binding as oracle
+    from rkifield_b200 import cudart
+    from rkifield_b200.engine import Context
+    spec = scenes.SCENE_SMALL
+    prims = scenes.make_prims(spec)
+    vp = scenes.voxelize_params(spec, prims)
+    w, h = args.width, args.height
+    cam = scenes.seeded_camera(spec, w, h, seed=11)
+    p = scenes.march_params(spec)
+    vs = spec.voxel_size
+    threads = os.cpu_count() or 1
+    v = oracle.Voxelized(prims, vp, threads=threads)
+    f64 = oracle.voxel_values_f64(prims, vp, v.map, v.n_bricks, threads)
+    w0 = v.words[0::2]
+    mat = (((w0 >> 16) & 0x3F) | (((w0 >> 22) & 0x3F) << 6)).astype(np.uint16)
+    blend = (v.words[1::2] >> 24).astype(np.uint8)
+    sc64 = oracle.Scene([v.gpu_object()], brick_maps=v.map, mat_plane=mat, blend_plane=blend,
+                        precision=oracle.PRECISION_F64, dist_f64=f64)
+    t0 = time.perf_counter()
+    ref = oracle.march(sc64, cam, p, w, h, fp64=True, threads=threads, with_margin=True)
+    oracle_s = time.perf_counter() - t0
+    hit64 = (ref["flags"] & 1) != 0
+    n64 = ref["normal64"].reshape(-1, 3)
+    report = {"scene": spec.name, "view": f"{w}x{h}", "rays": w * h, "fp64_hit_fraction": float(hit64.mean()),
+              "fp64_oracle_s": oracle_s, "precisions": {}}
+    ao_ref = None
+    for prec in ("f32", "f16", "u8"):
+        ctx = Context(pool_capacity=v.n_bricks + 1024, precision=prec, keep_reference_pool=False)
+        ctx.voxelize(prims, vp)
+        g = ctx.march(cam, p, w, h)
+        hit = (g["flags"] & 1) != 0
+        both = hit & hit64
+        # grazing: a decision of the FP64 march within 1e-3 voxel of its threshold,
+        # or a hit whose ray meets the surface at under ~3 degrees
+        graze = ref["margin"] < 1e-3 * vs
+        dirs_dot = None
+        nonz = both & ~graze
+        dt = np.abs(g["t"][nonz].astype(np.float64) - ref["t64"][nonz]) / vs
+        ng = g["normal"].reshape(-1, 3)[nonz].astype(np.float64)
+        cosang = np.clip(np.sum(ng * n64[nonz], axis=1) / np.maximum(
+            np.linalg.norm(ng, axis=1) * np.linalg.norm(n64[nonz], axis=1), 1e-300), -1.0, 1.0)
+        ang = np.arccos(cosang)
+        del dirs_dot
+        entry = {"hit_agreement": float((hit == hit64).mean()),
+                 "hit_agreement_non_grazing": float((hit == hit64)[~graze].mean()),
+                 "material_agreement": float((g["material"][both] == ref["material"][both]).mean()) if both.any() else None,
+                 "grazing_fraction": float(graze.mean()),
+                 "dt_voxels": {"max": float(dt.max()), "p99": float(np.percentile(dt, 99)), "mean": float(dt.mean())},
+                 "normal_rad": {"max": float(ang.max()), "p99": float(np.percentile(ang, 99)), "mean": float(ang.mean())},
+                 "within_0.01_voxel": float((dt <= 0.01).mean()),
+                 "bytes_per_voxel_distance": {"f32": 4, "f16": 2, "u8": 1}[prec]}
+        # AO rays (any hit, 1 m) from the FP64 primary hits, traced through each plane
+        if ao_ref is None:
+            dev = cudart.device_gbuffer(w * h)
+            for k in ("t", "normal", "flags"):
+                dev[k].upload(g[k] if k != "t" else np.where(hit64, ref["t64"], 3.4e38).astype(np.float32))
+            dev["flags"].upload(np.where(hit64, 1, 0).astype(np.uint16))
+            dev["normal"].upload(n64.astype(np.float32).ravel())
+            rays = [cudart.DeviceArray(3 * 8 * w * h, np.float32), cudart.DeviceArray(3 * 8 * w * h, np.float32),
+                    cudart.DeviceArray(8 * w * h, np.float32)]
+            gb = abi.rkf_gbuffer()
+            gb.t, gb.normal, gb.flags, gb.mem = dev["t"].ptr, dev["normal"].ptr, dev["flags"].ptr, abi.RKF_MEM_DEVICE
+            nh = C.c_uint32()
+            abi.check(ctx.lib.rkf_secondary_rays(ctx.h, C.byref(cam), w, h, C.byref(gb), None, 0, 8, 1.0, 7,
+                                                 None, None, None, rays[0].ptr, rays[1].ptr, rays[2].ptr,
+                                                 C.byref(nh), None), "ao rays")
+            ao_o, ao_d, ao_t = (r.download() for r in rays)
+            live = ao_t > 0
+            ao_o, ao_d, ao_t = ao_o.reshape(-1, 3)[live], ao_d.reshape(-1, 3)[live], ao_t[live]
+            ao_ref = oracle.trace(sc64, ao_o.ravel(), ao_d.ravel(), ao_t, abi.RKF_TRACE_ANY, p, fp64=True,
+                                  threads=threads, with_margin=True)
+        ao = ctx.trace(ao_o, ao_d, ao_t, abi.RKF_TRACE_ANY, p)
+        ag = (ao["flags"] & 1) == (ao_ref["flags"] & 1)
+        entry["ao_rays"] = int(ao_t.size)
+        entry["ao_occlusion_agreement"] = float(ag.mean())
+        entry["ao_occlusion_agreement_non_grazing"] = float(ag[ao_ref["margin"] >= 1e-3 * vs].mean())
+        report["precisions"][prec] = entry
+        ctx.close()
+    print(json.dumps({"report": "precision", **report}), flush=True)
+
+
 def run_b200(args, world, rank, local, dist):
     from rkifield_b200 import cudart
     from rkifield_b200.engine import Context, gbuffer_host
@@ -508,7 +600,10 @@ def run_b200(args, world, rank, local, dist):
     w, h = args.width, args.height
     n = w * h
     cudart.set_device(local)
-    ctx = Context(device=local, pool_capacity=LARGE_POOL if args.scene == "large" else 65_536)
+    cap = args.pool_bricks or (LARGE_POOL if args.scene == "large" else 65_536)
+    if args.no_reference_pool:
+        args.no_plain = True
+    ctx = Context(device=local, pool_capacity=cap, keep_reference_pool=not args.no_reference_pool)
     prims = scenes.make_prims(spec)
     vp = scenes.voxelize_params(spec, prims)
     t0 = time.perf_counter()
@@ -648,7 +743,10 @@ def main():
     args = parse()
     world, rank, local, dist = dist_setup()
     try:
-        if args.impl == "reference":
+        if args.report == "precision":
+            if rank == 0:
+                run_precision_report(args)
+        elif args.impl == "reference":
             run_reference(args, world, rank, dist)
         else:
             run_b200(args, world, rank, local, dist)

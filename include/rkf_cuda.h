@@ -200,6 +200,14 @@ RKF_API rkf_status rkf_scene_info_get(rkf_ctx* ctx, rkf_scene_info* out);
  * (inverse of rkf_pool_import_voxelsample; used to cross-check). */
 RKF_API rkf_status rkf_pool_export_voxelsample(rkf_ctx* ctx, uint32_t first_slot,
                                        uint32_t n_bricks, uint32_t* words);
+/* Download n_bricks of the structure-of-arrays planes: distances at the
+ * context precision (f16: u16 bits, f32: float, u8: int8 codes; 512 per
+ * brick), the u8 per-brick step (u8 precision only, may be NULL), material
+ * (mat | secondary<<6) and blend planes (may be NULL).  No reference
+ * counterpart (the reference pool is AoS); used to cross-check. */
+RKF_API rkf_status rkf_pool_export_planes(rkf_ctx* ctx, uint32_t first_slot, uint32_t n_bricks,
+                                          void* dist, float* step, uint16_t* mat, uint8_t* blend);
+
 /* Copy the device brick index out: the top grids (8^3-brick blocks: EMPTY,
  * INTERIOR or a leaf number), the 512-entry leaves, and per object
  * {top offset, top dims x, y, z}.  No reference counterpart (the reference

@@ -29,7 +29,9 @@ class orc_scene(C.Structure):
                 ("blend_plane", C.c_void_p), ("precision", C.c_uint32),
                 ("brick_maps", C.c_void_p), ("top", C.c_void_p), ("leaves", C.c_void_p),
                 ("obj_top_info", C.c_void_p), ("objects", C.c_void_p),
-                ("num_objects", C.c_uint32)]
+                ("num_objects", C.c_uint32), ("dist_f64", C.c_void_p)]
+
+PRECISION_F64 = 3
 
 
 class orc_stats(C.Structure):
@@ -78,6 +80,7 @@ def lib() -> C.CDLL:
         L.orc_sample_brick_trilinear.restype = C.c_float
         L.orc_sample_brick_trilinear.argtypes = [P, P, C.c_float]
         L.orc_march_params_default.argtypes = [P]
+        L.orc_voxel_values_f64.argtypes = [P, U32, P, P, U32, P, I]
         _lib = L
     return _lib
 
@@ -151,15 +154,15 @@ class Scene:
     def __init__(self, objects, pool_words=None, brick_maps=None, top=None, leaves=None,
                  obj_top_info=None, dist_f16=None, dist_f32=None, dist_u8=None,
                  brick_scale=None, mat_plane=None, blend_plane=None,
-                 precision=abi.RKF_PRECISION_F16):
+                 precision=abi.RKF_PRECISION_F16, dist_f64=None):
         n = len(objects)
         self.objects = (abi.rkf_gpu_object * n)(*objects)
         self._keep = [pool_words, brick_maps, top, leaves, obj_top_info, dist_f16, dist_f32,
-                      dist_u8, brick_scale, mat_plane, blend_plane]
+                      dist_u8, brick_scale, mat_plane, blend_plane, dist_f64]
         self.s = orc_scene(ptr(pool_words), ptr(dist_f16), ptr(dist_f32), ptr(dist_u8),
                            ptr(brick_scale), ptr(mat_plane), ptr(blend_plane), precision,
                            ptr(brick_maps), ptr(top), ptr(leaves), ptr(obj_top_info),
-                           C.addressof(self.objects), n)
+                           C.addressof(self.objects), n, ptr(dist_f64))
 
 
 def march(scene: Scene, cam, params, w: int, h: int, fp64: bool = False, threads: int | None = None,
@@ -220,3 +223,11 @@ def query_points(scene: Scene, points, threads: int | None = None):
     lib().orc_query_points(C.byref(scene.s), ptr(points), n, ptr(d), ptr(g), ptr(m),
                            threads or nthreads())
     return d, g, m
+
+
+def voxel_values_f64(prims, vp, brick_map, n_slots: int, threads: int | None = None):
+    """FP64 scene SDF at the voxel centres of every allocated brick."""
+    out = np.zeros(n_slots * 512, np.float64)
+    lib().orc_voxel_values_f64(ptr(prims), len(prims), C.byref(vp), ptr(brick_map), n_slots, ptr(out),
+                               threads or nthreads())
+    return out

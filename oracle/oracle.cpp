@@ -407,6 +407,9 @@ struct Marcher {
       case RKF_PRECISION_U8:
         tr->touch(1, v);
         return R(static_cast<float>(s->dist_u8[v])) * R(s->brick_scale[slot]);
+      case ORC_PRECISION_F64:  // analytic values at voxel centres (error reference)
+        tr->touch(1, v * 8);
+        return R(s->dist_f64[v]);
       default:
         tr->touch(1, v * 2);
         return R(f16_to_f32(s->dist_f16[v]));
@@ -1052,6 +1055,33 @@ void orc_voxelized_copy_f32(const orc_voxelized* v, float* dist) {
   std::memcpy(dist, v->dist.data(), v->dist.size() * 4);
 }
 void orc_voxelized_free(orc_voxelized* v) { delete v; }
+
+void orc_voxel_values_f64(const rkf_prim* prims, uint32_t n_prims, const rkf_voxelize_params* vp,
+                          const uint32_t* map, uint32_t n_slots, double* dist, int threads) {
+  const Grid g = make_grid(vp);
+  const uint64_t nb = static_cast<uint64_t>(g.dims[0]) * g.dims[1] * g.dims[2];
+  std::vector<std::vector<uint32_t>> cands(std::max(threads, 1));
+  parallel_for(nb, threads, [&](uint64_t f, int th) {
+    const uint32_t slot = map[f];
+    if (slot >= RKF_INTERIOR_SLOT || slot >= n_slots) return;
+    const uint32_t bx = static_cast<uint32_t>(f % g.dims[0]);
+    const uint32_t by = static_cast<uint32_t>((f / g.dims[0]) % g.dims[1]);
+    const uint32_t bz = static_cast<uint32_t>(f / (static_cast<uint64_t>(g.dims[0]) * g.dims[1]));
+    float bmin[3];
+    brick_min_of(g, bx, by, bz, bmin);
+    brick_candidates(prims, n_prims, bmin, g.bws, vp->cut_distance, cands[th]);
+    const float hv = g.vs * 0.5f;
+    for (uint32_t v = 0; v < 512; ++v) {
+      // the voxel centre the reference samples (voxelize_object.rs:170-176), evaluated in FP64
+      const double px = bmin[0] + (static_cast<float>(v & 7) * g.vs + hv);
+      const double py = bmin[1] + (static_cast<float>((v >> 3) & 7) * g.vs + hv);
+      const double pz = bmin[2] + (static_cast<float>(v >> 6) * g.vs + hv);
+      dist[static_cast<uint64_t>(slot) * 512 + v] =
+          scene_eval<double>(prims, cands[th].data(), static_cast<uint32_t>(cands[th].size()), vp->smooth_k,
+                             vp->cut_distance, px, py, pz, nullptr, nullptr, nullptr);
+    }
+  });
+}
 
 void orc_voxelize_bricks(const rkf_prim* prims, uint32_t n_prims, const rkf_voxelize_params* vp,
                          const uint32_t* bxyz, uint32_t n, uint32_t* cls, uint32_t* words,

@@ -86,7 +86,17 @@ typedef struct orc_scene {
     const uint32_t* obj_top_info;  /* per object: top_offset, bdx, bdy, bdz */
     const rkf_gpu_object* objects;
     uint32_t num_objects;
+    const double* dist_f64;        /* analytic distances (precision 3)      */
 } orc_scene;
+
+/* Distance-plane code for orc_scene.dist_f64. */
+#define ORC_PRECISION_F64 3u
+
+/* The scene SDF evaluated in FP64 at the voxel centres of the allocated
+ * bricks of a flat brick map (dist[slot*512 + x+8y+64z]): the analytic
+ * values a perfect storage format would hold. */
+void orc_voxel_values_f64(const rkf_prim* prims, uint32_t n_prims, const rkf_voxelize_params* vp,
+                          const uint32_t* map, uint32_t n_slots, double* dist, int threads);
 
 typedef struct orc_stats {
     uint64_t sectors;        /* distinct 32-B sectors, summed over rays     */

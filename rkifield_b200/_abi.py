@@ -184,6 +184,7 @@ SIGNATURES = {
     "rkf_scene_info_get": (_I, [_P, C.POINTER(rkf_scene_info)]),
     "rkf_pool_export_voxelsample": (_I, [_P, _U32, _U32, _P]),
     "rkf_brick_lookup": (_I, [_P, _U32, _P, _U32, _P]),
+    "rkf_pool_export_planes": (_I, [_P, _U32, _U32, _P, _P, _P, _P]),
     "rkf_index_export": (_I, [_P, _P, C.POINTER(_U64), _P, C.POINTER(_U64), _P, C.POINTER(_U32)]),
     "rkf_voxelize_prims": (_I, [_P, _P, _U32, C.POINTER(rkf_voxelize_params), C.POINTER(_U32)]),
     "rkf_object_get": (_I, [_P, _U32, C.POINTER(rkf_gpu_object)]),

@@ -23,8 +23,8 @@ extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t
   if (n_views + n_batches == 0) return fail(RKF_INVALID_ARG, "rkf_autotune: no work to tune on");
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   RKF_CUDA_TRY(cudaSetDevice(c->device));
-  static const uint32_t tiles[][2] = {{8, 4}, {4, 8}, {16, 2}, {32, 1}, {16, 4}, {8, 8}};
-  static const uint32_t intervals[] = {4, 8, 16, 32, 64};
+  static const uint32_t tiles[][2] = {{8, 4}, {4, 8}, {16, 2}};
+  static const uint32_t intervals[] = {8, 16, 32, 64};
   static const uint32_t threads[] = {128, 256};
   cudaEvent_t e0, e1;
   RKF_CUDA_TRY(cudaEventCreate(&e0));

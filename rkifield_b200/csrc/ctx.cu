@@ -241,8 +241,9 @@ rkf_status lookup_bricks(Ctx* c, uint32_t obj, const uint32_t* d_bxyz, uint32_t 
 }
 
 // Band-normalised signed u8 code of one brick: step = range/127 with range the
-// largest finite |d| in the brick; |code| = min(floor(|d|/step), 127) so the
-// decoded |d| never exceeds the stored one (sphere tracing never overshoots).
+// largest finite |d| in the brick; |code| = min(floor(|d|/step), 127), less one
+// when the decoded product code*step would round above |d|, so a decoded |d|
+// never exceeds the stored one (sphere tracing never overshoots).
 __global__ void k_encode_u8(const float* __restrict__ src_f32, const uint16_t* __restrict__ src_f16,
                             uint32_t first_slot, uint32_t n_bricks, int8_t* code, float* step) {
   const uint32_t b = blockIdx.x;
@@ -266,8 +267,12 @@ __global__ void k_encode_u8(const float* __restrict__ src_f32, const uint16_t* _
   if (threadIdx.x == 0) step[first_slot + b] = st;
   for (int i = threadIdx.x; i < 512; i += blockDim.x) {
     const float d = src_f32 ? src_f32[base + i] : __half2float(__ushort_as_half(src_f16[base + i]));
-    const float q = floorf(__fdiv_rn(fabsf(d), st));
-    const int c = q >= 127.0f ? 127 : static_cast<int>(q);
+    const float a = fabsf(d);
+    const float q = floorf(__fdiv_rn(a, st));
+    int c = q >= 127.0f ? 127 : static_cast<int>(q);
+    // the decoder's product RN(c*step) must not exceed |d| (the quotient
+    // may round up to the next integer)
+    if (c > 0 && __fmul_rn(static_cast<float>(c), st) > a) --c;
     code[base + i] = static_cast<int8_t>(d < 0.0f ? -c : c);
   }
 }
@@ -516,6 +521,33 @@ rkf_status rkf_scene_info_get(rkf_ctx* ctx, rkf_scene_info* out) {
                       c->mat.bytes + c->blend.bytes + c->aos.bytes + c->top.bytes + c->leaves.bytes +
                       c->flat_maps.bytes + c->objdev.bytes;
   out->epoch = c->epoch;
+  return RKF_OK;
+}
+
+rkf_status rkf_pool_export_planes(rkf_ctx* ctx, uint32_t first_slot, uint32_t n_bricks, void* dist,
+                                  float* step, uint16_t* mat, uint8_t* blend) {
+  if (!ctx) return fail(RKF_INVALID_ARG, "rkf_pool_export_planes: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (static_cast<uint64_t>(first_slot) + n_bricks > c->capacity)
+    return fail(RKF_INVALID_ARG, "rkf_pool_export_planes: range beyond capacity");
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  const size_t v0 = static_cast<size_t>(first_slot) * 512, nv = static_cast<size_t>(n_bricks) * 512;
+  if (dist) {
+    switch (c->cfg.precision) {
+      case RKF_PRECISION_F32:
+        RKF_CUDA_TRY(cudaMemcpy(dist, c->dist_f32.as<float>() + v0, nv * 4, cudaMemcpyDeviceToHost));
+        break;
+      case RKF_PRECISION_U8:
+        RKF_CUDA_TRY(cudaMemcpy(dist, c->dist_u8.as<int8_t>() + v0, nv, cudaMemcpyDeviceToHost));
+        break;
+      default:
+        RKF_CUDA_TRY(cudaMemcpy(dist, c->dist_f16.as<uint16_t>() + v0, nv * 2, cudaMemcpyDeviceToHost));
+    }
+  }
+  if (step && c->cfg.precision == RKF_PRECISION_U8)
+    RKF_CUDA_TRY(cudaMemcpy(step, c->brick_step.as<float>() + first_slot, n_bricks * 4ull, cudaMemcpyDeviceToHost));
+  if (mat) RKF_CUDA_TRY(cudaMemcpy(mat, c->mat.as<uint16_t>() + v0, nv * 2, cudaMemcpyDeviceToHost));
+  if (blend) RKF_CUDA_TRY(cudaMemcpy(blend, c->blend.as<uint8_t>() + v0, nv, cudaMemcpyDeviceToHost));
   return RKF_OK;
 }
 

@@ -120,6 +120,17 @@ class Context:
               "rkf_pool_export_voxelsample")
         return w
 
+    def export_planes(self, first_slot: int, n_bricks: int) -> dict:
+        """SoA planes of the device pool (distance at the context precision)."""
+        dt = {"f16": np.uint16, "f32": np.float32, "u8": np.int8}[self.precision]
+        out = {"dist": np.zeros(n_bricks * 512, dt), "mat": np.zeros(n_bricks * 512, np.uint16),
+               "blend": np.zeros(n_bricks * 512, np.uint8)}
+        if self.precision == "u8":
+            out["step"] = np.zeros(n_bricks, np.float32)
+        check(self.lib.rkf_pool_export_planes(self.h, first_slot, n_bricks, _p(out["dist"]), _p(out.get("step")),
+                                              _p(out["mat"]), _p(out["blend"])), "rkf_pool_export_planes")
+        return out
+
     def export_index(self) -> dict:
         """Device brick index (top grids, leaves, per-object top info)."""
         tn, ln, no = C.c_uint64(), C.c_uint64(), C.c_uint32()
