@@ -217,6 +217,7 @@ SIGNATURES = {
     "rkf_submit": (_I, [_P, C.POINTER(rkf_request), C.POINTER(_U64)]),
     "rkf_poll": (_I, [_P, _U64, C.POINTER(rkf_result), _U32]),
     "rkf_cancel": (_I, [_P, _U64]),
+    "rkf_testing_fail_allocation_after": (None, [C.c_longlong]),
     "rkf_world_relative": (None, [C.POINTER(rkf_world_pos), C.POINTER(rkf_world_pos),
                                   C.POINTER(C.c_double), C.POINTER(C.c_float)]),
 }

@@ -1,10 +1,12 @@
 // ctx.cu — context lifetime, scene import (the reference upload path), the
 // two-level brick index, and small query entry points.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
 
+#include "../../include/rkf_cuda_testing.h"
 #include "ctx.h"
 #include "edit.h"
 
@@ -12,7 +14,20 @@ namespace rkf {
 
 namespace {
 thread_local std::string t_last_error;
-cudaError_t default_alloc(void** p, size_t bytes) { return cudaMalloc(p, bytes); }
+// >= 0: that many more context allocations succeed, then one reports
+// cudaErrorMemoryAllocation without calling cudaMalloc (rkf_testing_*).
+std::atomic<long long> g_fail_after{-1};
+cudaError_t default_alloc(void** p, size_t bytes) {
+  long long n = g_fail_after.load();
+  while (n >= 0) {
+    if (n == 0) {
+      g_fail_after.store(-1);
+      return cudaErrorMemoryAllocation;
+    }
+    if (g_fail_after.compare_exchange_weak(n, n - 1)) break;
+  }
+  return cudaMalloc(p, bytes);
+}
 }  // namespace
 
 alloc_hook_fn g_alloc_hook = default_alloc;
@@ -168,8 +183,11 @@ rkf_status Ctx::upload_objects() {
   if (vst != RKF_OK) return vst;
   const size_t bytes = objdev_host.size() * sizeof(ObjDev);
   if (objdev.bytes < bytes) {
-    rkf_status st = objdev.alloc(bytes);
+    DevBuf nb;  // the old table stays valid if this allocation fails
+    rkf_status st = nb.alloc(bytes);
     if (st != RKF_OK) return st;
+    std::swap(objdev.p, nb.p);
+    std::swap(objdev.bytes, nb.bytes);
   }
   RKF_CUDA_TRY(cudaMemcpyAsync(objdev.p, objdev_host.data(), bytes, cudaMemcpyHostToDevice, stream));
   RKF_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -284,6 +302,8 @@ using namespace rkf;
 extern "C" {
 
 const char* rkf_last_error(void) { return t_last_error.c_str(); }
+
+void rkf_testing_fail_allocation_after(long long n) { g_fail_after.store(n < 0 ? -1 : n); }
 
 void rkf_march_params_default(rkf_march_params* p) {
   if (!p) return;

@@ -51,6 +51,21 @@ struct DevBuf {
 using alloc_hook_fn = cudaError_t (*)(void** p, size_t bytes);
 extern alloc_hook_fn g_alloc_hook;
 
+// Runs its function when the scope ends unless dismissed: undoes a
+// multi-step change of the context that failed part-way.
+template <class F>
+struct Rollback {
+  F f;
+  bool armed = true;
+  explicit Rollback(F fn) : f(fn) {}
+  Rollback(const Rollback&) = delete;
+  Rollback& operator=(const Rollback&) = delete;
+  ~Rollback() {
+    if (armed) f();
+  }
+  void dismiss() { armed = false; }
+};
+
 struct ServeState;  // serve.cu
 
 struct Ctx {

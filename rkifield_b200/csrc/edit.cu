@@ -267,6 +267,18 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
     dst.push_back(c->free_slots.back());
     c->free_slots.pop_back();
   }
+  // Until the new top grid exists, a failure gives the taken slots back and
+  // leaves the index untouched (the copies went to slots nothing references).
+  std::vector<uint32_t> taken = dst;
+  const uint32_t used0 = c->used_slots, leaves0 = c->n_leaves;
+  Rollback undo([&] {
+    for (size_t i = taken.size(); i-- > 0;) c->free_slots.push_back(taken[i]);
+    c->used_slots = used0;
+    c->n_leaves = leaves0;
+    out->retired.clear();
+    out->changed_bricks = 0;
+    out->new_top.release();
+  });
   DevBuf dargs;
   rkf_status s2 = dargs.alloc(static_cast<size_t>(n) * 24 + 256);
   if (s2 != RKF_OK) return s2;
@@ -310,9 +322,13 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
       c->free_slots.push_back(dst[i]);
     }
   }
+  taken = ch_slot;
   c->used_slots += static_cast<uint32_t>(ch_slot.size()) - static_cast<uint32_t>(out->retired.size());
   out->changed_bricks = static_cast<uint32_t>(ch_slot.size());
-  if (ch_slot.empty()) return RKF_OK;
+  if (ch_slot.empty()) {
+    undo.dismiss();
+    return RKF_OK;
+  }
 
   // ---- new epoch of the index: copy the top grid, new leaves for the blocks
   std::vector<uint32_t> blocks;  // global top indices of touched blocks
@@ -364,6 +380,7 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
     }
   }
   RKF_CUDA_TRY(cudaStreamSynchronize(st));
+  undo.dismiss();
   return RKF_OK;
 }
 

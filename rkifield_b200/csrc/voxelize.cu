@@ -383,6 +383,17 @@ extern "C" rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, ui
     cidx[i] = alloc[i].second;
   }
   c->used_slots += n_alloc;
+  // Until the object is committed, a failure gives the slots back (in the
+  // order they were taken) and leaves the index and object table as they were;
+  // bytes already written past top_len / n_leaves are unreferenced.
+  Rollback undo([&, leaves0 = c->n_leaves, top_len0 = c->top_len, nobj0 = c->objects.size()] {
+    for (uint32_t i = n_alloc; i-- > 0;) c->free_slots.push_back(slots[i]);
+    c->used_slots -= n_alloc;
+    c->n_leaves = leaves0;
+    c->top_len = top_len0;
+    c->objects.resize(nobj0);
+    c->objdev_host.resize(nobj0);
+  });
 
   const uint32_t tdim[3] = {(g.dims[0] + 7) / 8, (g.dims[1] + 7) / 8, (g.dims[2] + 7) / 8};
   const size_t ntop = static_cast<size_t>(tdim[0]) * tdim[1] * tdim[2];
@@ -507,6 +518,7 @@ extern "C" rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, ui
   c->objects.push_back(o);
   c->objdev_host.push_back(make_objdev(o, static_cast<uint32_t>(top_off), 0u));
   if ((st = c->upload_objects()) != RKF_OK) return st;
+  undo.dismiss();
   c->epoch++;
   if (out_object_index) *out_object_index = c->obj_count() - 1;
   return RKF_OK;
