@@ -17,6 +17,13 @@ extern "C" {
  * the injection off.  Process-wide. */
 RKF_API void rkf_testing_fail_allocation_after(long long n);
 
+/* Copy the empty-space distance field (one byte per top-grid cell, indexed
+ * like the top grid of rkf_index_export: 0 for a block that is not EMPTY,
+ * else the Chebyshev distance in blocks to the nearest such block of the
+ * same object, capped at 64) into out (may be NULL); *n receives the cell
+ * count. */
+RKF_API rkf_status rkf_testing_export_empty_dist(rkf_ctx* ctx, uint8_t* out, uint64_t* n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,6 +9,7 @@
 #include "../../include/rkf_cuda_testing.h"
 #include "ctx.h"
 #include "edit.h"
+#include "empty_dist.h"
 
 namespace rkf {
 
@@ -119,6 +120,7 @@ SceneDev Ctx::scene_dev() const {
   s.blend = blend.as<uint8_t>();
   s.aos = aos.as<uint2>();
   s.top = top.as<uint32_t>();
+  s.empty_dist = empty_dist.as<uint8_t>();
   s.leaves = leaves.as<uint32_t>();
   s.flat_maps = flat_maps.as<uint32_t>();
   s.objs = objdev.as<ObjDev>();
@@ -440,11 +442,15 @@ rkf_status rkf_pool_export_voxelsample(rkf_ctx* ctx, uint32_t first_slot, uint32
 rkf_status rkf_brickmap_import(rkf_ctx* ctx, const uint32_t* packed, uint64_t n) {
   if (!ctx || (!packed && n)) return fail(RKF_INVALID_ARG, "rkf_brickmap_import: null argument");
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (c->serve) return fail(RKF_BUSY, "rkf_brickmap_import: the context is serving");
   RKF_CUDA_TRY(cudaSetDevice(c->device));
-  c->flat_host.assign(packed, packed + n);
-  rkf_status st = c->flat_maps.alloc(n * 4);
+  DevBuf nb;  // the previous maps stay if this fails
+  rkf_status st = nb.alloc(n * 4);
   if (st != RKF_OK) return st;
-  if (n) RKF_CUDA_TRY(cudaMemcpy(c->flat_maps.p, packed, n * 4, cudaMemcpyHostToDevice));
+  if (n) RKF_CUDA_TRY(cudaMemcpy(nb.p, packed, n * 4, cudaMemcpyHostToDevice));
+  std::swap(c->flat_maps.p, nb.p);
+  std::swap(c->flat_maps.bytes, nb.bytes);
+  c->flat_host.assign(packed, packed + n);
   c->flat_len = n;
   return RKF_OK;
 }
@@ -452,6 +458,7 @@ rkf_status rkf_brickmap_import(rkf_ctx* ctx, const uint32_t* packed, uint64_t n)
 rkf_status rkf_objects_import(rkf_ctx* ctx, const rkf_gpu_object* objects, uint32_t n) {
   if (!ctx || (!objects && n)) return fail(RKF_INVALID_ARG, "rkf_objects_import: null argument");
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (c->serve) return fail(RKF_BUSY, "rkf_objects_import: the context is serving");
   RKF_CUDA_TRY(cudaSetDevice(c->device));
   // validate and build the two-level index of every voxelized object
   std::vector<uint32_t> top;
@@ -502,22 +509,38 @@ rkf_status rkf_objects_import(rkf_ctx* ctx, const rkf_gpu_object* objects, uint3
     }
     od.push_back(make_objdev(o, top_off, o.sdf_type == RKF_SDF_VOXELIZED ? 1u : 0u));
   }
-  // replace the index wholesale
-  c->n_leaves = 0;
+  // replace the index wholesale: build it in fresh buffers, so a failure
+  // leaves the previous scene in place
   const uint32_t nl = static_cast<uint32_t>(leaf_host.size() / 512);
-  rkf_status st = c->ensure_leaf_capacity(nl ? nl : 1);
+  uint32_t cap = 64;
+  while (cap < nl) cap *= 2;
+  DevBuf nleaves, ntop, nfield;
+  rkf_status st = nleaves.alloc(static_cast<size_t>(cap) * 2048);
+  if (st == RKF_OK) st = ntop.alloc(std::max<size_t>(top.size(), 1) * 4);
+  if (st == RKF_OK) st = nfield.alloc(std::max<size_t>(top.size(), 1));
   if (st != RKF_OK) return st;
   if (nl)
-    RKF_CUDA_TRY(cudaMemcpy(c->leaves.p, leaf_host.data(), leaf_host.size() * 4, cudaMemcpyHostToDevice));
+    RKF_CUDA_TRY(cudaMemcpy(nleaves.p, leaf_host.data(), leaf_host.size() * 4, cudaMemcpyHostToDevice));
+  if (!top.empty()) RKF_CUDA_TRY(cudaMemcpy(ntop.p, top.data(), top.size() * 4, cudaMemcpyHostToDevice));
+  for (const ObjDev& d : od)
+    if ((st = build_empty_dist(d, ntop.as<uint32_t>(), nfield.as<uint8_t>(), c->stream)) != RKF_OK) return st;
+  std::vector<rkf_gpu_object> objects0(objects, objects + n);
+  std::swap(c->objects, objects0);
+  std::swap(c->objdev_host, od);
+  if ((st = c->upload_objects()) != RKF_OK) {
+    std::swap(c->objects, objects0);
+    std::swap(c->objdev_host, od);
+    return st;
+  }
+  std::swap(c->leaves.p, nleaves.p);
+  std::swap(c->leaves.bytes, nleaves.bytes);
+  c->leaf_cap = cap;
   c->n_leaves = nl;
-  st = c->top.alloc(std::max<size_t>(top.size(), 1) * 4);
-  if (st != RKF_OK) return st;
-  if (!top.empty()) RKF_CUDA_TRY(cudaMemcpy(c->top.p, top.data(), top.size() * 4, cudaMemcpyHostToDevice));
+  std::swap(c->top.p, ntop.p);
+  std::swap(c->top.bytes, ntop.bytes);
+  std::swap(c->empty_dist.p, nfield.p);
+  std::swap(c->empty_dist.bytes, nfield.bytes);
   c->top_len = top.size();
-  c->objects.assign(objects, objects + n);
-  c->objdev_host = od;
-  st = c->upload_objects();
-  if (st != RKF_OK) return st;
   c->epoch++;
   return RKF_OK;
 }
@@ -538,7 +561,7 @@ rkf_status rkf_scene_info_get(rkf_ctx* ctx, rkf_scene_info* out) {
   out->pool_capacity = c->capacity;
   out->leaf_blocks = c->n_leaves;
   out->device_bytes = c->dist_f16.bytes + c->dist_f32.bytes + c->dist_u8.bytes + c->brick_step.bytes +
-                      c->mat.bytes + c->blend.bytes + c->aos.bytes + c->top.bytes + c->leaves.bytes +
+                      c->mat.bytes + c->blend.bytes + c->aos.bytes + c->top.bytes + c->empty_dist.bytes + c->leaves.bytes +
                       c->flat_maps.bytes + c->objdev.bytes;
   out->epoch = c->epoch;
   return RKF_OK;
@@ -589,6 +612,15 @@ rkf_status rkf_index_export(rkf_ctx* ctx, uint32_t* top, uint64_t* top_n, uint32
       obj_top_info[4 * i] = c->objdev_host[i].top_off;
       for (int a = 0; a < 3; ++a) obj_top_info[4 * i + 1 + a] = c->objdev_host[i].tdim[a];
     }
+  return RKF_OK;
+}
+
+rkf_status rkf_testing_export_empty_dist(rkf_ctx* ctx, uint8_t* out, uint64_t* n) {
+  if (!ctx || !n) return fail(RKF_INVALID_ARG, "rkf_testing_export_empty_dist: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  *n = c->top_len;
+  if (out && c->top_len) RKF_CUDA_TRY(cudaMemcpy(out, c->empty_dist.p, c->top_len, cudaMemcpyDeviceToHost));
   return RKF_OK;
 }
 

@@ -88,6 +88,7 @@ struct Ctx {
   // two-level index
   DevBuf top;
   uint64_t top_len = 0;
+  DevBuf empty_dist;  // u8 per top cell: empty-space distance field (empty_dist.h)
   DevBuf leaves;
   uint32_t n_leaves = 0, leaf_cap = 0;
   bool leaves_frozen = false;  // set while serving: the leaf buffer must not move

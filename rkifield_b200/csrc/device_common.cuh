@@ -76,6 +76,7 @@ struct SceneDev {
   const uint8_t* __restrict__ blend;
   const uint2* __restrict__ aos;
   const uint32_t* __restrict__ top;
+  const uint8_t* __restrict__ empty_dist;  // per top cell, see empty_dist.h
   const uint32_t* __restrict__ leaves;
   const uint32_t* __restrict__ flat_maps;
   const ObjDev* __restrict__ objs;

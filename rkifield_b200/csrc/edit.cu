@@ -23,6 +23,7 @@
 
 #include "ctx.h"
 #include "edit.h"
+#include "empty_dist.h"
 
 namespace rkf {
 namespace detail {
@@ -267,17 +268,20 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
     dst.push_back(c->free_slots.back());
     c->free_slots.pop_back();
   }
-  // Until the new top grid exists, a failure gives the taken slots back and
-  // leaves the index untouched (the copies went to slots nothing references).
-  std::vector<uint32_t> taken = dst;
+  // Until the new top grid exists, a failure restores the free list exactly
+  // (order included) and leaves the index untouched (the copies went to
+  // slots nothing references).
+  const size_t free_kept = c->free_slots.size();
   const uint32_t used0 = c->used_slots, leaves0 = c->n_leaves;
   Rollback undo([&] {
-    for (size_t i = taken.size(); i-- > 0;) c->free_slots.push_back(taken[i]);
+    c->free_slots.resize(free_kept);
+    for (size_t i = dst.size(); i-- > 0;) c->free_slots.push_back(dst[i]);
     c->used_slots = used0;
     c->n_leaves = leaves0;
     out->retired.clear();
     out->changed_bricks = 0;
     out->new_top.release();
+    out->new_empty_dist.release();
   });
   DevBuf dargs;
   rkf_status s2 = dargs.alloc(static_cast<size_t>(n) * 24 + 256);
@@ -322,7 +326,6 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
       c->free_slots.push_back(dst[i]);
     }
   }
-  taken = ch_slot;
   c->used_slots += static_cast<uint32_t>(ch_slot.size()) - static_cast<uint32_t>(out->retired.size());
   out->changed_bricks = static_cast<uint32_t>(ch_slot.size());
   if (ch_slot.empty()) {
@@ -368,6 +371,10 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   RKF_CUDA_TRY(cudaMemcpyAsync(d_topv, newtop.data(), nb * 4ull, cudaMemcpyHostToDevice, st));
   detail::k_scatter_top<<<(nb + 127) / 128, 128, 0, st>>>(out->new_top.as<uint32_t>(), d_blocks, d_topv, nb);
   RKF_CUDA_TRY(cudaGetLastError());
+  // the touched blocks are leaf blocks now: lower the field around them
+  if ((s2 = out->new_empty_dist.alloc(std::max<uint64_t>(c->top_len, 1))) != RKF_OK) return s2;
+  RKF_CUDA_TRY(cudaMemcpyAsync(out->new_empty_dist.p, c->empty_dist.p, c->top_len, cudaMemcpyDeviceToDevice, st));
+  if ((s2 = lower_empty_dist(od, out->new_empty_dist.as<uint8_t>(), d_blocks, blocks, st)) != RKF_OK) return s2;
   c->n_leaves += nb;
   // the reference flat map (read only by the plain march) is updated in place
   if (od.has_flat && !c->flat_host.empty()) {
@@ -401,6 +408,8 @@ extern "C" rkf_status rkf_edit_csg(rkf_ctx* ctx, const rkf_edit_op* op, uint64_t
   if (r.new_top.p) {
     std::swap(c->top.p, r.new_top.p);
     std::swap(c->top.bytes, r.new_top.bytes);
+    std::swap(c->empty_dist.p, r.new_empty_dist.p);
+    std::swap(c->empty_dist.bytes, r.new_empty_dist.bytes);
     c->epoch++;
     for (uint32_t s : r.retired) c->free_slots.push_back(s);
   }

@@ -10,6 +10,7 @@ namespace rkf {
 struct EditOutcome {
   uint32_t changed_bricks = 0;
   DevBuf new_top;                 // top grid of the new epoch (empty: no change)
+  DevBuf new_empty_dist;          // its empty-space distance field
   std::vector<uint32_t> retired;  // slots the new epoch no longer references
 };
 

@@ -53,7 +53,76 @@ struct KParams {
   uint64_t total;
   unsigned long long* counter;
   rkf_march_params p;
+  float probe_min;  // empty-space path: probe for a cube once a sample was at least this
 };
+
+// Object set of a launch: several objects, exactly one, or exactly one that
+// qualifies for the empty-space path (voxelized, translation-only
+// inverse_world, verified exact quotient, fewer than 2^20 voxels per axis).
+enum : int { OBJ_MULTI = 0, OBJ_SINGLE = 1, OBJ_SINGLE_EMPTY = 2 };
+
+// Grid coordinate (position + half grid size, object-local) of the ray at t,
+// rounded exactly as eval_obj -> sample_vox round it for a translation-only
+// object.
+__device__ __forceinline__ float grid_coord(float o, float d, float t, float m, float half) {
+  return __fadd_rn(__fadd_rn(__fadd_rn(o, __fmul_rn(d, t)), m), half);
+}
+
+// The EMPTY sampling value of sample_vox at a grid coordinate whose trilinear
+// cell lies in EMPTY blocks inside the grid and the geometry box (no clamp,
+// no outside term), times the object's scale: eval_obj's result there.
+__device__ __forceinline__ float empty_value(const ObjDev& o, float gx, float gy, float gz) {
+  const float vx = __fsub_rn(exact_div_vs(gx, o.vs, o.rcp_vs), 0.5f);
+  const float vy = __fsub_rn(exact_div_vs(gy, o.vs, o.rcp_vs), 0.5f);
+  const float vz = __fsub_rn(exact_div_vs(gz, o.vs, o.rcp_vs), 0.5f);
+  const float v = mix3_const(o.be, __fsub_rn(vx, floorf(vx)), __fsub_rn(vy, floorf(vy)), __fsub_rn(vz, floorf(vz)));
+  return __fmul_rn(v, o.min_scale);
+}
+
+// Largest t up to which the ray o + d*t stays inside a cube of EMPTY blocks
+// around its position at t (from the empty-space distance field), clipped to
+// the grid and the geometry box; -1 when the position is not in an EMPTY
+// block.  The cube is shrunk by a margin that covers every rounding between
+// t and the sampler's grid coordinate, so for each t' in [t, result] the
+// trilinear corners of the sample at t' lie in the cube: the sample there is
+// exactly empty_value().  Positions are monotone in t along each axis, so
+// checking the exit faces suffices.
+__device__ float probe_empty(const ObjDev& o, const uint8_t* __restrict__ field, float ox, float oy,
+                             float oz, float dx, float dy, float dz, float t) {
+  const float o3[3] = {ox, oy, oz}, d3[3] = {dx, dy, dz};
+  int k[3];
+  float p[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    p[a] = __fadd_rn(o3[a], __fmul_rn(d3[a], t));
+    const float g = __fadd_rn(__fadd_rn(p[a], o.m[12 + a]), o.half_gs[a]);
+    const float f = floorf(__fsub_rn(exact_div_vs(g, o.vs, o.rcp_vs), 0.5f));
+    if (!(f >= 0.0f && f <= static_cast<float>(o.tv[a] - 2))) return -1.0f;
+    k[a] = static_cast<int>(f) >> 6;
+  }
+  const uint32_t s = __ldg(field + o.top_off + k[0] + k[1] * o.tdim[0] + k[2] * o.tdim[0] * o.tdim[1]);
+  if (s == 0) return -1.0f;
+  const int r = static_cast<int>(s) - 1;  // every block within r is EMPTY
+  float mag = 1.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) mag += fabsf(o3[a]) + fabsf(o.m[12 + a]) + o.gs[a];
+  const float margin = 0.1f * o.vs + mag * 3.814697265625e-6f;  // 0.1 voxel + mag * 2^-18
+  float t_exit = kMaxFloat;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int lo_v = max(0, (k[a] - r) * 64), hi_v = min(o.tv[a] - 1, (k[a] + r) * 64 + 63);
+    float wlo = (static_cast<float>(lo_v) + 0.5f) * o.vs - o.half_gs[a] - o.m[12 + a] + margin;
+    float whi = (static_cast<float>(hi_v) + 0.5f) * o.vs - o.half_gs[a] - o.m[12 + a] - margin;
+    if (o.has_geom) {
+      wlo = fmaxf(wlo, o.gmin[a] - o.m[12 + a] + margin);
+      whi = fminf(whi, o.gmax[a] - o.m[12 + a] - margin);
+    }
+    if (!(p[a] >= wlo && p[a] <= whi)) return -1.0f;
+    if (d3[a] > 0.0f) t_exit = fminf(t_exit, (whi - o3[a]) / d3[a]);
+    else if (d3[a] < 0.0f) t_exit = fminf(t_exit, (wlo - o3[a]) / d3[a]);
+  }
+  return t_exit;
+}
 
 __device__ __forceinline__ uint32_t find_segment(const Segment* segs, uint32_t nseg, uint64_t id) {
   uint32_t lo = 0, hi = nseg;  // last segment with first <= id
@@ -89,8 +158,10 @@ __device__ __forceinline__ float eval_min(const SceneDev& s, const ObjDev* objs,
   return best;
 }
 
-template <int PREC, bool SINGLE>
+template <int PREC, int OBJ>
 __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_constant__ KParams kp) {
+  constexpr bool SINGLE = OBJ != OBJ_MULTI;
+  constexpr bool EMPTY_PATH = OBJ == OBJ_SINGLE_EMPTY;
   const ObjDev* sh_objs = kp.objs;
   const SceneDev& s = kp.s;
   const rkf_march_params& p = kp.p;
@@ -107,6 +178,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
   ColdState& cs = cold_all[threadIdx.x];
   float ox = 0, oy = 0, oz = 0, rdx = 0, rdy = 0, rdz = 0;
   float t = 0, prev_t = 0, prev_dist = kMaxFloat, tmax = 0;
+  float box_t = -1.0f;  // empty-space path: positions up to here sample the EMPTY value
   uint32_t near = 0, step = 0;
   bool exhausted = false;
 
@@ -172,6 +244,8 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
             if (valid) {
               near = 0;
               step = 0;
+              box_t = -1.0f;
+              prev_dist = kMaxFloat;
               cs.hit = cs.bisected = cs.mat_ok = false;
               if (mode == RKF_TRACE_SHADOW) {
                 t = 0.005f;  // SHADOW_EPSILON (shade_common.wgsl:274)
@@ -201,7 +275,40 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
     // ---- 2. tight march loop -------------------------------------------------
 #pragma unroll 1
     for (uint32_t k = 0; k < kp.interval; ++k) {
-      if (state == ST_MARCH) {
+      bool full = true;  // take a full step (index lookups) this iteration
+      if (EMPTY_PATH && (state == ST_MARCH || state == ST_SHADOW)) {
+        // empty-space path: inside a cube of EMPTY blocks every sample is
+        // empty_value(), so the steps run without the sampler
+        const ObjDev& o0 = sh_objs[0];
+        const bool sh = state == ST_SHADOW;
+        const float dx = sh ? rdx : qdx, dy = sh ? rdy : qdy, dz = sh ? rdz : qdz;
+        if (t > box_t && prev_dist >= kp.probe_min)
+          box_t = probe_empty(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, t);
+        if (t <= box_t) {
+          const float lim = fminf(box_t, tmax);
+          const uint32_t max_step = sh ? 256u : p.hard_max_steps;
+          const uint32_t max_near = sh ? 32u : p.scene.max_steps;
+          // a sample below these goes to the full step, which decides it
+          const float brk = sh ? 0.02f : fmaxf(hit_thr, 0.0f);
+          const float near_thr = sh ? -1.0f : p.near_surface_threshold;
+          const float min_step = sh ? 0.005f : p.min_step;
+#pragma unroll 1
+          while (t <= lim && step < max_step && near < max_near) {
+            const float d = empty_value(o0, grid_coord(ox, dx, t, o0.m[12], o0.half_gs[0]),
+                                        grid_coord(oy, dy, t, o0.m[13], o0.half_gs[1]),
+                                        grid_coord(oz, dz, t, o0.m[14], o0.half_gs[2]));
+            if (!(d >= brk)) break;
+            if (d < near_thr) ++near;
+            prev_t = t;
+            prev_dist = d;
+            t = __fadd_rn(t, fmax_(d, min_step));
+            ++step;
+          }
+          full = t <= box_t;  // past the cube: probe again next iteration
+        }
+      }
+      if (!full) {
+      } else if (state == ST_MARCH) {
         if (step >= p.hard_max_steps || t > tmax || near >= p.scene.max_steps) {
           cs.hit = false;
           state = ST_EPI;
@@ -257,6 +364,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
           const float best = eval_min<PREC, SINGLE>(s, sh_objs, 0, nobj, __fadd_rn(ox, __fmul_rn(rdx, t)),
                                                     __fadd_rn(oy, __fmul_rn(rdy, t)),
                                                     __fadd_rn(oz, __fmul_rn(rdz, t)), best_un, best_i, lc);
+          prev_dist = best;
           if (best < 0.005f) {
             cs.shadow = 0.0f;
             cs.hit = true;
@@ -271,7 +379,10 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
           }
         }
       }
-      if ((k & 3u) == 3u && !__any_sync(kFull, state == ST_MARCH || state == ST_SHADOW)) break;
+      // leave to finish and refill once a quarter of the lanes are done (or,
+      // with no work left to fetch, once none is marching)
+      const uint32_t active = __popc(__ballot_sync(kFull, state == ST_MARCH || state == ST_SHADOW));
+      if (active <= (exhausted ? 0u : 24u)) break;
     }
 
     // ---- 3. finish: bisection and central differences -------------------------
@@ -506,12 +617,26 @@ __global__ void k_query_points(SceneDev s, const float* __restrict__ pts, uint32
   }
 }
 
-template <int PREC, bool SINGLE>
-const void* persistent_fn() {
-  return reinterpret_cast<const void*>(&k_march_persistent<PREC, SINGLE>);
+template <int PREC>
+const void* persistent_fn(int obj) {
+  if (obj == OBJ_SINGLE_EMPTY) return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_SINGLE_EMPTY>);
+  if (obj == OBJ_SINGLE) return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_SINGLE>);
+  return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_MULTI>);
 }
 
 }  // namespace detail
+
+namespace {
+// Which kernel variant a launch over this context's objects uses.
+int object_set(const Ctx* c) {
+  if (c->obj_count() != 1) return detail::OBJ_MULTI;
+  const ObjDev& o = c->objdev_host[0];
+  const bool empty_path = o.sdf_type == RKF_SDF_VOXELIZED && o.translate_only && o.div_ok &&
+                          c->empty_dist.p != nullptr && o.tv[0] < (1 << 20) && o.tv[1] < (1 << 20) &&
+                          o.tv[2] < (1 << 20);
+  return empty_path ? detail::OBJ_SINGLE_EMPTY : detail::OBJ_SINGLE;
+}
+}  // namespace
 
 rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint64_t total,
                              const rkf_march_params* p, const rkf_batch_tuning& tu,
@@ -539,17 +664,18 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   kp.counter = counter;
   kp.p = *p;
   kp.p.scene.num_objects = c->obj_count();
-  const bool single = c->obj_count() == 1;
+  const int obj = object_set(c);
+  kp.probe_min = obj == detail::OBJ_SINGLE_EMPTY ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
   const void* fn = nullptr;
   switch (c->cfg.precision) {
     case RKF_PRECISION_F32:
-      fn = single ? detail::persistent_fn<RKF_PRECISION_F32, true>() : detail::persistent_fn<RKF_PRECISION_F32, false>();
+      fn = detail::persistent_fn<RKF_PRECISION_F32>(obj);
       break;
     case RKF_PRECISION_U8:
-      fn = single ? detail::persistent_fn<RKF_PRECISION_U8, true>() : detail::persistent_fn<RKF_PRECISION_U8, false>();
+      fn = detail::persistent_fn<RKF_PRECISION_U8>(obj);
       break;
     default:
-      fn = single ? detail::persistent_fn<RKF_PRECISION_F16, true>() : detail::persistent_fn<RKF_PRECISION_F16, false>();
+      fn = detail::persistent_fn<RKF_PRECISION_F16>(obj);
   }
   const uint32_t threads = tu.threads_per_block ? tu.threads_per_block : 256;
   if (threads > 256 || threads % 32)
@@ -591,17 +717,18 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
   kp.counter = dev_counter;
   kp.p = *p;
   kp.p.scene.num_objects = c->obj_count();
-  const bool single = c->obj_count() == 1;
+  const int obj = object_set(c);
+  kp.probe_min = obj == detail::OBJ_SINGLE_EMPTY ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
   const void* fn = nullptr;
   switch (c->cfg.precision) {
     case RKF_PRECISION_F32:
-      fn = single ? detail::persistent_fn<RKF_PRECISION_F32, true>() : detail::persistent_fn<RKF_PRECISION_F32, false>();
+      fn = detail::persistent_fn<RKF_PRECISION_F32>(obj);
       break;
     case RKF_PRECISION_U8:
-      fn = single ? detail::persistent_fn<RKF_PRECISION_U8, true>() : detail::persistent_fn<RKF_PRECISION_U8, false>();
+      fn = detail::persistent_fn<RKF_PRECISION_U8>(obj);
       break;
     default:
-      fn = single ? detail::persistent_fn<RKF_PRECISION_F16, true>() : detail::persistent_fn<RKF_PRECISION_F16, false>();
+      fn = detail::persistent_fn<RKF_PRECISION_F16>(obj);
   }
   const uint32_t threads = tu.threads_per_block ? tu.threads_per_block : 256;
   if (threads > 256 || threads % 32)

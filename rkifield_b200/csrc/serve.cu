@@ -156,6 +156,12 @@ void ServeState::do_edit(uint64_t id) {
     std::swap(c->top.p, out.new_top.p);
     std::swap(c->top.bytes, out.new_top.bytes);
     old_tops.push_back(old);
+    DevBuf* old_field = new DevBuf();
+    std::swap(old_field->p, c->empty_dist.p);
+    std::swap(old_field->bytes, c->empty_dist.bytes);
+    std::swap(c->empty_dist.p, out.new_empty_dist.p);
+    std::swap(c->empty_dist.bytes, out.new_empty_dist.bytes);
+    old_tops.push_back(old_field);
     retired.insert(retired.end(), out.retired.begin(), out.retired.end());
     c->epoch++;
   }

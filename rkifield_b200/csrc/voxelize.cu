@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "ctx.h"
+#include "empty_dist.h"
 
 namespace rkf {
 namespace detail {
@@ -482,18 +483,6 @@ extern "C" rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, ui
     RKF_CUDA_TRY(cudaMemcpyAsync(c->leaves.as<uint32_t>() + static_cast<size_t>(c->n_leaves) * 512, leaves.data(),
                                  leaves.size() * 4, cudaMemcpyHostToDevice, c->stream));
   const uint64_t top_off = c->top_len;
-  {
-    DevBuf nt;
-    if ((st = nt.alloc((top_off + ntop) * 4)) != RKF_OK) return st;
-    if (top_off) RKF_CUDA_TRY(cudaMemcpyAsync(nt.p, c->top.p, top_off * 4, cudaMemcpyDeviceToDevice, c->stream));
-    RKF_CUDA_TRY(cudaMemcpyAsync(nt.as<uint32_t>() + top_off, top.data(), ntop * 4, cudaMemcpyHostToDevice, c->stream));
-    RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    std::swap(c->top.p, nt.p);
-    std::swap(c->top.bytes, nt.bytes);
-  }
-  c->top_len = top_off + ntop;
-  c->n_leaves += n_new_leaves;
-
   rkf_gpu_object o;
   std::memset(&o, 0, sizeof(o));
   for (int i = 0; i < 4; ++i) o.inverse_world[i * 4 + i] = 1.0f;
@@ -515,8 +504,24 @@ extern "C" rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, ui
       o.geometry_aabb_max[a] = static_cast<float>(gh[a]) * be - gs[a] * 0.5f;
     }
   }
+  const ObjDev od = make_objdev(o, static_cast<uint32_t>(top_off), 0u);
+  {
+    DevBuf nt, nf;
+    if ((st = nt.alloc((top_off + ntop) * 4)) != RKF_OK) return st;
+    if ((st = nf.alloc(top_off + ntop)) != RKF_OK) return st;
+    if (top_off) RKF_CUDA_TRY(cudaMemcpyAsync(nt.p, c->top.p, top_off * 4, cudaMemcpyDeviceToDevice, c->stream));
+    if (top_off) RKF_CUDA_TRY(cudaMemcpyAsync(nf.p, c->empty_dist.p, top_off, cudaMemcpyDeviceToDevice, c->stream));
+    RKF_CUDA_TRY(cudaMemcpyAsync(nt.as<uint32_t>() + top_off, top.data(), ntop * 4, cudaMemcpyHostToDevice, c->stream));
+    if ((st = build_empty_dist(od, nt.as<uint32_t>(), nf.as<uint8_t>(), c->stream)) != RKF_OK) return st;
+    std::swap(c->top.p, nt.p);
+    std::swap(c->top.bytes, nt.bytes);
+    std::swap(c->empty_dist.p, nf.p);
+    std::swap(c->empty_dist.bytes, nf.bytes);
+  }
+  c->top_len = top_off + ntop;
+  c->n_leaves += n_new_leaves;
   c->objects.push_back(o);
-  c->objdev_host.push_back(make_objdev(o, static_cast<uint32_t>(top_off), 0u));
+  c->objdev_host.push_back(od);
   if ((st = c->upload_objects()) != RKF_OK) return st;
   undo.dismiss();
   c->epoch++;

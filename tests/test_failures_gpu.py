@@ -119,10 +119,13 @@ def test_edit_failure_rolls_back(inject, small_scene, kind):
     from rkifield_b200 import _abi as abi
     spec = small_scene["spec"]
     n = small_scene["vox"].n_bricks * 2 + 1024
-    p = small_scene["prims"][3]["centre"]
+    prim = small_scene["prims"][3]
+    p = prim["centre"]
+    # additive: a sphere across the primitive's bound; subtractive: carve its centre
+    dx = float(prim["bound_radius"]) + 0.3 if kind == 0 else 0.0
     op = abi.rkf_edit_op()
     op.object_index, op.edit_type, op.shape_type, op.falloff = 0, kind, 0, 1
-    op.position[:] = [float(p[0]) + 0.3, float(p[1]), float(p[2])]
+    op.position[:] = [float(p[0]) + dx, float(p[1]), float(p[2])]
     op.rotation[:] = (0.0, 0.0, 0.0, 1.0)
     op.dimensions[:] = (0.6, 0.0, 0.0)
     op.strength, op.blend_k, op.material_id = 1.0, 0.05, 7
