@@ -358,6 +358,7 @@ def run_batching(ctx, spec, prims, p, args, stream):
     return {"views": nv, "primary_rays": wl["n_primary"], "secondary_rays_live": wl["n_secondary_live"],
             "secondary_ray_slots": wl["n_secondary_slots"],
             "tuning": {"tile": [tu.tile_w, tu.tile_h], "compact_interval": tu.compact_interval,
+                       "step_budget": tu.step_budget,
                        "threads_per_block": tu.threads_per_block, "tune_s": tune_s},
             "batched": {"value": val(mb), "unit": "Mrays/s", "ms": float(np.mean(mb)), "launches": 1},
             "plain_per_request": {"value": val(mp), "unit": "Mrays/s", "ms": float(np.mean(mp)),

@@ -412,8 +412,11 @@ typedef struct rkf_ray_batch {
 
 typedef struct rkf_batch_tuning {
     uint32_t tile_w, tile_h;     /* ray-tile shape of a work item            */
-    uint32_t step_budget;        /* iterations before a ray is re-queued     */
-    uint32_t compact_interval;   /* iterations between warp compactions      */
+    uint32_t step_budget;        /* empty-space steps a lane runs before its */
+                                 /* warp re-converges (0 = 32)               */
+    uint32_t compact_interval;   /* march iterations between lane refills;   */
+                                 /* a warp also refills once a quarter of    */
+                                 /* its lanes are done (0 = 16)              */
     uint32_t blocks_per_sm;
     uint32_t threads_per_block;
 } rkf_batch_tuning;

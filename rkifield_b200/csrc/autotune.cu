@@ -1,11 +1,14 @@
 // autotune.cu — pick the persistent march's launch tuning for a workload.
 //
-// The batched march has three knobs that change speed but never results:
+// The batched march has four knobs that change speed but never results:
 // the ray-tile shape that orders a view's work ids (the spatial coherence of
 // the rays a warp holds), the compaction interval (march iterations between
-// lane refills) and the block size / blocks per SM.  rkf_autotune times every
-// candidate on the caller's sample of the work with CUDA events and keeps
-// the fastest in the context, where rkf_march and rkf_march_batch use it.
+// lane refills), the step budget (empty-space steps a lane runs before its
+// warp re-converges) and the block size.  rkf_autotune times candidates on
+// the caller's sample of the work with CUDA events: every tile x interval x
+// block size at the default budget, then every budget at the best of those.
+// The fastest is kept in the context, where rkf_march and rkf_march_batch
+// use it.
 #include <cfloat>
 #include <cstring>
 #include <vector>
@@ -26,42 +29,46 @@ extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t
   static const uint32_t tiles[][2] = {{8, 4}, {4, 8}, {16, 2}};
   static const uint32_t intervals[] = {8, 16, 32, 64};
   static const uint32_t threads[] = {128, 256};
+  static const uint32_t budgets[] = {8, 16, 64, 128};
   cudaEvent_t e0, e1;
   RKF_CUDA_TRY(cudaEventCreate(&e0));
   RKF_CUDA_TRY(cudaEventCreate(&e1));
   rkf_batch_tuning best = c->tuning;
   float best_ms = FLT_MAX;
   rkf_status st = RKF_OK;
-  for (const auto& tl : tiles) {
-    for (uint32_t iv : intervals) {
-      for (uint32_t th : threads) {
-        rkf_batch_tuning tu{tl[0], tl[1], 0, iv, 0, th};
-        // one untimed launch, then the best of two timed ones
-        st = rkf_march_batch_async(ctx, views, n_views, batches, n_batches, p, &tu, nullptr);
-        if (st != RKF_OK) break;
-        float ms = FLT_MAX;
-        for (int r = 0; r < 2; ++r) {
-          cudaEventRecord(e0, c->stream);
-          st = rkf_march_batch_async(ctx, views, n_views, batches, n_batches, p, &tu, nullptr);
-          if (st != RKF_OK) break;
-          cudaEventRecord(e1, c->stream);
-          if (cudaEventSynchronize(e1) != cudaSuccess) {
-            st = fail(RKF_CUDA_ERROR, "rkf_autotune: launch failed");
-            break;
-          }
-          float m = 0.0f;
-          cudaEventElapsedTime(&m, e0, e1);
-          if (m < ms) ms = m;
-        }
-        if (st != RKF_OK) break;
-        if (ms < best_ms) {
-          best_ms = ms;
-          best = tu;
-        }
+  // one untimed launch, then the best of two timed ones
+  auto trial = [&](const rkf_batch_tuning& tu) {
+    st = rkf_march_batch_async(ctx, views, n_views, batches, n_batches, p, &tu, nullptr);
+    if (st != RKF_OK) return;
+    float ms = FLT_MAX;
+    for (int r = 0; r < 2; ++r) {
+      cudaEventRecord(e0, c->stream);
+      st = rkf_march_batch_async(ctx, views, n_views, batches, n_batches, p, &tu, nullptr);
+      if (st != RKF_OK) return;
+      cudaEventRecord(e1, c->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        st = fail(RKF_CUDA_ERROR, "rkf_autotune: launch failed");
+        return;
       }
-      if (st != RKF_OK) break;
+      float m = 0.0f;
+      cudaEventElapsedTime(&m, e0, e1);
+      if (m < ms) ms = m;
     }
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = tu;
+    }
+  };
+  for (const auto& tl : tiles)
+    for (uint32_t iv : intervals)
+      for (uint32_t th : threads)
+        if (st == RKF_OK) trial(rkf_batch_tuning{tl[0], tl[1], 32, iv, 0, th});
+  const rkf_batch_tuning base = best;
+  for (uint32_t b : budgets) {
     if (st != RKF_OK) break;
+    rkf_batch_tuning tu = base;
+    tu.step_budget = b;
+    trial(tu);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

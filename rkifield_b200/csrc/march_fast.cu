@@ -54,6 +54,8 @@ struct KParams {
   unsigned long long* counter;
   rkf_march_params p;
   float probe_min;  // empty-space path: probe for a cube once a sample was at least this
+  uint32_t budget;     // empty-space path: steps per run before the warp re-converges
+  uint32_t plain_obj;  // object 0 has zero translation and unit scale
 };
 
 // Object set of a launch: several objects, exactly one, or exactly one that
@@ -156,6 +158,49 @@ __device__ __forceinline__ float eval_min(const SceneDev& s, const ObjDev* objs,
     }
   }
   return best;
+}
+
+// Up to n march steps of a ray inside an EMPTY cube (t <= lim): each sample
+// is empty_value(); a sample below brk stops the run before its step (the
+// full step decides it), as does reaching max_near samples below near_thr.
+// PLAIN: the object's translation is zero and its scale one, where adding
+// the translation and multiplying by the scale are exact identities.
+// Returns the number of steps taken.
+template <bool PLAIN>
+__device__ __forceinline__ uint32_t empty_run(const ObjDev& o, float ox, float oy, float oz, float dx,
+                                              float dy, float dz, float lim, uint32_t n, float brk,
+                                              float near_thr, float min_step, uint32_t max_near, float& t,
+                                              float& prev_t, float& prev_dist, uint32_t& near) {
+  uint32_t c = 0;
+#pragma unroll 1
+  for (; c < n && t <= lim; ++c) {
+    float gx, gy, gz;
+    if (PLAIN) {
+      gx = __fadd_rn(__fadd_rn(ox, __fmul_rn(dx, t)), o.half_gs[0]);
+      gy = __fadd_rn(__fadd_rn(oy, __fmul_rn(dy, t)), o.half_gs[1]);
+      gz = __fadd_rn(__fadd_rn(oz, __fmul_rn(dz, t)), o.half_gs[2]);
+    } else {
+      gx = grid_coord(ox, dx, t, o.m[12], o.half_gs[0]);
+      gy = grid_coord(oy, dy, t, o.m[13], o.half_gs[1]);
+      gz = grid_coord(oz, dz, t, o.m[14], o.half_gs[2]);
+    }
+    const float vx = __fsub_rn(exact_div_vs(gx, o.vs, o.rcp_vs), 0.5f);
+    const float vy = __fsub_rn(exact_div_vs(gy, o.vs, o.rcp_vs), 0.5f);
+    const float vz = __fsub_rn(exact_div_vs(gz, o.vs, o.rcp_vs), 0.5f);
+    float d = mix3_const(o.be, __fsub_rn(vx, floorf(vx)), __fsub_rn(vy, floorf(vy)), __fsub_rn(vz, floorf(vz)));
+    if (!PLAIN) d = __fmul_rn(d, o.min_scale);
+    if (!(d >= brk)) break;
+    if (d < near_thr && ++near >= max_near) {
+      prev_t = t;
+      prev_dist = d;
+      t = __fadd_rn(t, fmax_(d, min_step));
+      return c + 1;
+    }
+    prev_t = t;
+    prev_dist = d;
+    t = __fadd_rn(t, fmax_(d, min_step));
+  }
+  return c;
 }
 
 template <int PREC, int OBJ>
@@ -277,34 +322,37 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
     for (uint32_t k = 0; k < kp.interval; ++k) {
       bool full = true;  // take a full step (index lookups) this iteration
       if (EMPTY_PATH && (state == ST_MARCH || state == ST_SHADOW)) {
-        // empty-space path: inside a cube of EMPTY blocks every sample is
-        // empty_value(), so the steps run without the sampler
+        // empty-space run: inside a cube of EMPTY blocks every sample is
+        // empty_value(), so up to kp.budget steps run without the sampler
         const ObjDev& o0 = sh_objs[0];
         const bool sh = state == ST_SHADOW;
         const float dx = sh ? rdx : qdx, dy = sh ? rdy : qdy, dz = sh ? rdz : qdz;
         if (t > box_t && prev_dist >= kp.probe_min)
           box_t = probe_empty(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, t);
         if (t <= box_t) {
-          const float lim = fminf(box_t, tmax);
           const uint32_t max_step = sh ? 256u : p.hard_max_steps;
           const uint32_t max_near = sh ? 32u : p.scene.max_steps;
-          // a sample below these goes to the full step, which decides it
+          const float lim = fminf(box_t, tmax);
+          const uint32_t n = step < max_step ? min(kp.budget, max_step - step) : 0u;
+          // a sample below brk goes to the full step, which decides it
           const float brk = sh ? 0.02f : fmaxf(hit_thr, 0.0f);
           const float near_thr = sh ? -1.0f : p.near_surface_threshold;
           const float min_step = sh ? 0.005f : p.min_step;
-#pragma unroll 1
-          while (t <= lim && step < max_step && near < max_near) {
-            const float d = empty_value(o0, grid_coord(ox, dx, t, o0.m[12], o0.half_gs[0]),
-                                        grid_coord(oy, dy, t, o0.m[13], o0.half_gs[1]),
-                                        grid_coord(oz, dz, t, o0.m[14], o0.half_gs[2]));
-            if (!(d >= brk)) break;
-            if (d < near_thr) ++near;
-            prev_t = t;
-            prev_dist = d;
-            t = __fadd_rn(t, fmax_(d, min_step));
-            ++step;
+          uint32_t c = 0;
+          if (near < max_near) {
+            if (kp.plain_obj)
+              c = empty_run<true>(o0, ox, oy, oz, dx, dy, dz, lim, n, brk, near_thr, min_step, max_near, t,
+                                  prev_t, prev_dist, near);
+            else
+              c = empty_run<false>(o0, ox, oy, oz, dx, dy, dz, lim, n, brk, near_thr, min_step, max_near, t,
+                                   prev_t, prev_dist, near);
           }
-          full = t <= box_t;  // past the cube: probe again next iteration
+          step += c;
+          // the run ends at the budget or the cube's end (the next iteration
+          // continues or probes again) unless a sample needs the full step's
+          // decision or a limit ends the ray
+          const bool run_out = c == n || t > lim;
+          full = !run_out || step >= max_step || t > tmax || near >= max_near;
         }
       }
       if (!full) {
@@ -666,6 +714,11 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   kp.p.scene.num_objects = c->obj_count();
   const int obj = object_set(c);
   kp.probe_min = obj == detail::OBJ_SINGLE_EMPTY ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
+  kp.budget = tu.step_budget ? tu.step_budget : 32;
+  kp.plain_obj = (kp.objs[0].m[12] == 0.0f && kp.objs[0].m[13] == 0.0f && kp.objs[0].m[14] == 0.0f &&
+                  kp.objs[0].min_scale == 1.0f)
+                     ? 1u
+                     : 0u;
   const void* fn = nullptr;
   switch (c->cfg.precision) {
     case RKF_PRECISION_F32:
@@ -719,6 +772,11 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
   kp.p.scene.num_objects = c->obj_count();
   const int obj = object_set(c);
   kp.probe_min = obj == detail::OBJ_SINGLE_EMPTY ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
+  kp.budget = tu.step_budget ? tu.step_budget : 32;
+  kp.plain_obj = (kp.objs[0].m[12] == 0.0f && kp.objs[0].m[13] == 0.0f && kp.objs[0].m[14] == 0.0f &&
+                  kp.objs[0].min_scale == 1.0f)
+                     ? 1u
+                     : 0u;
   const void* fn = nullptr;
   switch (c->cfg.precision) {
     case RKF_PRECISION_F32:
