@@ -358,7 +358,8 @@ def run_batching(ctx, spec, prims, p, args, stream):
     return {"views": nv, "primary_rays": wl["n_primary"], "secondary_rays_live": wl["n_secondary_live"],
             "secondary_ray_slots": wl["n_secondary_slots"],
             "tuning": {"tile": [tu.tile_w, tu.tile_h], "compact_interval": tu.compact_interval,
-                       "step_budget": tu.step_budget,
+                       "step_budget": tu.step_budget, "refill_idle": tu.refill_idle,
+                       "probe_in_run": tu.probe_in_run,
                        "threads_per_block": tu.threads_per_block, "tune_s": tune_s},
             "batched": {"value": val(mb), "unit": "Mrays/s", "ms": float(np.mean(mb)), "launches": 1},
             "plain_per_request": {"value": val(mp), "unit": "Mrays/s", "ms": float(np.mean(mp)),
@@ -463,9 +464,20 @@ def run_serving(args, spec, prims, p, local):
               "busy_retries": busy, "wall_s": wall}
 
     # ---- plain: one launch per request, in arrival order, one at a time --------
+    # device buffers are allocated once (the largest request); each request
+    # copies its inputs in from page-locked memory, launches, copies back
     ctx = Context(device=local, pool_capacity=LARGE_POOL)
     ctx.voxelize(prims, scenes.voxelize_params(spec, prims))
     stream = cudart.Stream()
+    max_rays = max([r.n for r in reqs if r.kind == 1] + [1])
+    dev_in = [cudart.DeviceArray(3 * max_rays, np.float32), cudart.DeviceArray(3 * max_rays, np.float32),
+              cudart.DeviceArray(max_rays, np.float32)]
+    ray_planes = engine.rays_out(max_rays, 0)
+    dev_out = {kk: cudart.DeviceArray(v.size, v.dtype) for kk, v in ray_planes.items()}
+    hits = abi.rkf_hits()
+    for kk, v in dev_out.items():
+        setattr(hits, kk, v.ptr)
+    hits.mem = abi.RKF_MEM_DEVICE
     service = []
     for k, r in enumerate(reqs):
         ins, out = bufs[k]
@@ -474,18 +486,13 @@ def run_serving(args, spec, prims, p, local):
             ctx.march(r.cam, p, r.width, r.height, out=out, plain=True)
         elif r.kind == 1:
             n = r.n
-            dev = [cudart.DeviceArray(3 * n, np.float32).upload(ins[0]), cudart.DeviceArray(3 * n, np.float32).upload(ins[1]),
-                   cudart.DeviceArray(n, np.float32).upload(ins[2])]
-            ho = {kk: cudart.DeviceArray(v.size, v.dtype) for kk, v in out.items()}
-            h = abi.rkf_hits()
-            for kk, v in ho.items():
-                setattr(h, kk, v.ptr)
-            h.mem = abi.RKF_MEM_DEVICE
-            abi.check(ctx.lib.rkf_trace_rays_plain_async(ctx.h, dev[0].ptr, dev[1].ptr, dev[2].ptr, n, 0, C.byref(p),
-                                                         C.byref(h), stream.ptr), "plain rays")
+            for dv, hv in zip(dev_in, ins):
+                dv.upload(hv, stream)
+            abi.check(ctx.lib.rkf_trace_rays_plain_async(ctx.h, dev_in[0].ptr, dev_in[1].ptr, dev_in[2].ptr, n, 0,
+                                                         C.byref(p), C.byref(hits), stream.ptr), "plain rays")
+            for kk, v in out.items():
+                dev_out[kk].download_into(v, stream)
             stream.synchronize()
-            for kk, v in ho.items():
-                out[kk][:] = v.download()
         elif r.kind == 2:
             d, g, m = ctx.query_points(ins[0])
             out["dist"][:], out["grad"][:], out["material"][:] = d, g, m

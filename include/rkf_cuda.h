@@ -415,10 +415,16 @@ typedef struct rkf_batch_tuning {
     uint32_t step_budget;        /* empty-space steps a lane runs before its */
                                  /* warp re-converges (0 = 32)               */
     uint32_t compact_interval;   /* march iterations between lane refills;   */
-                                 /* a warp also refills once a quarter of    */
-                                 /* its lanes are done (0 = 16)              */
+                                 /* a warp also refills once refill_idle of  */
+                                 /* its lanes are done (0 = 64)              */
     uint32_t blocks_per_sm;
     uint32_t threads_per_block;
+    uint32_t refill_idle;        /* a warp leaves the march loop to refill   */
+                                 /* once this many of its lanes are idle     */
+                                 /* (0 = 32: only when all are idle)         */
+    uint32_t probe_in_run;       /* 1: a lane whose EMPTY cube ends probes   */
+                                 /* the next one inside the run (0: at the   */
+                                 /* run's end, with the warp's other lanes)  */
 } rkf_batch_tuning;
 
 /* Run every view and ray batch in one persistent work-stealing launch.

@@ -1,12 +1,15 @@
 // autotune.cu — pick the persistent march's launch tuning for a workload.
 //
-// The batched march has four knobs that change speed but never results:
+// The batched march has six knobs that change speed but never results:
 // the ray-tile shape that orders a view's work ids (the spatial coherence of
 // the rays a warp holds), the compaction interval (march iterations between
 // lane refills), the step budget (empty-space steps a lane runs before its
-// warp re-converges) and the block size.  rkf_autotune times candidates on
-// the caller's sample of the work with CUDA events: every tile x interval x
-// block size at the default budget, then every budget at the best of those.
+// warp re-converges), the refill threshold (idle lanes that make a warp
+// refill), where a lane probes its next EMPTY cube (inside a run or between
+// runs) and the block size.  rkf_autotune times candidates on the caller's
+// sample of the work with CUDA events: every tile x interval x block size at
+// the default budget and threshold, then every budget, then every threshold,
+// then the other probe placement, each at the best so far.
 // The fastest is kept in the context, where rkf_march and rkf_march_batch
 // use it.
 #include <cfloat>
@@ -26,10 +29,11 @@ extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t
   if (n_views + n_batches == 0) return fail(RKF_INVALID_ARG, "rkf_autotune: no work to tune on");
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   RKF_CUDA_TRY(cudaSetDevice(c->device));
-  static const uint32_t tiles[][2] = {{8, 4}, {4, 8}, {16, 2}};
-  static const uint32_t intervals[] = {8, 16, 32, 64};
+  static const uint32_t tiles[][2] = {{4, 8}, {8, 4}, {16, 2}};
+  static const uint32_t intervals[] = {16, 32, 64, 128};
   static const uint32_t threads[] = {128, 256};
-  static const uint32_t budgets[] = {8, 16, 64, 128};
+  static const uint32_t budgets[] = {16, 64};
+  static const uint32_t refills[] = {8, 16, 24};
   cudaEvent_t e0, e1;
   RKF_CUDA_TRY(cudaEventCreate(&e0));
   RKF_CUDA_TRY(cudaEventCreate(&e1));
@@ -62,12 +66,24 @@ extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t
   for (const auto& tl : tiles)
     for (uint32_t iv : intervals)
       for (uint32_t th : threads)
-        if (st == RKF_OK) trial(rkf_batch_tuning{tl[0], tl[1], 32, iv, 0, th});
+        if (st == RKF_OK) trial(rkf_batch_tuning{tl[0], tl[1], 32, iv, 0, th, 32, 0});
   const rkf_batch_tuning base = best;
   for (uint32_t b : budgets) {
     if (st != RKF_OK) break;
     rkf_batch_tuning tu = base;
     tu.step_budget = b;
+    trial(tu);
+  }
+  const rkf_batch_tuning base2 = best;
+  for (uint32_t r : refills) {
+    if (st != RKF_OK) break;
+    rkf_batch_tuning tu = base2;
+    tu.refill_idle = r;
+    trial(tu);
+  }
+  if (st == RKF_OK) {
+    rkf_batch_tuning tu = best;
+    tu.probe_in_run = 1;
     trial(tu);
   }
   cudaEventDestroy(e0);

@@ -56,6 +56,9 @@ struct KParams {
   float probe_min;  // empty-space path: probe for a cube once a sample was at least this
   uint32_t budget;     // empty-space path: steps per run before the warp re-converges
   uint32_t plain_obj;  // object 0 has zero translation and unit scale
+  uint32_t refill_active;  // leave the march loop once at most this many lanes march
+  uint32_t run_probe;      // empty-space path: probe the next cube inside a run
+  float empty_lo;          // empty-space path: lower bound of every EMPTY value
 };
 
 // Object set of a launch: several objects, exactly one, or exactly one that
@@ -160,20 +163,40 @@ __device__ __forceinline__ float eval_min(const SceneDev& s, const ObjDev* objs,
   return best;
 }
 
-// Up to n march steps of a ray inside an EMPTY cube (t <= lim): each sample
-// is empty_value(); a sample below brk stops the run before its step (the
-// full step decides it), as does reaching max_near samples below near_thr.
-// PLAIN: the object's translation is zero and its scale one, where adding
-// the translation and multiplying by the scale are exact identities.
+// Up to n march steps of a ray through EMPTY cubes: each sample is
+// empty_value().  The run stops before a step whose sample is below brk or
+// whose t is past tmax (the full step decides those), after the step that
+// makes max_near samples below near_thr, and where the ray leaves its cube
+// (t > box_t).  INRUN: a lane whose cube ends probes the next cube in place
+// and runs on; stop_full tells whether the next step must be a full one.
+// PLAIN: the object's translation is zero and its scale one, where adding the
+// translation and multiplying by the scale are exact identities.  CLEAN: every
+// EMPTY value is at least brk, near_thr and min_step (the caller checks this
+// against a lower bound), so those comparisons are known and skipped.
 // Returns the number of steps taken.
-template <bool PLAIN>
-__device__ __forceinline__ uint32_t empty_run(const ObjDev& o, float ox, float oy, float oz, float dx,
-                                              float dy, float dz, float lim, uint32_t n, float brk,
-                                              float near_thr, float min_step, uint32_t max_near, float& t,
-                                              float& prev_t, float& prev_dist, uint32_t& near) {
+template <bool PLAIN, bool CLEAN, bool INRUN>
+__device__ __forceinline__ uint32_t empty_run(const ObjDev& o, const uint8_t* __restrict__ field, float ox,
+                                              float oy, float oz, float dx, float dy, float dz, float tmax,
+                                              uint32_t n, float brk, float near_thr, float min_step,
+                                              uint32_t max_near, float& t, float& box_t, float& prev_t,
+                                              float& prev_dist, uint32_t& near, bool& stop_full) {
   uint32_t c = 0;
-#pragma unroll 1
-  for (; c < n && t <= lim; ++c) {
+  float lim = fminf(box_t, tmax);
+  stop_full = false;
+#pragma unroll 2
+  for (; c < n; ++c) {
+    if (t > lim) {
+      if (!INRUN || t > tmax) {
+        stop_full = t > tmax;
+        break;
+      }
+      box_t = probe_empty(o, field, ox, oy, oz, dx, dy, dz, t);
+      lim = fminf(box_t, tmax);
+      if (t > lim) {
+        stop_full = true;
+        break;
+      }
+    }
     float gx, gy, gz;
     if (PLAIN) {
       gx = __fadd_rn(__fadd_rn(ox, __fmul_rn(dx, t)), o.half_gs[0]);
@@ -189,16 +212,21 @@ __device__ __forceinline__ uint32_t empty_run(const ObjDev& o, float ox, float o
     const float vz = __fsub_rn(exact_div_vs(gz, o.vs, o.rcp_vs), 0.5f);
     float d = mix3_const(o.be, __fsub_rn(vx, floorf(vx)), __fsub_rn(vy, floorf(vy)), __fsub_rn(vz, floorf(vz)));
     if (!PLAIN) d = __fmul_rn(d, o.min_scale);
-    if (!(d >= brk)) break;
-    if (d < near_thr && ++near >= max_near) {
-      prev_t = t;
-      prev_dist = d;
-      t = __fadd_rn(t, fmax_(d, min_step));
-      return c + 1;
+    if (!CLEAN && !(d >= brk)) {  // no step: the full step redoes this sample
+      stop_full = true;
+      break;
     }
     prev_t = t;
     prev_dist = d;
+    if (CLEAN) {
+      t = __fadd_rn(t, d);
+      continue;
+    }
     t = __fadd_rn(t, fmax_(d, min_step));
+    if (d < near_thr && ++near >= max_near) {
+      stop_full = true;
+      return c + 1;
+    }
   }
   return c;
 }
@@ -332,27 +360,31 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
         if (t <= box_t) {
           const uint32_t max_step = sh ? 256u : p.hard_max_steps;
           const uint32_t max_near = sh ? 32u : p.scene.max_steps;
-          const float lim = fminf(box_t, tmax);
           const uint32_t n = step < max_step ? min(kp.budget, max_step - step) : 0u;
           // a sample below brk goes to the full step, which decides it
           const float brk = sh ? 0.02f : fmaxf(hit_thr, 0.0f);
           const float near_thr = sh ? -1.0f : p.near_surface_threshold;
           const float min_step = sh ? 0.005f : p.min_step;
           uint32_t c = 0;
+          bool stop_full = true;
           if (near < max_near) {
-            if (kp.plain_obj)
-              c = empty_run<true>(o0, ox, oy, oz, dx, dy, dz, lim, n, brk, near_thr, min_step, max_near, t,
-                                  prev_t, prev_dist, near);
+            const bool clean = kp.empty_lo >= brk && kp.empty_lo >= near_thr && kp.empty_lo >= min_step;
+#define RKF_RUN(P, CL, IN)                                                                                   \
+  empty_run<P, CL, IN>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n, brk, near_thr, min_step, max_near, t, \
+                       box_t, prev_t, prev_dist, near, stop_full)
+            if (kp.plain_obj && clean)
+              c = kp.run_probe ? RKF_RUN(true, true, true) : RKF_RUN(true, true, false);
+            else if (kp.plain_obj)
+              c = kp.run_probe ? RKF_RUN(true, false, true) : RKF_RUN(true, false, false);
             else
-              c = empty_run<false>(o0, ox, oy, oz, dx, dy, dz, lim, n, brk, near_thr, min_step, max_near, t,
-                                   prev_t, prev_dist, near);
+              c = kp.run_probe ? RKF_RUN(false, false, true) : RKF_RUN(false, false, false);
+#undef RKF_RUN
           }
           step += c;
-          // the run ends at the budget or the cube's end (the next iteration
-          // continues or probes again) unless a sample needs the full step's
-          // decision or a limit ends the ray
-          const bool run_out = c == n || t > lim;
-          full = !run_out || step >= max_step || t > tmax || near >= max_near;
+          // a run that used its whole budget, or reached the end of its cube
+          // between probes, continues next iteration unless a limit ends the
+          // ray; any other stop needs the full step's decision
+          full = stop_full || step >= max_step || t > tmax || near >= max_near;
         }
       }
       if (!full) {
@@ -427,10 +459,10 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
           }
         }
       }
-      // leave to finish and refill once a quarter of the lanes are done (or,
+      // leave to finish and refill once refill_idle lanes are done (or,
       // with no work left to fetch, once none is marching)
       const uint32_t active = __popc(__ballot_sync(kFull, state == ST_MARCH || state == ST_SHADOW));
-      if (active <= (exhausted ? 0u : 24u)) break;
+      if (active <= (exhausted ? 0u : kp.refill_active)) break;
     }
 
     // ---- 3. finish: bisection and central differences -------------------------
@@ -707,7 +739,7 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   kp.nseg = static_cast<uint32_t>(segs_host.size());
   kp.tile_w = tu.tile_w ? tu.tile_w : 8;
   kp.tile_h = tu.tile_h ? tu.tile_h : 4;
-  kp.interval = tu.compact_interval ? tu.compact_interval : 16;
+  kp.interval = tu.compact_interval ? tu.compact_interval : 64;
   kp.total = total;
   kp.counter = counter;
   kp.p = *p;
@@ -715,6 +747,11 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   const int obj = object_set(c);
   kp.probe_min = obj == detail::OBJ_SINGLE_EMPTY ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
   kp.budget = tu.step_budget ? tu.step_budget : 32;
+  kp.refill_active = 32u - std::min<uint32_t>(tu.refill_idle ? tu.refill_idle : 32u, 32u);
+  kp.run_probe = tu.probe_in_run ? 1u : 0u;
+  // mix(c, c, t) three times stays within 12 roundings of c (relative 2^-24
+  // each); 0.999 leaves a wide margin
+  kp.empty_lo = obj == detail::OBJ_SINGLE_EMPTY ? 0.999f * kp.objs[0].be * kp.objs[0].min_scale : 0.0f;
   kp.plain_obj = (kp.objs[0].m[12] == 0.0f && kp.objs[0].m[13] == 0.0f && kp.objs[0].m[14] == 0.0f &&
                   kp.objs[0].min_scale == 1.0f)
                      ? 1u
@@ -765,7 +802,7 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
   kp.nseg = nseg;
   kp.tile_w = tu.tile_w ? tu.tile_w : 8;
   kp.tile_h = tu.tile_h ? tu.tile_h : 4;
-  kp.interval = tu.compact_interval ? tu.compact_interval : 16;
+  kp.interval = tu.compact_interval ? tu.compact_interval : 64;
   kp.total = total;
   kp.counter = dev_counter;
   kp.p = *p;
@@ -773,6 +810,11 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
   const int obj = object_set(c);
   kp.probe_min = obj == detail::OBJ_SINGLE_EMPTY ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
   kp.budget = tu.step_budget ? tu.step_budget : 32;
+  kp.refill_active = 32u - std::min<uint32_t>(tu.refill_idle ? tu.refill_idle : 32u, 32u);
+  kp.run_probe = tu.probe_in_run ? 1u : 0u;
+  // mix(c, c, t) three times stays within 12 roundings of c (relative 2^-24
+  // each); 0.999 leaves a wide margin
+  kp.empty_lo = obj == detail::OBJ_SINGLE_EMPTY ? 0.999f * kp.objs[0].be * kp.objs[0].min_scale : 0.0f;
   kp.plain_obj = (kp.objs[0].m[12] == 0.0f && kp.objs[0].m[13] == 0.0f && kp.objs[0].m[14] == 0.0f &&
                   kp.objs[0].min_scale == 1.0f)
                      ? 1u

@@ -51,6 +51,17 @@ class DeviceArray:
         _ok(rt.cudaMemcpy(out.ctypes.data, self.ptr, out.nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost))
         return out
 
+    def download_into(self, host: np.ndarray, stream=None) -> np.ndarray:
+        """Copy the first host.size elements into ``host`` (asynchronously on
+        ``stream`` when given: ``host`` should then be page-locked)."""
+        assert host.dtype == self.dtype and host.flags.c_contiguous and host.nbytes <= self.nbytes
+        if stream is None:
+            _ok(rt.cudaMemcpy(host.ctypes.data, self.ptr, host.nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost))
+        else:
+            _ok(rt.cudaMemcpyAsync(host.ctypes.data, self.ptr, host.nbytes,
+                                   rt.cudaMemcpyKind.cudaMemcpyDeviceToHost, stream.handle))
+        return host
+
     def memset(self, value: int = 0, stream=None):
         if stream is None:
             _ok(rt.cudaMemset(self.ptr, value, self.nbytes))

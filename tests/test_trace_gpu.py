@@ -108,7 +108,8 @@ def test_batch_equals_separate_calls(small_scene, small_ctx):
         for k, a in h.items():
             setattr(batches[j].out, k, a.ptr)
         batches[j].out.mem = abi.RKF_MEM_DEVICE
-    for tu in (None, (16, 2, 0, 4, 0, 128), (4, 8, 0, 64, 1, 256)):
+    for tu in (None, (16, 2, 0, 4, 0, 128, 0, 0), (4, 8, 0, 64, 1, 256, 0, 1), (8, 4, 3, 16, 0, 256, 32, 0),
+               (4, 8, 200, 8, 0, 64, 1, 1)):
         tuning = None
         if tu is not None:
             tuning = abi.rkf_batch_tuning(*tu)
