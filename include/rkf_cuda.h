@@ -176,6 +176,14 @@ RKF_API const char* rkf_last_error(void);
 RKF_API rkf_status rkf_pool_import_voxelsample(rkf_ctx* ctx, const uint32_t* words,
                                        uint32_t first_slot, uint32_t n_bricks);
 
+/* Upload bricks given as structure-of-arrays planes, 512 voxels per brick in
+ * x+8y+64z order: dist_f16 (binary16 bits), mat (material | secondary << 6,
+ * 6 bits each) and blend, into slots [first_slot, first_slot+n_bricks).
+ * The same content as rkf_pool_import_voxelsample without the 8-byte word
+ * packing (VoxelSample::new_blended, voxel.rs:43-54, is how the words hold it). */
+RKF_API rkf_status rkf_pool_import_soa(rkf_ctx* ctx, const uint16_t* dist_f16, const uint16_t* mat,
+                                       const uint8_t* blend, uint32_t first_slot, uint32_t n_bricks);
+
 /* Upload the packed BrickMapAllocator buffer (brick_map.rs:246 as_slice).
  * Replaces GpuScene::upload_brick_maps (gpu_scene.rs:170). */
 RKF_API rkf_status rkf_brickmap_import(rkf_ctx* ctx, const uint32_t* packed, uint64_t n);
@@ -367,6 +375,13 @@ RKF_API rkf_status rkf_secondary_rays(rkf_ctx* ctx, const rkf_camera* cam, uint3
  * material[n] (may be NULL).  mem applies to all pointers. */
 RKF_API rkf_status rkf_query_points(rkf_ctx* ctx, const float* points, uint32_t n,
                             float* dist, float* grad, uint16_t* material, uint32_t mem);
+
+/* Ambient occlusion: sdf_ao (shade_common_shading.wgsl:37-47) at pos[3n]
+ * along normal[3n] (4 taps 0.12 m apart through sample_sdf, strength 0.7)
+ * -> ao[n] in [0, 1].  The shading pass calls it at world_pos + normal *
+ * SHADOW_BIAS (0.08, shade_main.wgsl:186).  mem applies to all pointers. */
+RKF_API rkf_status rkf_sdf_ao(rkf_ctx* ctx, const float* pos, const float* normal, uint32_t n,
+                              float* ao, uint32_t mem);
 
 /* ------------------------------------------------------------------------ */
 /* CSG edits (crates/rkf-edit/src/edit_op.rs:15, cpu_apply.rs:28-229)       */

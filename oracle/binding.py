@@ -225,6 +225,14 @@ def query_points(scene: Scene, points, threads: int | None = None):
     return d, g, m
 
 
+def sdf_ao(scene: Scene, pos, normal, threads: int | None = None):
+    pos = np.ascontiguousarray(pos, np.float32).ravel()
+    normal = np.ascontiguousarray(normal, np.float32).ravel()
+    out = np.zeros(pos.size // 3, np.float32)
+    lib().orc_sdf_ao(C.byref(scene.s), ptr(pos), ptr(normal), out.size, ptr(out), threads or nthreads())
+    return out
+
+
 def voxel_values_f64(prims, vp, brick_map, n_slots: int, threads: int | None = None):
     """FP64 scene SDF at the voxel centres of every allocated brick."""
     out = np.zeros(n_slots * 512, np.float64)

@@ -1153,6 +1153,35 @@ void orc_query_points(const orc_scene* s, const float* points, uint32_t n, float
   });
 }
 
+// sdf_ao (shade_common_shading.wgsl:37-47) through sample_sdf
+// (shade_common.wgsl:521-572: inside the objects' bounds, the minimum of
+// evaluate_object over the objects).
+void orc_sdf_ao(const orc_scene* s, const float* pos, const float* normal, uint32_t n, float* ao,
+                int threads) {
+  parallel_for(n, threads, [&](uint64_t i, int) {
+    Tracker tr;
+    Marcher<float> mc{s, &tr, nullptr};
+    const V3<float> p = v3<float>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+    const V3<float> nv = v3<float>(normal[3 * i], normal[3 * i + 1], normal[3 * i + 2]);
+    float acc = 0.0f, scale = 1.0f;
+    for (uint32_t k = 1; k <= 4; ++k) {
+      const float dist = 0.12f * static_cast<float>(k);  // AO_STEP_SIZE * f32(i)
+      const V3<float> q = add(p, mul(nv, dist));
+      float d = kMaxFloat;
+      for (uint32_t oi = 0; oi < s->num_objects; ++oi) {
+        uint32_t m;
+        const float e = mc.evaluate(q, oi, &m);
+        d = e < d ? e : d;
+      }
+      acc = acc + scale * (dist - d);
+      scale = scale * 0.5f;
+    }
+    const float v = 1.0f - 0.7f * acc;  // AO_STRENGTH
+    const float lo = v < 0.0f ? 0.0f : v;
+    ao[i] = lo > 1.0f ? 1.0f : lo;
+  });
+}
+
 // ---------------------------------------------------------------------------
 // CSG edits (crates/rkf-edit/src/cpu_apply.rs)
 // ---------------------------------------------------------------------------

@@ -132,6 +132,10 @@ void orc_trace_rays(const orc_scene* s, const float* origins, const float* dirs,
 void orc_query_points(const orc_scene* s, const float* points, uint32_t n,
                       float* dist, float* grad, uint16_t* material, int threads);
 
+/* sdf_ao (shade_common_shading.wgsl:37-47) at pos along normal -> ao[n]. */
+void orc_sdf_ao(const orc_scene* s, const float* pos, const float* normal, uint32_t n, float* ao,
+                int threads);
+
 /* CPU CSG edit on one brick (cpu_apply.rs:28-200): rewrites the 1024 words
  * of the brick in place; brick_local_min as find_affected_bricks computes
  * it.  Returns 1 when the brick counts as modified. */

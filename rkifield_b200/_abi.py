@@ -218,6 +218,8 @@ SIGNATURES = {
     "rkf_submit": (_I, [_P, C.POINTER(rkf_request), C.POINTER(_U64)]),
     "rkf_poll": (_I, [_P, _U64, C.POINTER(rkf_result), _U32]),
     "rkf_cancel": (_I, [_P, _U64]),
+    "rkf_sdf_ao": (_I, [_P, _P, _P, _U32, _P, _U32]),
+    "rkf_pool_import_soa": (_I, [_P, _P, _P, _P, _U32, _U32]),
     "rkf_testing_fail_allocation_after": (None, [C.c_longlong]),
     "rkf_testing_export_empty_dist": (_I, [_P, _P, C.POINTER(C.c_uint64)]),
     "rkf_world_relative": (None, [C.POINTER(rkf_world_pos), C.POINTER(rkf_world_pos),

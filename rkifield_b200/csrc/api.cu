@@ -256,6 +256,34 @@ rkf_status rkf_query_points(rkf_ctx* ctx, const float* points, uint32_t n, float
   return RKF_OK;
 }
 
+rkf_status rkf_sdf_ao(rkf_ctx* ctx, const float* pos, const float* normal, uint32_t n, float* ao,
+                      uint32_t mem) {
+  if (!ctx || (n && (!pos || !normal || !ao))) return fail(RKF_INVALID_ARG, "rkf_sdf_ao: null argument");
+  if (mem > RKF_MEM_DEVICE) return fail(RKF_INVALID_ARG, "rkf_sdf_ao: bad mem kind");
+  if (n == 0) return RKF_OK;
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  if (mem == RKF_MEM_DEVICE) {
+    rkf_status st = launch_ao(c, pos, normal, n, ao, c->stream);
+    if (st != RKF_OK) return st;
+    RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return RKF_OK;
+  }
+  const size_t b_in = align256(12ull * n), b_ao = align256(4ull * n);
+  rkf_status st = c->stage_bytes(2 * b_in + b_ao);
+  if (st != RKF_OK) return st;
+  char* b = c->stage.as<char>();
+  float* dp = reinterpret_cast<float*>(b);
+  float* dn = reinterpret_cast<float*>(b + b_in);
+  float* da = reinterpret_cast<float*>(b + 2 * b_in);
+  RKF_CUDA_TRY(cudaMemcpyAsync(dp, pos, 12ull * n, cudaMemcpyHostToDevice, c->stream));
+  RKF_CUDA_TRY(cudaMemcpyAsync(dn, normal, 12ull * n, cudaMemcpyHostToDevice, c->stream));
+  if ((st = launch_ao(c, dp, dn, n, da, c->stream)) != RKF_OK) return st;
+  RKF_CUDA_TRY(cudaMemcpyAsync(ao, da, 4ull * n, cudaMemcpyDeviceToHost, c->stream));
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return RKF_OK;
+}
+
 rkf_status rkf_march_batch(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views,
                            const rkf_ray_batch* batches, uint32_t n_batches,
                            const rkf_march_params* p, const rkf_batch_tuning* tuning) {

@@ -238,6 +238,25 @@ __global__ void k_import_words(const uint2* __restrict__ words, uint64_t nvox, u
   if (aos) aos[v] = w;
 }
 
+// SoA planes (f16 distance, material | secondary << 6, blend) -> the context
+// planes (+ the reference word pair, packed as VoxelSample::new_blended packs
+// it, voxel.rs:43-54).  One thread per voxel.
+__global__ void k_import_soa(const uint16_t* __restrict__ d16, const uint16_t* __restrict__ m16,
+                             const uint8_t* __restrict__ bl, uint64_t nvox, uint64_t first_vox, uint16_t* dist_f16,
+                             float* dist_f32, uint16_t* mat, uint8_t* blend, uint2* aos) {
+  const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  if (i >= nvox) return;
+  const uint64_t v = first_vox + i;
+  const uint16_t d = d16[i];
+  const uint32_t mm = m16[i] & 0xFFFu;
+  const uint8_t b = bl[i];
+  if (dist_f16) dist_f16[v] = d;
+  if (dist_f32) dist_f32[v] = __half2float(__ushort_as_half(d));
+  mat[v] = static_cast<uint16_t>(mm);
+  blend[v] = b;
+  if (aos) aos[v] = make_uint2(d | ((mm & 0x3Fu) << 16) | (((mm >> 6) & 0x3Fu) << 22), static_cast<uint32_t>(b) << 24);
+}
+
 __global__ void k_lookup(SceneDev s, uint32_t obj, const uint32_t* bxyz, uint32_t n, uint32_t* out) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -389,10 +408,59 @@ rkf_status rkf_destroy(rkf_ctx* ctx) {
   return RKF_OK;
 }
 
+namespace {
+// Tail of a pool import into slots [first_slot, first_slot + n_bricks): the u8
+// encoding when the context stores codes, then the slots leave the free list.
+rkf_status finish_pool_import(Ctx* c, uint32_t first_slot, uint32_t n_bricks) {
+  if (c->cfg.precision == RKF_PRECISION_U8) {
+    k_encode_u8<<<n_bricks, 256, 0, c->stream>>>(nullptr, c->dist_f16.as<uint16_t>(), first_slot, n_bricks,
+                                                 c->dist_u8.as<int8_t>(), c->brick_step.as<float>());
+    RKF_CUDA_TRY(cudaGetLastError());
+  }
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  std::vector<uint32_t> keep;
+  keep.reserve(c->free_slots.size());
+  for (uint32_t s : c->free_slots)
+    if (s < first_slot || s >= first_slot + n_bricks) keep.push_back(s);
+  c->used_slots += static_cast<uint32_t>(c->free_slots.size() - keep.size());
+  c->free_slots.swap(keep);
+  return RKF_OK;
+}
+}  // namespace
+
+rkf_status rkf_pool_import_soa(rkf_ctx* ctx, const uint16_t* dist_f16, const uint16_t* mat, const uint8_t* blend,
+                               uint32_t first_slot, uint32_t n_bricks) {
+  if (!ctx || (n_bricks && (!dist_f16 || !mat || !blend)))
+    return fail(RKF_INVALID_ARG, "rkf_pool_import_soa: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (c->serve) return fail(RKF_BUSY, "rkf_pool_import_soa: the context is serving");
+  if (static_cast<uint64_t>(first_slot) + n_bricks > c->capacity)
+    return fail(RKF_INVALID_ARG, "rkf_pool_import_soa: slots beyond pool capacity");
+  if (n_bricks == 0) return RKF_OK;
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  const uint64_t nvox = static_cast<uint64_t>(n_bricks) * 512;
+  const size_t b16 = (nvox * 2 + 255) & ~static_cast<size_t>(255);
+  rkf_status st = c->stage_bytes(2 * b16 + nvox);
+  if (st != RKF_OK) return st;
+  char* b = c->stage.as<char>();
+  RKF_CUDA_TRY(cudaMemcpyAsync(b, dist_f16, nvox * 2, cudaMemcpyHostToDevice, c->stream));
+  RKF_CUDA_TRY(cudaMemcpyAsync(b + b16, mat, nvox * 2, cudaMemcpyHostToDevice, c->stream));
+  RKF_CUDA_TRY(cudaMemcpyAsync(b + 2 * b16, blend, nvox, cudaMemcpyHostToDevice, c->stream));
+  const unsigned blocks = static_cast<unsigned>((nvox + 255) / 256);
+  detail::k_import_soa<<<blocks, 256, 0, c->stream>>>(
+      reinterpret_cast<const uint16_t*>(b), reinterpret_cast<const uint16_t*>(b + b16),
+      reinterpret_cast<const uint8_t*>(b + 2 * b16), nvox, static_cast<uint64_t>(first_slot) * 512,
+      c->dist_f16.as<uint16_t>(), c->dist_f32.as<float>(), c->mat.as<uint16_t>(), c->blend.as<uint8_t>(),
+      c->aos.as<uint2>());
+  RKF_CUDA_TRY(cudaGetLastError());
+  return finish_pool_import(c, first_slot, n_bricks);
+}
+
 rkf_status rkf_pool_import_voxelsample(rkf_ctx* ctx, const uint32_t* words, uint32_t first_slot,
                                        uint32_t n_bricks) {
   if (!ctx || (!words && n_bricks)) return fail(RKF_INVALID_ARG, "rkf_pool_import_voxelsample: null argument");
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (c->serve) return fail(RKF_BUSY, "rkf_pool_import_voxelsample: the context is serving");
   if (static_cast<uint64_t>(first_slot) + n_bricks > c->capacity)
     return fail(RKF_INVALID_ARG, "rkf_pool_import_voxelsample: slots beyond pool capacity");
   if (n_bricks == 0) return RKF_OK;
@@ -408,21 +476,7 @@ rkf_status rkf_pool_import_voxelsample(rkf_ctx* ctx, const uint32_t* words, uint
                                                 c->mat.as<uint16_t>(), c->blend.as<uint8_t>(),
                                                 c->aos.as<uint2>());
   RKF_CUDA_TRY(cudaGetLastError());
-  if (c->cfg.precision == RKF_PRECISION_U8) {
-    k_encode_u8<<<n_bricks, 256, 0, c->stream>>>(nullptr, c->dist_f16.as<uint16_t>(), first_slot,
-                                                 n_bricks, c->dist_u8.as<int8_t>(),
-                                                 c->brick_step.as<float>());
-    RKF_CUDA_TRY(cudaGetLastError());
-  }
-  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  // mark imported slots used (remove them from the free list)
-  std::vector<uint32_t> keep;
-  keep.reserve(c->free_slots.size());
-  for (uint32_t s : c->free_slots)
-    if (s < first_slot || s >= first_slot + n_bricks) keep.push_back(s);
-  c->used_slots += static_cast<uint32_t>(c->free_slots.size() - keep.size());
-  c->free_slots.swap(keep);
-  return RKF_OK;
+  return finish_pool_import(c, first_slot, n_bricks);
 }
 
 rkf_status rkf_pool_export_voxelsample(rkf_ctx* ctx, uint32_t first_slot, uint32_t n_bricks,

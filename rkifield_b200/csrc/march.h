@@ -46,6 +46,7 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
 rkf_status launch_trace_plain(Ctx* c, const float* o, const float* d, const float* tmax, uint32_t n,
                               uint32_t mode, const rkf_march_params* p, const rkf_hits& out,
                               cudaStream_t st);
+rkf_status launch_ao(Ctx* c, const float* pos, const float* nrm, uint32_t n, float* ao, cudaStream_t st);
 rkf_status launch_query(Ctx* c, const float* pts, uint32_t n, float* d, float* g, uint16_t* m,
                         cudaStream_t st);
 

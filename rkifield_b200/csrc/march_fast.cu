@@ -697,6 +697,38 @@ __global__ void k_query_points(SceneDev s, const float* __restrict__ pts, uint32
   }
 }
 
+// One thread per point: sdf_ao (shade_common_shading.wgsl:37-47), four taps
+// along the normal at AO_STEP_SIZE * i (0.12 m) through sample_sdf, which for
+// points inside the objects' bounds is the minimum of evaluate_object over the
+// objects (shade_common.wgsl:521-572); ao = clamp(1 - AO_STRENGTH * sum, 0, 1)
+// with AO_STRENGTH 0.7 and tap weights 1, 1/2, 1/4, 1/8.
+template <int PREC>
+__global__ void k_sdf_ao(SceneDev s, const float* __restrict__ pos, const float* __restrict__ nrm, uint32_t n,
+                         float* __restrict__ ao) {
+  extern __shared__ ObjDev sh_objs[];
+  for (uint32_t i = threadIdx.x; i < s.n_objs; i += blockDim.x) sh_objs[i] = s.objs[i];
+  __syncthreads();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  LaneCache lc;
+  const size_t i3 = 3 * static_cast<size_t>(i);
+  const float px = pos[i3], py = pos[i3 + 1], pz = pos[i3 + 2];
+  const float nx = nrm[i3], ny = nrm[i3 + 1], nz = nrm[i3 + 2];
+  float acc = 0.0f, scale = 1.0f;
+#pragma unroll 1
+  for (uint32_t k = 1; k <= 4; ++k) {
+    const float dist = __fmul_rn(0.12f, static_cast<float>(k));
+    float du;
+    uint32_t bi;
+    const float d = eval_min<PREC, false>(s, sh_objs, 0, s.n_objs, __fadd_rn(px, __fmul_rn(nx, dist)),
+                                         __fadd_rn(py, __fmul_rn(ny, dist)), __fadd_rn(pz, __fmul_rn(nz, dist)), du,
+                                         bi, lc);
+    acc = __fadd_rn(acc, __fmul_rn(scale, __fsub_rn(dist, d)));
+    scale = __fmul_rn(scale, 0.5f);
+  }
+  ao[i] = clampf(__fsub_rn(1.0f, __fmul_rn(0.7f, acc)), 0.0f, 1.0f);
+}
+
 template <int PREC>
 const void* persistent_fn(int obj) {
   if (obj == OBJ_SINGLE_EMPTY) return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_SINGLE_EMPTY>);
@@ -861,6 +893,24 @@ rkf_status launch_query(Ctx* c, const float* pts, uint32_t n, float* d, float* g
       break;
     default:
       detail::k_query_points<RKF_PRECISION_F16><<<blocks, 128, smem, st>>>(c->scene_dev(), pts, n, d, g, m);
+  }
+  RKF_CUDA_TRY(cudaGetLastError());
+  return RKF_OK;
+}
+
+rkf_status launch_ao(Ctx* c, const float* pos, const float* nrm, uint32_t n, float* ao, cudaStream_t st) {
+  if (n == 0) return RKF_OK;
+  const size_t smem = sizeof(ObjDev) * std::max<uint32_t>(1, c->obj_count());
+  const unsigned blocks = (n + 127) / 128;
+  switch (c->cfg.precision) {
+    case RKF_PRECISION_F32:
+      detail::k_sdf_ao<RKF_PRECISION_F32><<<blocks, 128, smem, st>>>(c->scene_dev(), pos, nrm, n, ao);
+      break;
+    case RKF_PRECISION_U8:
+      detail::k_sdf_ao<RKF_PRECISION_U8><<<blocks, 128, smem, st>>>(c->scene_dev(), pos, nrm, n, ao);
+      break;
+    default:
+      detail::k_sdf_ao<RKF_PRECISION_F16><<<blocks, 128, smem, st>>>(c->scene_dev(), pos, nrm, n, ao);
   }
   RKF_CUDA_TRY(cudaGetLastError());
   return RKF_OK;

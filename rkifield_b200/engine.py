@@ -89,6 +89,16 @@ class Context:
         check(self.lib.rkf_pool_import_voxelsample(self.h, _p(words), first_slot, words.size // 1024),
               "rkf_pool_import_voxelsample")
 
+    def set_brick_pool_planes(self, dist_f16: np.ndarray, mat: np.ndarray, blend: np.ndarray,
+                              first_slot: int = 0):
+        """Pool bricks as SoA planes (binary16 bits, material | secondary << 6, blend)."""
+        d = np.ascontiguousarray(dist_f16, np.uint16)
+        m = np.ascontiguousarray(mat, np.uint16)
+        b = np.ascontiguousarray(blend, np.uint8)
+        assert d.size == m.size == b.size and d.size % 512 == 0
+        check(self.lib.rkf_pool_import_soa(self.h, _p(d), _p(m), _p(b), first_slot, d.size // 512),
+              "rkf_pool_import_soa")
+
     def upload_brick_maps(self, packed: np.ndarray):
         packed = np.ascontiguousarray(packed, np.uint32)
         check(self.lib.rkf_brickmap_import(self.h, _p(packed), packed.size), "rkf_brickmap_import")
@@ -207,6 +217,15 @@ class Context:
         return d, g, m
 
     # -- edits ---------------------------------------------------------------
+    def sdf_ao(self, pos, normal) -> np.ndarray:
+        """sdf_ao at each position along its normal (host arrays)."""
+        pos = np.ascontiguousarray(pos, np.float32).ravel()
+        normal = np.ascontiguousarray(normal, np.float32).ravel()
+        assert pos.size == normal.size and pos.size % 3 == 0
+        out = np.zeros(pos.size // 3, np.float32)
+        check(self.lib.rkf_sdf_ao(self.h, _p(pos), _p(normal), out.size, _p(out), abi.RKF_MEM_HOST), "rkf_sdf_ao")
+        return out
+
     def edit(self, op: abi.rkf_edit_op) -> int:
         ep = C.c_uint64()
         check(self.lib.rkf_edit_csg(self.h, C.byref(op), C.byref(ep)), "rkf_edit_csg")

@@ -47,3 +47,41 @@ def test_small_scene_non_square_and_ragged(oracle, small_scene, small_ctx):
         got = small_ctx.march(cam, p, w, h, reference_planes=True)
         for k in PLANES:
             assert_bits_equal(got[k], ref[k], f"{k} @ {w}x{h}")
+
+
+@pytest.mark.parametrize("precision", ["f16", "u8"])
+def test_soa_import_matches_voxelsample_import(oracle, small_scene, small_ctx, precision):
+    """The same pool given as SoA planes: identical planes, reference words
+    and march (f16), and the same u8 codes as the word import (u8)."""
+    from rkifield_b200 import scenes
+    from rkifield_b200.engine import Context
+    v = small_scene["vox"]
+    w = v.words.reshape(-1, 2)
+    d16 = (w[:, 0] & 0xFFFF).astype(np.uint16)
+    mat = (((w[:, 0] >> 16) & 0x3F) | (((w[:, 0] >> 22) & 0x3F) << 6)).astype(np.uint16)
+    blend = (w[:, 1] >> 24).astype(np.uint8)
+    cap = v.n_bricks + 1024
+    a = Context(pool_capacity=cap, precision=precision)
+    b = Context(pool_capacity=cap, precision=precision)
+    try:
+        for ctx in (a, b):
+            ctx.upload_brick_maps(v.map)
+        a.set_brick_pool_planes(d16, mat, blend)
+        b.set_brick_pool(v.words)
+        for ctx in (a, b):
+            ctx.upload_objects([small_scene["obj"]])
+        pa, pb = a.export_planes(0, v.n_bricks), b.export_planes(0, v.n_bricks)
+        for k in pa:
+            assert_bits_equal(pa[k], pb[k], f"{precision} plane {k}")
+        assert a.info()["pool_bricks_used"] == b.info()["pool_bricks_used"] == v.n_bricks
+        if precision == "f16":
+            assert_bits_equal(a.export_pool(0, v.n_bricks), v.words, "reference words rebuilt from planes")
+        spec = small_scene["spec"]
+        cam = scenes.seeded_camera(spec, 128, 128, seed=17)
+        p = scenes.march_params(spec)
+        ga, gb = a.march(cam, p, 128, 128, reference_planes=True), b.march(cam, p, 128, 128, reference_planes=True)
+        for k in PLANES:
+            assert_bits_equal(ga[k], gb[k], f"{precision} march {k}")
+    finally:
+        a.close()
+        b.close()

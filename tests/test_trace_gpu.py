@@ -121,3 +121,32 @@ def test_batch_equals_separate_calls(small_scene, small_ctx):
         for h, r in zip(hb, ray_ref):
             for k in h:
                 assert_bits_equal(h[k].download(), r[k], f"rays {k} tuning {tu}")
+
+
+def test_sdf_ao_bit_exact(oracle, small_scene, small_ctx):
+    """sdf_ao (shade_common_shading.wgsl:37-47) at hit points offset by
+    SHADOW_BIAS along their normals, as the shading pass calls it, and at
+    random points of the scene box."""
+    from rkifield_b200 import scenes
+    v = small_scene["vox"]
+    sc = oracle.Scene([small_scene["obj"]], pool_words=v.words, brick_maps=v.map)
+    spec = small_scene["spec"]
+    cam = scenes.seeded_camera(spec, 160, 120, seed=41)
+    g = small_ctx.march(cam, scenes.march_params(spec), 160, 120, reference_planes=True)
+    hit = (g["flags"] & 1) != 0
+    assert hit.sum() > 500
+    n = g["normal"].reshape(-1, 3)[hit]
+    pos = g["position"].reshape(-1, 4)[hit, :3]
+    pos = (pos + (n * np.float32(0.08)).astype(np.float32)).astype(np.float32)
+    rng = np.random.default_rng(9)
+    lo = np.array(small_scene["vp"].aabb_min[:], np.float32)
+    hi = np.array(small_scene["vp"].aabb_max[:], np.float32)
+    rp = rng.uniform(lo, hi, size=(4000, 3)).astype(np.float32)
+    rn = rng.normal(size=(4000, 3))
+    rn = (rn / np.linalg.norm(rn, axis=1, keepdims=True)).astype(np.float32)
+    P = np.concatenate([pos, rp]).astype(np.float32)
+    N = np.concatenate([n, rn]).astype(np.float32)
+    ref = oracle.sdf_ao(sc, P, N)
+    got = small_ctx.sdf_ao(P, N)
+    assert ((ref > 0.0) & (ref < 1.0)).sum() > 100, "AO should vary"
+    assert_bits_equal(got, ref, "sdf_ao")
