@@ -25,6 +25,7 @@
 
 #include "ctx.h"
 #include "march.h"
+#include "f32x2.cuh"
 #include "sampler.cuh"
 
 namespace rkf {
@@ -231,6 +232,52 @@ __device__ __forceinline__ uint32_t empty_run(const ObjDev& o, const uint8_t* __
   return c;
 }
 
+// empty_run<PLAIN=true, CLEAN=true> with the x and y chains of a step packed
+// into two-wide FP32 instructions (z stays scalar): the same operations on
+// the same values, so the same bits.
+template <bool INRUN>
+__device__ __forceinline__ uint32_t empty_run_x2(const ObjDev& o, const uint8_t* __restrict__ field, float ox,
+                                                 float oy, float oz, float dx, float dy, float dz, float tmax,
+                                                 uint32_t n, float& t, float& box_t, float& prev_t,
+                                                 float& prev_dist, bool& stop_full) {
+  uint32_t c = 0;
+  float lim = fminf(box_t, tmax);
+  stop_full = false;
+  const f2 o01 = f2_pack(ox, oy), d01 = f2_pack(dx, dy), h01 = f2_pack(o.half_gs[0], o.half_gs[1]);
+  const f2 r2 = f2_pack(o.rcp_vs, o.rcp_vs), nvs2 = f2_pack(-o.vs, -o.vs), half2 = f2_pack(0.5f, 0.5f);
+  const float hz = o.half_gs[2], vs = o.vs, rcp = o.rcp_vs, be = o.be;
+#pragma unroll 2
+  for (; c < n; ++c) {
+    if (t > lim) {
+      if (!INRUN || t > tmax) {
+        stop_full = t > tmax;
+        break;
+      }
+      box_t = probe_empty(o, field, ox, oy, oz, dx, dy, dz, t);
+      lim = fminf(box_t, tmax);
+      if (t > lim) {
+        stop_full = true;
+        break;
+      }
+    }
+    // grid coordinate (o + d*t) + half; exact quotient by vs (q0 + (g - q0*vs)*rcp,
+    // with -vs so that the FMA adds); minus 0.5
+    const f2 g01 = f2_add(f2_add(o01, f2_mul(d01, f2_pack(t, t))), h01);
+    const f2 q0 = f2_mul(g01, r2);
+    const f2 v01 = f2_sub(f2_fma(f2_fma(q0, nvs2, g01), r2, q0), half2);
+    const float vz = __fsub_rn(exact_div_vs(__fadd_rn(__fadd_rn(oz, __fmul_rn(dz, t)), hz), vs, rcp), 0.5f);
+    float vx, vy;
+    f2_unpack(v01, vx, vy);
+    float tx, ty;
+    f2_unpack(f2_sub(v01, f2_pack(floorf(vx), floorf(vy))), tx, ty);
+    const float d = mix3_const(be, tx, ty, __fsub_rn(vz, floorf(vz)));
+    prev_t = t;
+    prev_dist = d;
+    t = __fadd_rn(t, d);
+  }
+  return c;
+}
+
 template <int PREC, int OBJ>
 __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_constant__ KParams kp) {
   constexpr bool SINGLE = OBJ != OBJ_MULTI;
@@ -373,7 +420,10 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
   empty_run<P, CL, IN>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n, brk, near_thr, min_step, max_near, t, \
                        box_t, prev_t, prev_dist, near, stop_full)
             if (kp.plain_obj && clean)
-              c = kp.run_probe ? RKF_RUN(true, true, true) : RKF_RUN(true, true, false);
+              c = kp.run_probe ? empty_run_x2<true>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n, t, box_t,
+                                                    prev_t, prev_dist, stop_full)
+                               : empty_run_x2<false>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n, t, box_t,
+                                                     prev_t, prev_dist, stop_full);
             else if (kp.plain_obj)
               c = kp.run_probe ? RKF_RUN(true, false, true) : RKF_RUN(true, false, false);
             else
