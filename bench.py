@@ -55,10 +55,14 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-sectors", action="store_true")
+    ap.add_argument("--extras", action=argparse.BooleanOptionalAction, default=True,
+                    help="also time the 960x540 view and the f32 / u8 planes")
     ap.add_argument("--cb-views", type=int, default=64, help="views in the batching workload (0 = skip)")
     ap.add_argument("--cb-steps", type=int, default=3)
     ap.add_argument("--cs-requests", type=int, default=600, help="requests in the serving run (0 = skip)")
     ap.add_argument("--cs-rate", type=float, default=2000.0)
+    ap.add_argument("--cs-sat-rate", type=float, default=50000.0,
+                    help="arrival rate of a second serving run that saturates the loop (0 = skip)")
     ap.add_argument("--cs-budget", type=int, default=8192, help="serving memory budget, MiB")
     ap.add_argument("--pool-bricks", type=int, default=0, help="brick slots to reserve (0 = default)")
     ap.add_argument("--no-reference-pool", action="store_true",
@@ -384,14 +388,15 @@ def _pinned_copy(arrs, keep):
     return out
 
 
-def run_serving(args, spec, prims, p, local):
+def run_serving(args, spec, prims, p, local, rate=None, with_plain=True):
     """Poisson request stream through the serving loop vs plain per-request
     launches of the same requests."""
     import ctypes as C
 
     from rkifield_b200 import cudart, engine, workloads
     from rkifield_b200.engine import Context, RkfError, Server
-    reqs = workloads.make_request_stream(spec, prims, args.cs_requests, seed=500, rate_hz=args.cs_rate)
+    rate = rate or args.cs_rate
+    reqs = workloads.make_request_stream(spec, prims, args.cs_requests, seed=500, rate_hz=rate)
     keep = []
     # page-locked inputs and outputs for every request
     bufs = []
@@ -462,6 +467,8 @@ def run_serving(args, spec, prims, p, local):
     served = {"value": total_rays / wall / 1e6, "unit": "Mrays/s", "points_per_s": total_pts / wall,
               "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
               "busy_retries": busy, "wall_s": wall}
+    if not with_plain:
+        return {"requests": len(reqs), "rate_hz": rate, "served": served}
 
     # ---- plain: one launch per request, in arrival order, one at a time --------
     # device buffers are allocated once (the largest request); each request
@@ -509,7 +516,7 @@ def run_serving(args, spec, prims, p, local):
     plain_wall = sum(service)
     plain = {"value": total_rays / plain_wall / 1e6, "unit": "Mrays/s", "points_per_s": total_pts / plain_wall,
              "latency_ms": {"p50": float(np.percentile(lat_p, 50)), "p99": float(np.percentile(lat_p, 99))}}
-    return {"requests": len(reqs), "rate_hz": args.cs_rate, "rays": total_rays, "points": total_pts,
+    return {"requests": len(reqs), "rate_hz": rate, "rays": total_rays, "points": total_pts,
             "edits": sum(1 for r in reqs if r.kind == 3), "served": served, "plain_per_request": plain,
             "vs_plain": served["value"] / plain["value"]}
 
@@ -601,6 +608,52 @@ def run_precision_report(args):
     print(json.dumps({"report": "precision", **report}), flush=True)
 
 
+def time_view(ctx, cam, p, w, h, stream, steps, plain=False):
+    """Mean CUDA-event ms of one view march (untimed warm-up first)."""
+    from rkifield_b200 import cudart
+    g = cudart.device_gbuffer(w * h)
+    gp = cudart.gbuffer_ptrs(g)
+    ctx.march_async(cam, p, w, h, gp, stream.ptr, plain=plain)
+    ms = []
+    for _ in range(steps):
+        a, b = cudart.Event(), cudart.Event()
+        a.record(stream)
+        ctx.march_async(cam, p, w, h, gp, stream.ptr, plain=plain)
+        b.record(stream)
+        stream.synchronize()
+        ms.append(a.elapsed_ms(b))
+    return float(np.mean(ms))
+
+
+def run_extras(args, spec, prims, p, ctx, stream):
+    """Secondary figures: the 960x540 view, and the headline view over the f32
+    and u8 distance planes (same scene, separate contexts)."""
+    from rkifield_b200.engine import Context
+    out = {}
+    w, h = 960, 540
+    cam = camera_for(spec, w, h, 0)
+    b = time_view(ctx, cam, p, w, h, stream, 5)
+    v = {"b200_mrays": w * h / b / 1e3, "b200_ms": b}
+    if not args.no_plain:
+        pl = time_view(ctx, cam, p, w, h, stream, 2, plain=True)
+        v.update(plain_mrays=w * h / pl / 1e3, plain_ms=pl, vs_plain=pl / b)
+    out["view_960x540"] = v
+    prec = {}
+    cam = camera_for(spec, args.width, args.height, 0)
+    n = args.width * args.height
+    for name in ("f32", "u8"):
+        c2 = Context(pool_capacity=ctx.info()["pool_bricks_used"] + 4096, precision=name, keep_reference_pool=False)
+        try:
+            c2.voxelize(prims, scenes.voxelize_params(spec, prims))
+            ms = time_view(c2, cam, p, args.width, args.height, stream, 5)
+            prec[name] = {"mrays": n / ms / 1e3, "ms": ms}
+        finally:
+            c2.close()
+    out["precision_views"] = prec
+    out["note"] = "CUDA-event means without the L2 flush of the headline steps"
+    return out
+
+
 def run_b200(args, world, rank, local, dist):
     from rkifield_b200 import cudart
     from rkifield_b200.engine import Context, gbuffer_host
@@ -678,12 +731,21 @@ def run_b200(args, world, rank, local, dist):
     d2h = sum(v.nbytes for v in host_out.values())
     h2d = 144 + 32  # camera uniforms + march parameters
 
+    extras = None
+    if args.extras and rank == 0:
+        extras = run_extras(args, spec, prims, p, ctx, stream)
     batching = None
     if args.cb_views > 0:
         batching = run_batching(ctx, spec, prims, p, args, stream)
     serving = None
     if args.cs_requests > 0 and rank == 0:
         serving = run_serving(args, spec, prims, p, local)
+        if args.cs_sat_rate > 0:
+            # the same requests arriving faster than they can be served:
+            # throughput at capacity instead of at the offered load
+            sat = run_serving(args, spec, prims, p, local, rate=args.cs_sat_rate, with_plain=False)
+            sat["vs_plain"] = sat["served"]["value"] / serving["plain_per_request"]["value"]
+            serving["saturated"] = sat
 
     out = None
     if rank == 0:
@@ -719,8 +781,12 @@ def run_b200(args, world, rank, local, dist):
             if not args.no_cpu:
                 rows = sample_rows(h, args.cpu_rows)
                 rate, nr, dt = cpu_march_rate(oracle, sc, cam, p, w, h, rows, threads)
+                rows1 = sample_rows(h, 2)
+                rate1, nr1, dt1 = cpu_march_rate(oracle, sc, cam, p, w, h, rows1, 1)
                 cpu = {"value": rate, "unit": "Mrays/s", "cores": threads, "kind": "port",
-                       "sample": f"{len(rows)} rows x {w} px ({nr} rays) of the same view, {dt:.1f} s"}
+                       "sample": f"{len(rows)} rows x {w} px ({nr} rays) of the same view, {dt:.1f} s",
+                       "single_core": {"value": rate1, "unit": "Mrays/s", "cores": 1,
+                                       "sample": f"{len(rows1)} rows x {w} px ({nr1} rays), {dt1:.1f} s"}}
         out = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": float(np.mean(ms)), "higher_is_better": True,
@@ -736,6 +802,7 @@ def run_b200(args, world, rank, local, dist):
             "vs_plain": (value / plain["value"]) if plain else None,
             "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roof,
+            "extras": extras,
             "batching": batching,
             "serving": serving,
             "cpu_baseline": cpu,

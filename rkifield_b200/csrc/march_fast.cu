@@ -60,6 +60,8 @@ struct KParams {
   uint32_t refill_active;  // leave the march loop once at most this many lanes march
   uint32_t run_probe;      // empty-space path: probe the next cube inside a run
   float empty_lo;          // empty-space path: lower bound of every EMPTY value
+  float empty_lo_t, empty_hi;  // empty-space path: tight bounds of an EMPTY step
+  uint32_t settle_links;   // empty-space path: cubes a settling chain may add (0 = off)
 };
 
 // Object set of a launch: several objects, exactly one, or exactly one that
@@ -93,15 +95,20 @@ __device__ __forceinline__ float empty_value(const ObjDev& o, float gx, float gy
 // trilinear corners of the sample at t' lie in the cube: the sample there is
 // exactly empty_value().  Positions are monotone in t along each axis, so
 // checking the exit faces suffices.
-__device__ float probe_empty(const ObjDev& o, const uint8_t* __restrict__ field, float ox, float oy,
-                             float oz, float dx, float dy, float dz, float t) {
+//
+// probe_cube is the general form: the cube is the one around the block of the
+// position at t_probe, and the interval it vouches for starts at t_anchor
+// (whose position must lie in the shrunk cube): [t_anchor, result].
+__device__ float probe_cube(const ObjDev& o, const uint8_t* __restrict__ field, float ox, float oy, float oz,
+                            float dx, float dy, float dz, float t_anchor, float t_probe) {
   const float o3[3] = {ox, oy, oz}, d3[3] = {dx, dy, dz};
   int k[3];
   float p[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    p[a] = __fadd_rn(o3[a], __fmul_rn(d3[a], t));
-    const float g = __fadd_rn(__fadd_rn(p[a], o.m[12 + a]), o.half_gs[a]);
+    p[a] = __fadd_rn(o3[a], __fmul_rn(d3[a], t_anchor));
+    const float pp = t_probe == t_anchor ? p[a] : __fadd_rn(o3[a], __fmul_rn(d3[a], t_probe));
+    const float g = __fadd_rn(__fadd_rn(pp, o.m[12 + a]), o.half_gs[a]);
     const float f = floorf(__fsub_rn(exact_div_vs(g, o.vs, o.rcp_vs), 0.5f));
     if (!(f >= 0.0f && f <= static_cast<float>(o.tv[a] - 2))) return -1.0f;
     k[a] = static_cast<int>(f) >> 6;
@@ -128,6 +135,30 @@ __device__ float probe_empty(const ObjDev& o, const uint8_t* __restrict__ field,
     else if (d3[a] < 0.0f) t_exit = fminf(t_exit, (wlo - o3[a]) / d3[a]);
   }
   return t_exit;
+}
+
+__device__ __forceinline__ float probe_empty(const ObjDev& o, const uint8_t* __restrict__ field, float ox,
+                                             float oy, float oz, float dx, float dy, float dz, float t) {
+  return probe_cube(o, field, ox, oy, oz, dx, dy, dz, t, t);
+}
+
+// Extend an interval [t, cover] of EMPTY-cube positions along the ray through
+// at most `links` further cubes, until it reaches `need`.  The next cube is
+// the one around the block half a block ahead of the current end (else around
+// the end's own block) and must contain the current end, so the union stays
+// one interval.  Returns the new end.
+__device__ float extend_cover(const ObjDev& o, const uint8_t* __restrict__ field, float ox, float oy, float oz,
+                              float dx, float dy, float dz, float cover, float need, uint32_t links) {
+  const float ahead = 32.0f * o.vs;
+  for (uint32_t i = 0; i < links && cover < need; ++i) {
+    float nx = probe_cube(o, field, ox, oy, oz, dx, dy, dz, cover, cover + ahead);
+    if (!(nx > cover)) {
+      nx = probe_cube(o, field, ox, oy, oz, dx, dy, dz, cover, cover);
+      if (!(nx > cover)) break;
+    }
+    cover = nx;
+  }
+  return cover;
 }
 
 __device__ __forceinline__ uint32_t find_segment(const Segment* segs, uint32_t nseg, uint64_t id) {
@@ -402,20 +433,48 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
         const ObjDev& o0 = sh_objs[0];
         const bool sh = state == ST_SHADOW;
         const float dx = sh ? rdx : qdx, dy = sh ? rdy : qdy, dz = sh ? rdz : qdz;
-        if (t > box_t && prev_dist >= kp.probe_min)
+        const uint32_t max_step = sh ? 256u : p.hard_max_steps;
+        const uint32_t max_near = sh ? 32u : p.scene.max_steps;
+        // a sample below brk goes to the full step, which decides it
+        const float brk = sh ? 0.02f : fmaxf(hit_thr, 0.0f);
+        const float near_thr = sh ? -1.0f : p.near_surface_threshold;
+        const float min_step = sh ? 0.005f : p.min_step;
+        const bool clean = kp.empty_lo >= brk && kp.empty_lo >= near_thr && kp.empty_lo >= min_step;
+        if (t > box_t && prev_dist >= kp.probe_min) {
           box_t = probe_empty(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, t);
-        if (t <= box_t) {
-          const uint32_t max_step = sh ? 256u : p.hard_max_steps;
-          const uint32_t max_near = sh ? 32u : p.scene.max_steps;
+          if (t <= box_t && clean && kp.settle_links && step < max_step && near < max_near) {
+            // Settle the ray if every sample it has left is the EMPTY value:
+            // then no threshold acts on it, it misses, and its outputs do not
+            // depend on its exact t.  t after k more steps lies in
+            // [t + k*lo, t + k*hi] widened by one rounding (2^-24) per step;
+            // 2^-22 per step (and 4 more) leaves room for this bound's own
+            // rounding.  The last sample is the (max_step-step-1)th ahead; the
+            // ray runs out of steps if even its largest t stays <= tmax, and
+            // ends past tmax (with no step flag) if even its smallest t exceeds
+            // tmax.  Either way, when EMPTY cubes cover every position up to
+            // that bound (or tmax), the outcome is settled.
+            const float k = static_cast<float>(max_step - step - 1);
+            const float grow = (k + 4.0f) * 2.384185791015625e-7f;
+            const float t_hi = (t + k * kp.empty_hi) * (1.0f + grow);
+            const float t_lo = (t + k * kp.empty_lo_t) * (1.0f - grow);
+            const bool out_of_steps = t_hi <= tmax;
+            if (out_of_steps || t_lo > tmax) {
+              const float need = out_of_steps ? t_hi : tmax;
+              box_t = extend_cover(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, box_t, need, kp.settle_links);
+              if (box_t >= need) {
+                if (sh) cs.shadow = clampf(cs.shadow, 0.0f, 1.0f);
+                else if (out_of_steps) step = max_step;
+                cs.hit = false;
+                state = ST_EPI;
+              }
+            }
+          }
+        }
+        if (state != ST_EPI && t <= box_t) {
           const uint32_t n = step < max_step ? min(kp.budget, max_step - step) : 0u;
-          // a sample below brk goes to the full step, which decides it
-          const float brk = sh ? 0.02f : fmaxf(hit_thr, 0.0f);
-          const float near_thr = sh ? -1.0f : p.near_surface_threshold;
-          const float min_step = sh ? 0.005f : p.min_step;
           uint32_t c = 0;
           bool stop_full = true;
           if (near < max_near) {
-            const bool clean = kp.empty_lo >= brk && kp.empty_lo >= near_thr && kp.empty_lo >= min_step;
 #define RKF_RUN(P, CL, IN)                                                                                   \
   empty_run<P, CL, IN>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n, brk, near_thr, min_step, max_near, t, \
                        box_t, prev_t, prev_dist, near, stop_full)
@@ -834,6 +893,10 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   // mix(c, c, t) three times stays within 12 roundings of c (relative 2^-24
   // each); 0.999 leaves a wide margin
   kp.empty_lo = obj == detail::OBJ_SINGLE_EMPTY ? 0.999f * kp.objs[0].be * kp.objs[0].min_scale : 0.0f;
+  // twelve roundings of 2^-24 stay far inside 2^-16
+  kp.empty_lo_t = kp.objs[0].be * kp.objs[0].min_scale * (1.0f - 1.52587890625e-5f);
+  kp.empty_hi = kp.objs[0].be * kp.objs[0].min_scale * (1.0f + 1.52587890625e-5f);
+  kp.settle_links = obj == detail::OBJ_SINGLE_EMPTY ? 48u : 0u;
   kp.plain_obj = (kp.objs[0].m[12] == 0.0f && kp.objs[0].m[13] == 0.0f && kp.objs[0].m[14] == 0.0f &&
                   kp.objs[0].min_scale == 1.0f)
                      ? 1u
@@ -897,6 +960,10 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
   // mix(c, c, t) three times stays within 12 roundings of c (relative 2^-24
   // each); 0.999 leaves a wide margin
   kp.empty_lo = obj == detail::OBJ_SINGLE_EMPTY ? 0.999f * kp.objs[0].be * kp.objs[0].min_scale : 0.0f;
+  // twelve roundings of 2^-24 stay far inside 2^-16
+  kp.empty_lo_t = kp.objs[0].be * kp.objs[0].min_scale * (1.0f - 1.52587890625e-5f);
+  kp.empty_hi = kp.objs[0].be * kp.objs[0].min_scale * (1.0f + 1.52587890625e-5f);
+  kp.settle_links = obj == detail::OBJ_SINGLE_EMPTY ? 48u : 0u;
   kp.plain_obj = (kp.objs[0].m[12] == 0.0f && kp.objs[0].m[13] == 0.0f && kp.objs[0].m[14] == 0.0f &&
                   kp.objs[0].min_scale == 1.0f)
                      ? 1u
