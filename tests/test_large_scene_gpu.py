@@ -2,8 +2,10 @@
 2 cm on the device (about 1.1 M bricks), one 1920x1080 view from inside the
 grid.  Sampled rows are compared bit for bit with the FP32 oracle reading
 the same pool planes and index, and the whole frame is checked for
-properties that need no oracle: the batched and single-view entry points
-agree, and a repeat of the march is identical."""
+properties that need no oracle: a repeat of the march is identical.  Ray
+batches whose tmax falls around the distance a ray covers in its step budget
+exercise both ways a miss can end (out of steps, or past tmax) where the march
+settles rays without stepping them."""
 import numpy as np
 import pytest
 
@@ -29,15 +31,21 @@ def large():
     ctx.close()
 
 
-def test_large_view_sampled_rows_bit_exact(oracle, large):
-    ctx, spec, cam, p = large
-    got = ctx.march(cam, p, W, H, reference_planes=True)
+@pytest.fixture(scope="module")
+def large_oracle(oracle, large):
+    ctx = large[0]
     n = ctx.info()["pool_bricks_used"]
     assert n > 1_000_000
     pl = ctx.export_planes(0, n)
     idx = ctx.export_index()
-    sc = oracle.Scene([ctx.object(0)], top=idx["top"], leaves=idx["leaves"], obj_top_info=idx["obj_top_info"],
-                      dist_f16=pl["dist"], mat_plane=pl["mat"], blend_plane=pl["blend"])
+    return oracle.Scene([ctx.object(0)], top=idx["top"], leaves=idx["leaves"], obj_top_info=idx["obj_top_info"],
+                        dist_f16=pl["dist"], mat_plane=pl["mat"], blend_plane=pl["blend"])
+
+
+def test_large_view_sampled_rows_bit_exact(oracle, large, large_oracle):
+    ctx, spec, cam, p = large
+    got = ctx.march(cam, p, W, H, reference_planes=True)
+    sc = large_oracle
     rows = [0, 137, 389, 540, 541, 777, 1023, 1079]
     hits = 0
     for r in rows:
@@ -59,3 +67,27 @@ def test_large_view_repeat_identical(large):
     flags = a["flags"]
     # most rays run out of steps in empty space; some hit
     assert (flags & 1).sum() > 10_000
+
+
+def test_large_rays_around_the_step_budget_bit_exact(oracle, large, large_oracle):
+    """Rays from inside the cube with tmax near the distance 1024 steps of
+    EMPTY space cover (about 164 m): some run out of steps, some pass tmax,
+    some are too close to call and are stepped; shadow rays with long tmax."""
+    from rkifield_b200 import _abi as abi
+    ctx, spec, cam, p = large
+    rng = np.random.default_rng(12)
+    n = 6000
+    o = rng.uniform(-60.0, 60.0, size=(n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    span = np.float32(1024 * 8 * spec.voxel_size)
+    tmax = (span * rng.uniform(0.97, 1.03, n)).astype(np.float32)
+    tmax[:200] = span  # on the boundary itself
+    for mode in (abi.RKF_TRACE_CLOSEST, abi.RKF_TRACE_ANY, abi.RKF_TRACE_SHADOW):
+        ref = oracle.trace(large_oracle, o.ravel(), d.ravel(), tmax, mode, p)
+        got = ctx.trace(o.ravel(), d.ravel(), tmax, mode, p)
+        for k in ("t", "flags"):
+            assert_bits_equal(got[k], ref[k], f"mode {mode} {k}")
+        if mode == abi.RKF_TRACE_CLOSEST:
+            steps_out = (ref["flags"] & 4) != 0
+            assert steps_out.sum() > 200 and (ref["flags"] == 0).sum() > 200, "both miss endings must occur"
