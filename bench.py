@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--cs-rate", type=float, default=2000.0)
     ap.add_argument("--cs-sat-rate", type=float, default=50000.0,
                     help="arrival rate of a second serving run that saturates the loop (0 = skip)")
-    ap.add_argument("--cs-budget", type=int, default=8192, help="serving memory budget, MiB")
+    ap.add_argument("--cs-budget", type=int, default=32768, help="serving memory budget, MiB")
     ap.add_argument("--pool-bricks", type=int, default=0, help="brick slots to reserve (0 = default)")
     ap.add_argument("--no-reference-pool", action="store_true",
                     help="keep no AoS reference pool (implies --no-plain; smaller device footprint)")
@@ -424,7 +424,7 @@ def run_serving(args, spec, prims, p, local, rate=None, with_plain=True):
 
     # ---- served ----------------------------------------------------------------
     ctx = Context(device=local, pool_capacity=LARGE_POOL, mem_budget_bytes=args.cs_budget << 20,
-                  max_inflight=256)
+                  max_inflight=1024)
     ctx.voxelize(prims, scenes.voxelize_params(spec, prims))
     srv = Server(ctx, p)
     t0 = time.perf_counter()

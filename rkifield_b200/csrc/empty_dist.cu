@@ -48,7 +48,6 @@ __global__ void k_empty_dist_axis(const uint8_t* __restrict__ in, uint8_t* __res
   const uint64_t n = static_cast<uint64_t>(g.nx) * g.ny * g.nz;
   const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const uint32_t x = static_cast<uint32_t>(i % g.nx);
   const uint32_t y = static_cast<uint32_t>((i / g.nx) % g.ny);
   const uint32_t z = static_cast<uint32_t>(i / (static_cast<uint64_t>(g.nx) * g.ny));
   const uint32_t pos = axis == 1 ? y : z;

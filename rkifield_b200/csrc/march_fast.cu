@@ -87,59 +87,77 @@ __device__ __forceinline__ float empty_value(const ObjDev& o, float gx, float gy
   return __fmul_rn(v, o.min_scale);
 }
 
-// Largest t up to which the ray o + d*t stays inside a cube of EMPTY blocks
-// around its position at t (from the empty-space distance field), clipped to
-// the grid and the geometry box; -1 when the position is not in an EMPTY
-// block.  The cube is shrunk by a margin that covers every rounding between
-// t and the sampler's grid coordinate, so for each t' in [t, result] the
-// trilinear corners of the sample at t' lie in the cube: the sample there is
-// exactly empty_value().  Positions are monotone in t along each axis, so
-// checking the exit faces suffices.
-//
-// probe_cube is the general form: the cube is the one around the block of the
-// position at t_probe, and the interval it vouches for starts at t_anchor
-// (whose position must lie in the shrunk cube): [t_anchor, result].
-__device__ float probe_cube(const ObjDev& o, const uint8_t* __restrict__ field, float ox, float oy, float oz,
-                            float dx, float dy, float dz, float t_anchor, float t_probe) {
-  const float o3[3] = {ox, oy, oz}, d3[3] = {dx, dy, dz};
+// A ray as the EMPTY-cube probes see it: origin and step direction, the
+// direction's reciprocals (for the exit times) and the containment margin:
+// 0.1 voxel plus 2^-18 of the magnitudes involved, which covers every
+// rounding between t and the sampler's grid coordinate and every rounding of
+// the cube's faces and exit times computed here.
+struct ProbeRay {
+  float o[3], d[3], inv[3], margin;
+};
+
+__device__ __forceinline__ ProbeRay probe_ray(const ObjDev& ob, float ox, float oy, float oz, float dx, float dy,
+                                              float dz) {
+  ProbeRay r;
+  r.o[0] = ox, r.o[1] = oy, r.o[2] = oz;
+  r.d[0] = dx, r.d[1] = dy, r.d[2] = dz;
+  float mag = 1.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    r.inv[a] = __frcp_rn(r.d[a]);
+    mag += fabsf(r.o[a]) + fabsf(ob.m[12 + a]) + ob.gs[a];
+  }
+  r.margin = 0.1f * ob.vs + mag * 3.814697265625e-6f;
+  return r;
+}
+
+// Largest t up to which the ray stays inside a cube of EMPTY blocks (from the
+// empty-space distance field), clipped to the grid and the geometry box, and
+// shrunk by the ray's margin: for each t' in [t_anchor, result] the trilinear
+// corners of the sample at t' lie in the cube, so the sample there is exactly
+// empty_value().  The cube is the one around the block of the position at
+// t_probe; which block that is only chooses the cube (its EMPTY-ness holds for
+// any block), so it is found with plain arithmetic, while the position at
+// t_anchor -- rounded exactly as the march rounds it -- must lie in the shrunk
+// cube.  Positions are monotone in t along each axis, so the exit faces
+// suffice.  -1 when there is no such cube.
+__device__ float probe_cube(const ObjDev& o, const uint8_t* __restrict__ field, const ProbeRay& r, float t_anchor,
+                            float t_probe) {
   int k[3];
   float p[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    p[a] = __fadd_rn(o3[a], __fmul_rn(d3[a], t_anchor));
-    const float pp = t_probe == t_anchor ? p[a] : __fadd_rn(o3[a], __fmul_rn(d3[a], t_probe));
-    const float g = __fadd_rn(__fadd_rn(pp, o.m[12 + a]), o.half_gs[a]);
-    const float f = floorf(__fsub_rn(exact_div_vs(g, o.vs, o.rcp_vs), 0.5f));
-    if (!(f >= 0.0f && f <= static_cast<float>(o.tv[a] - 2))) return -1.0f;
+    p[a] = __fadd_rn(r.o[a], __fmul_rn(r.d[a], t_anchor));
+    const float pp = r.o[a] + r.d[a] * t_probe;
+    const float f = floorf((pp + o.m[12 + a] + o.half_gs[a]) * o.rcp_vs - 0.5f);
+    if (!(f >= 0.0f && f <= static_cast<float>(o.tv[a] - 1))) return -1.0f;
     k[a] = static_cast<int>(f) >> 6;
   }
   const uint32_t s = __ldg(field + o.top_off + k[0] + k[1] * o.tdim[0] + k[2] * o.tdim[0] * o.tdim[1]);
   if (s == 0) return -1.0f;
-  const int r = static_cast<int>(s) - 1;  // every block within r is EMPTY
-  float mag = 1.0f;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) mag += fabsf(o3[a]) + fabsf(o.m[12 + a]) + o.gs[a];
-  const float margin = 0.1f * o.vs + mag * 3.814697265625e-6f;  // 0.1 voxel + mag * 2^-18
+  const int rad = static_cast<int>(s) - 1;  // every block within rad is EMPTY
   float t_exit = kMaxFloat;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const int lo_v = max(0, (k[a] - r) * 64), hi_v = min(o.tv[a] - 1, (k[a] + r) * 64 + 63);
-    float wlo = (static_cast<float>(lo_v) + 0.5f) * o.vs - o.half_gs[a] - o.m[12 + a] + margin;
-    float whi = (static_cast<float>(hi_v) + 0.5f) * o.vs - o.half_gs[a] - o.m[12 + a] - margin;
+    const int lo_v = max(0, (k[a] - rad) * 64), hi_v = min(o.tv[a] - 1, (k[a] + rad) * 64 + 63);
+    const float base = -o.half_gs[a] - o.m[12 + a];
+    float wlo = (static_cast<float>(lo_v) + 0.5f) * o.vs + base + r.margin;
+    float whi = (static_cast<float>(hi_v) + 0.5f) * o.vs + base - r.margin;
     if (o.has_geom) {
-      wlo = fmaxf(wlo, o.gmin[a] - o.m[12 + a] + margin);
-      whi = fminf(whi, o.gmax[a] - o.m[12 + a] - margin);
+      wlo = fmaxf(wlo, o.gmin[a] - o.m[12 + a] + r.margin);
+      whi = fminf(whi, o.gmax[a] - o.m[12 + a] - r.margin);
     }
     if (!(p[a] >= wlo && p[a] <= whi)) return -1.0f;
-    if (d3[a] > 0.0f) t_exit = fminf(t_exit, (whi - o3[a]) / d3[a]);
-    else if (d3[a] < 0.0f) t_exit = fminf(t_exit, (wlo - o3[a]) / d3[a]);
+    if (r.d[a] > 0.0f) t_exit = fminf(t_exit, (whi - r.o[a]) * r.inv[a]);
+    else if (r.d[a] < 0.0f) t_exit = fminf(t_exit, (wlo - r.o[a]) * r.inv[a]);
   }
   return t_exit;
 }
 
 __device__ __forceinline__ float probe_empty(const ObjDev& o, const uint8_t* __restrict__ field, float ox,
                                              float oy, float oz, float dx, float dy, float dz, float t) {
-  return probe_cube(o, field, ox, oy, oz, dx, dy, dz, t, t);
+  const ProbeRay r = probe_ray(o, ox, oy, oz, dx, dy, dz);
+  return probe_cube(o, field, r, t, t);
 }
 
 // Extend an interval [t, cover] of EMPTY-cube positions along the ray through
@@ -149,11 +167,12 @@ __device__ __forceinline__ float probe_empty(const ObjDev& o, const uint8_t* __r
 // one interval.  Returns the new end.
 __device__ float extend_cover(const ObjDev& o, const uint8_t* __restrict__ field, float ox, float oy, float oz,
                               float dx, float dy, float dz, float cover, float need, uint32_t links) {
+  const ProbeRay r = probe_ray(o, ox, oy, oz, dx, dy, dz);
   const float ahead = 32.0f * o.vs;
   for (uint32_t i = 0; i < links && cover < need; ++i) {
-    float nx = probe_cube(o, field, ox, oy, oz, dx, dy, dz, cover, cover + ahead);
+    float nx = probe_cube(o, field, r, cover, cover + ahead);
     if (!(nx > cover)) {
-      nx = probe_cube(o, field, ox, oy, oz, dx, dy, dz, cover, cover);
+      nx = probe_cube(o, field, r, cover, cover);
       if (!(nx > cover)) break;
     }
     cover = nx;
