@@ -117,12 +117,22 @@ typedef struct rkf_gpu_object {
 /* March parameters: SceneUniforms plus the shader's compile-time constants */
 /* as explicit fields (ray_march.wgsl:28-41).                               */
 /* ------------------------------------------------------------------------ */
+typedef enum rkf_strategy {
+    RKF_STRATEGY_BRUTE = 0,  /* ray_march_brute (:776-858): every object each */
+                             /* step (the BVH strategy gives the same result) */
+    RKF_STRATEGY_TILED = 1   /* ray_march_tiled (:874-985): coarse-field skips */
+                             /* and per-16x16-tile object lists; views only   */
+} rkf_strategy;
+
 typedef struct rkf_march_params {
     rkf_scene_uniforms scene;        /* num_objects is filled by the ctx   */
     uint32_t hard_max_steps;         /* HARD_MAX_STEPS = 1024              */
     uint32_t bisect_steps;           /* BISECT_STEPS = 8                   */
     float min_step;                  /* MIN_STEP = 0.0005                  */
     float near_surface_threshold;    /* NEAR_SURFACE_THRESHOLD = 0.02      */
+    uint32_t strategy;               /* rkf_strategy (views; ray batches   */
+                                     /* always march every object)         */
+    uint32_t reserved;
 } rkf_march_params;
 
 /* Fill p with the reference defaults (gpu_scene.rs:34-43, ray_march.wgsl:28-41). */

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cfloat>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -360,6 +361,170 @@ struct Tracker {  // distinct 32-byte sectors touched by one ray
   }
 };
 
+// ---------------------------------------------------------------------------
+// Tiled strategy inputs: the coarse acceleration field and the per-tile object
+// lists.
+// ---------------------------------------------------------------------------
+// CoarseField (crates/rkf-render/src/coarse_field.rs): cells of 0.32 m
+// (COARSE_VOXEL_SIZE, :21) over the union of the objects' AABBs grown by the
+// runtime's 1 m margin (from_scene_aabbs, :211-232; render.rs:257-263), at
+// most 128 per axis (:24, :93-97); each texel is the binary16 of the smallest
+// unsigned distance from the cell centre to an object AABB, starting from
+// vs * max(dims) (populate, :240-266; aabb_unsigned_distance, :72-79).
+struct CoarseField {
+  float origin[3];
+  uint32_t dims[3];
+  float vs, inv_vs;
+  std::vector<uint16_t> tex;  // x + y*dx + z*dx*dy
+};
+
+CoarseField coarse_build(const orc_scene* s) {
+  CoarseField c;
+  c.vs = 0.32f;
+  const float margin = 1.0f;
+  float lo[3], hi[3];
+  if (s->num_objects == 0) {
+    for (int a = 0; a < 3; ++a) lo[a] = 0.0f, hi[a] = c.vs;
+  } else {
+    for (int a = 0; a < 3; ++a) lo[a] = FLT_MAX, hi[a] = -FLT_MAX;
+    for (uint32_t i = 0; i < s->num_objects; ++i)
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::fmin(lo[a], s->objects[i].aabb_min[a]);
+        hi[a] = std::fmax(hi[a], s->objects[i].aabb_max[a]);
+      }
+  }
+  for (int a = 0; a < 3; ++a) {
+    c.origin[a] = lo[a] - margin;
+    const float extent = (hi[a] + margin) - c.origin[a];
+    const float cells = std::fmin(std::ceil(extent / c.vs), 128.0f);  // ceil() as u32, .min(128).max(1)
+    c.dims[a] = std::max<uint32_t>(1u, cells > 0.0f ? static_cast<uint32_t>(cells) : 0u);
+  }
+  c.inv_vs = 1.0f / c.vs;
+  const uint32_t dmax = std::max(c.dims[0], std::max(c.dims[1], c.dims[2]));
+  const float start = c.vs * static_cast<float>(dmax);
+  c.tex.resize(static_cast<size_t>(c.dims[0]) * c.dims[1] * c.dims[2]);
+  for (uint32_t z = 0; z < c.dims[2]; ++z)
+    for (uint32_t y = 0; y < c.dims[1]; ++y)
+      for (uint32_t x = 0; x < c.dims[0]; ++x) {
+        const float q[3] = {c.origin[0] + (static_cast<float>(x) + 0.5f) * c.vs,
+                            c.origin[1] + (static_cast<float>(y) + 0.5f) * c.vs,
+                            c.origin[2] + (static_cast<float>(z) + 0.5f) * c.vs};
+        float best = start;
+        for (uint32_t i = 0; i < s->num_objects; ++i) {
+          const rkf_gpu_object& o = s->objects[i];
+          float d3[3];
+          for (int a = 0; a < 3; ++a) {
+            const float e = std::fmax(o.aabb_min[a] - q[a], q[a] - o.aabb_max[a]);
+            d3[a] = std::fmax(e, 0.0f);
+          }
+          const float d = std::sqrt((d3[0] * d3[0] + d3[1] * d3[1]) + d3[2] * d3[2]);
+          best = std::fmin(best, d);
+        }
+        c.tex[x + y * static_cast<size_t>(c.dims[0]) + z * static_cast<size_t>(c.dims[0]) * c.dims[1]] =
+            f16_from_f32(best);
+      }
+  return c;
+}
+
+// sample_coarse_field (ray_march.wgsl:228-235): uvw = (cam_rel - origin_cam_rel)
+// * inv_voxel_size / dims, 0 outside [0,1]^3, else a linearly filtered,
+// clamp-to-edge read of the R16Float texture.  The filter is a model of the
+// texture unit: texel coordinate u*N - 0.5, its fraction quantised to 1/256
+// (the 8 fractional weight bits NVIDIA documents for linear filtering), then
+// mix(a, b, w) along x, y and z.  The reference's value comes from that
+// hardware and cannot be pinned here.
+float coarse_sample(const CoarseField& c, const float ocr[3], float cx, float cy, float cz) {
+  const float cr[3] = {cx, cy, cz};
+  int i0[3], i1[3];
+  float w[3];
+  for (int a = 0; a < 3; ++a) {
+    const float u = ((cr[a] - ocr[a]) * c.inv_vs) / static_cast<float>(c.dims[a]);
+    if (u < 0.0f || u > 1.0f) return 0.0f;
+    const float x = u * static_cast<float>(c.dims[a]) - 0.5f;
+    const float f = std::floor(x);
+    w[a] = std::nearbyint((x - f) * 256.0f) * 0.00390625f;
+    const int n = static_cast<int>(c.dims[a]);
+    const int k = static_cast<int>(f);
+    i0[a] = std::min(std::max(k, 0), n - 1);
+    i1[a] = std::min(std::max(k + 1, 0), n - 1);
+  }
+  const size_t sx = 1, sy = c.dims[0], sz = static_cast<size_t>(c.dims[0]) * c.dims[1];
+  auto T = [&](int x, int y, int z) { return f16_to_f32(c.tex[x * sx + y * sy + z * sz]); };
+  const float c00 = mixf(T(i0[0], i0[1], i0[2]), T(i1[0], i0[1], i0[2]), w[0]);
+  const float c10 = mixf(T(i0[0], i1[1], i0[2]), T(i1[0], i1[1], i0[2]), w[0]);
+  const float c01 = mixf(T(i0[0], i0[1], i1[2]), T(i1[0], i0[1], i1[2]), w[0]);
+  const float c11 = mixf(T(i0[0], i1[1], i1[2]), T(i1[0], i1[1], i1[2]), w[0]);
+  return mixf(mixf(c00, c10, w[1]), mixf(c01, c11, w[1]), w[2]);
+}
+
+// tile_object_cull.wgsl:90-205: per 16x16-pixel tile, the objects whose
+// projected AABB overlaps it (all 8 corners in front: screen rectangle test;
+// straddling the camera plane: always; all behind: never), at most 32.  The
+// shader appends with a shared-memory atomic, so its order (and, beyond 32,
+// its choice) is unspecified; here it is ascending object index.  The screen
+// is the view's size (the reference sizes its tiles and its G-buffer from
+// the same resolution).
+void tile_cull(const orc_scene* s, const rkf_camera* cam, uint32_t w, uint32_t h, std::vector<uint32_t>& cnt,
+               std::vector<uint32_t>& list, uint32_t* tiles_x) {
+  const float resx = static_cast<float>(w), resy = static_cast<float>(h);
+  const uint32_t ntx = static_cast<uint32_t>(std::ceil(resx / 16.0f));
+  const uint32_t nty = static_cast<uint32_t>(std::ceil(resy / 16.0f));
+  *tiles_x = ntx;
+  cnt.assign(static_cast<size_t>(ntx) * nty, 0);
+  list.assign(static_cast<size_t>(ntx) * nty * 32, 0);
+  const V3<float> fwd = v3<float>(cam->forward[0], cam->forward[1], cam->forward[2]);
+  const V3<float> rt = v3<float>(cam->right[0], cam->right[1], cam->right[2]);
+  const V3<float> up = v3<float>(cam->up[0], cam->up[1], cam->up[2]);
+  const V3<float> cp = v3<float>(cam->position[0], cam->position[1], cam->position[2]);
+  const float r_sq = dot(rt, rt), u_sq = dot(up, up);
+  for (uint32_t ty = 0; ty < nty; ++ty)
+    for (uint32_t tx = 0; tx < ntx; ++tx) {
+      const float tminx = static_cast<float>(tx * 16), tminy = static_cast<float>(ty * 16);
+      const float tmaxx = tminx + 16.0f, tmaxy = tminy + 16.0f;
+      uint32_t n = 0;
+      const size_t tile = static_cast<size_t>(ty) * ntx + tx;
+      for (uint32_t i = 0; i < s->num_objects; ++i) {
+        const rkf_gpu_object& o = s->objects[i];
+        if (o.sdf_type == RKF_SDF_NONE) continue;
+        float smin_x = resx, smin_y = resy, smax_x = 0.0f, smax_y = 0.0f;
+        bool front = false, behind = false;
+        for (uint32_t c = 0; c < 8; ++c) {
+          const V3<float> corner = v3<float>((c & 1u) ? o.aabb_max[0] : o.aabb_min[0],
+                                             (c & 2u) ? o.aabb_max[1] : o.aabb_min[1],
+                                             (c & 4u) ? o.aabb_max[2] : o.aabb_min[2]);
+          const V3<float> rel = sub(corner, cp);
+          const float depth = dot(rel, fwd);
+          if (depth > 0.0f) {
+            const float ndc_x = dot(rel, rt) / (depth * r_sq);
+            const float ndc_y = dot(rel, up) / (depth * u_sq);
+            const float px = (ndc_x * 0.5f + 0.5f) * resx;
+            const float py = (0.5f - ndc_y * 0.5f) * resy;
+            front = true;
+            smin_x = fmin_(smin_x, px), smin_y = fmin_(smin_y, py);
+            smax_x = fmax_(smax_x, px), smax_y = fmax_(smax_y, py);
+          } else {
+            behind = true;
+          }
+        }
+        bool overlaps = false;
+        if (behind && front) overlaps = true;
+        else if (!behind && front)
+          overlaps = smax_x >= tminx && smin_x < tmaxx && smax_y >= tminy && smin_y < tmaxy;
+        if (overlaps && n < 32) list[tile * 32 + n++] = i;
+      }
+      cnt[tile] = n;
+    }
+}
+
+// The tiled strategy's per-ray inputs.
+struct TiledRay {
+  const CoarseField* cf;
+  float ocr[3];        // field origin relative to the camera (CoarseField::upload, :297-305)
+  float cam[3];        // camera.position
+  const uint32_t* list;
+  uint32_t count;
+};
+
 template <class R>
 struct Marcher {
   const orc_scene* s;
@@ -601,8 +766,10 @@ struct Marcher {
   // result whenever object AABBs bound their SDFs.  any_hit stops at the
   // first surface contact without bisecting.
   Result march(V3<R> origin, V3<R> dir, const rkf_march_params* p, R max_distance,
-               bool any_hit, uint64_t* steps_out) {
+               bool any_hit, uint64_t* steps_out, const TiledRay* tl = nullptr) {
     Result r{R(kMaxFloat), false, false, false, 0, 0, 0};
+    // ray_march_tiled (:874-985): a tile with no objects is sky
+    if (tl && tl->count == 0) return r;
     const V3<R> sd = v3<R>(std::fabs(dir.x) < R(1e-10f) ? R(1e-10f) : dir.x,
                            std::fabs(dir.y) < R(1e-10f) ? R(1e-10f) : dir.y,
                            std::fabs(dir.z) < R(1e-10f) ? R(1e-10f) : dir.z);
@@ -616,9 +783,22 @@ struct Marcher {
       note(t, max_distance);
       if (t > max_distance || near_steps >= p->scene.max_steps) break;
       const V3<R> pos = add(origin, mul(sd, t));
+      if (tl) {
+        // coarse empty-space skip (:907-921): forget the previous sample
+        const R cd = R(coarse_sample(*tl->cf, tl->ocr, static_cast<float>(pos.x - R(tl->cam[0])),
+                                     static_cast<float>(pos.y - R(tl->cam[1])),
+                                     static_cast<float>(pos.z - R(tl->cam[2]))));
+        if (cd > R(0.5f)) {  // COARSE_NEAR_THRESHOLD (:863)
+          prev_dist = R(kMaxFloat);
+          t += cd;
+          continue;
+        }
+      }
       R min_dist = R(kMaxFloat);
       uint32_t best_mat = 0, best_id = 0, best_idx = 0;
-      for (uint32_t i = 0; i < s->num_objects; ++i) {
+      const uint32_t n_eval = tl ? tl->count : s->num_objects;
+      for (uint32_t j = 0; j < n_eval; ++j) {
+        const uint32_t i = tl ? tl->list[j] : j;
         uint32_t m;
         const R d = evaluate(pos, i, &m, !any_hit);
         if (d < min_dist) {
@@ -866,6 +1046,16 @@ void march_view(const orc_scene* s, const rkf_camera* cam, const rkf_march_param
   const uint64_t n = static_cast<uint64_t>(row1 - row0) * w;
   std::vector<orc_stats> per(std::max(threads, 1));
   std::memset(per.data(), 0, sizeof(orc_stats) * per.size());
+  const bool tiled = p->strategy == RKF_STRATEGY_TILED;
+  CoarseField cf;
+  std::vector<uint32_t> tcnt, tlist;
+  uint32_t tiles_x = 0;
+  float ocr[3] = {0.0f, 0.0f, 0.0f};
+  if (tiled) {
+    cf = coarse_build(s);
+    tile_cull(s, cam, w, h, tcnt, tlist, &tiles_x);
+    for (int a = 0; a < 3; ++a) ocr[a] = cf.origin[a] - cam->position[a];
+  }
   parallel_for(n, threads, [&](uint64_t li, int th) {
     Tracker tr;
     tr.on = count_sectors != 0;
@@ -886,7 +1076,17 @@ void march_view(const orc_scene* s, const rkf_camera* cam, const rkf_march_param
     const R dl = length(dv);
     const V3<R> dir = v3<R>(dv.x / dl, dv.y / dl, dv.z / dl);
     const V3<R> org = v3<R>(R(cam->position[0]), R(cam->position[1]), R(cam->position[2]));
-    const auto res = mc.march(org, dir, p, R(p->scene.max_distance), false, &per[th].steps);
+    TiledRay tr_{};
+    if (tiled) {
+      // the march's tile grid: dims from the view, (w + 15) / 16 tiles per row (:884-888)
+      const size_t tile = static_cast<size_t>(py / 16) * ((w + 15) / 16) + px / 16;
+      tr_.cf = &cf;
+      for (int a = 0; a < 3; ++a) tr_.ocr[a] = ocr[a], tr_.cam[a] = cam->position[a];
+      tr_.list = tlist.data() + tile * 32;
+      tr_.count = tcnt[tile];
+    }
+    const auto res = mc.march(org, dir, p, R(p->scene.max_distance), false, &per[th].steps,
+                              tiled ? &tr_ : nullptr);
     V3<R> hp, nn;
     uint32_t sec, blend;
     R sdf_hit;
@@ -1347,6 +1547,8 @@ void orc_march_params_default(rkf_march_params* p) {
   p->bisect_steps = 8;
   p->min_step = 0.0005f;
   p->near_surface_threshold = 0.02f;
+  p->strategy = RKF_STRATEGY_BRUTE;
+  p->reserved = 0;
 }
 
 }  // extern "C"

@@ -33,6 +33,7 @@ RKF_BAND_VOXELS, RKF_BAND_REFERENCE = 0, 1
 RKF_TRACE_CLOSEST, RKF_TRACE_ANY, RKF_TRACE_SHADOW = 0, 1, 2
 RKF_FLAG_HIT, RKF_FLAG_BISECTED, RKF_FLAG_STEPS_OUT = 1, 2, 4
 RKF_REQ_RENDER, RKF_REQ_RAYS, RKF_REQ_POINTS, RKF_REQ_EDIT = 0, 1, 2, 3
+RKF_STRATEGY_BRUTE, RKF_STRATEGY_TILED = 0, 1
 
 
 class rkf_camera(C.Structure):
@@ -62,7 +63,8 @@ class rkf_gpu_object(C.Structure):
 class rkf_march_params(C.Structure):
     _fields_ = [("scene", rkf_scene_uniforms), ("hard_max_steps", C.c_uint32),
                 ("bisect_steps", C.c_uint32), ("min_step", C.c_float),
-                ("near_surface_threshold", C.c_float)]
+                ("near_surface_threshold", C.c_float), ("strategy", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class rkf_config(C.Structure):
@@ -169,6 +171,7 @@ def march_params_default(p: rkf_march_params) -> None:
     p.bisect_steps = 8
     p.min_step = 0.0005
     p.near_surface_threshold = 0.02
+    p.strategy = RKF_STRATEGY_BRUTE
 
 
 # Every function the header declares, with its ctypes signature.

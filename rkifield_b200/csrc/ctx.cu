@@ -336,6 +336,8 @@ void rkf_march_params_default(rkf_march_params* p) {
   p->bisect_steps = 8;              // ray_march.wgsl:31
   p->min_step = 0.0005f;            // ray_march.wgsl:30
   p->near_surface_threshold = 0.02f;  // ray_march.wgsl:41
+  p->strategy = RKF_STRATEGY_BRUTE;
+  p->reserved = 0;
 }
 
 void rkf_config_default(rkf_config* cfg) {

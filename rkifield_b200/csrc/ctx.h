@@ -93,6 +93,12 @@ struct Ctx {
   uint32_t n_leaves = 0, leaf_cap = 0;
   bool leaves_frozen = false;  // set while serving: the leaf buffer must not move
 
+  // tiled strategy (tiled.h): coarse field (rebuilt when epoch changes) and tile lists
+  DevBuf coarse_tex, tile_buf;
+  float coarse_origin[3] = {0.0f, 0.0f, 0.0f};
+  uint32_t coarse_dims[3] = {0, 0, 0};
+  uint64_t coarse_epoch = ~0ull;
+
   // objects
   std::vector<rkf_gpu_object> objects;
   std::vector<ObjDev> objdev_host;

@@ -15,8 +15,10 @@ struct Segment {
   uint64_t first;     // first global work id of the segment
   uint64_t n_ids;     // work ids the segment spans
   uint32_t kind, mode;
-  uint32_t w, h, tiles_x, _pad;
+  uint32_t w, h, tiles_x, tile_off;  // tile_off: first object tile of the view (tiled strategy)
   float pos[3], fwd[3], right[3], up[3], jitter[2];
+  float coarse_ocr[3];                // coarse field origin relative to the camera (tiled strategy)
+  uint32_t _pad;
   float prev_vp[16];
   const float* origins;
   const float* dirs;

@@ -27,6 +27,7 @@
 #include "march.h"
 #include "f32x2.cuh"
 #include "sampler.cuh"
+#include "tiled.h"
 
 namespace rkf {
 
@@ -41,6 +42,7 @@ constexpr uint32_t kFull = 0xFFFFFFFFu;
 struct ColdState {
   uint32_t seg, idx, hit_obj, sub;
   float lo, hi, mat_t, gpos, shadow;
+  uint32_t tile_base, tile_count;  // tiled strategy: the ray's object list (kNoTiles: every object)
   bool hit, bisected, mat_ok;
 };
 
@@ -59,6 +61,8 @@ struct KParams {
   uint32_t plain_obj;  // object 0 has zero translation and unit scale
   uint32_t refill_active;  // leave the march loop once at most this many lanes march
   uint32_t run_probe;      // empty-space path: probe the next cube inside a run
+  TiledDev td;             // tiled strategy inputs (views of a tiled launch)
+  uint32_t tiled;
   float empty_lo;          // empty-space path: lower bound of every EMPTY value
   float empty_lo_t, empty_hi;  // empty-space path: tight bounds of an EMPTY step
   uint32_t settle_links;   // empty-space path: cubes a settling chain may add (0 = off)
@@ -398,8 +402,15 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                 oz = sg.pos[2];
                 tmax = p.scene.max_distance;
                 mode = RKF_TRACE_CLOSEST;
+                cs.tile_count = kNoTiles;
+                if (!EMPTY_PATH && kp.tiled) {  // the pixel's tile (ray_march.wgsl:884-893)
+                  const uint32_t tl = sg.tile_off + (py / 16) * ((sg.w + 15) / 16) + px / 16;
+                  cs.tile_base = tl * kTileObjects;
+                  cs.tile_count = __ldg(kp.td.tile_cnt + tl);
+                }
               }
             } else {
+              cs.tile_count = kNoTiles;
               cs.idx = static_cast<uint32_t>(local);
               const size_t i3 = 3 * static_cast<size_t>(cs.idx);
               ox = __ldg(sg.origins + i3);
@@ -425,7 +436,8 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                 t = 0.0f;
                 prev_t = 0.0f;
                 prev_dist = kMaxFloat;
-                state = ST_MARCH;
+                // a tile with no objects is sky (ray_march.wgsl:895-897)
+                state = cs.tile_count == 0 ? ST_EPI : ST_MARCH;
               }
             }
           }
@@ -523,10 +535,41 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
         } else {
           float best_un;
           uint32_t best_i;
-          const float best = eval_min<PREC, SINGLE>(s, sh_objs, 0, nobj, __fadd_rn(ox, __fmul_rn(qdx, t)),
-                                                    __fadd_rn(oy, __fmul_rn(qdy, t)),
-                                                    __fadd_rn(oz, __fmul_rn(qdz, t)), best_un, best_i, lc);
-          if (best < 0.0f && prev_dist > hit_thr) {  // overstep (ray_march.wgsl:816)
+          const float wx = __fadd_rn(ox, __fmul_rn(qdx, t)), wy = __fadd_rn(oy, __fmul_rn(qdy, t)),
+                      wz = __fadd_rn(oz, __fmul_rn(qdz, t));
+          float best;
+          bool skipped = false;
+          if (!EMPTY_PATH && kp.tiled && cs.tile_count != kNoTiles) {
+            // ray_march_tiled (:899-938): a coarse empty-space skip, else the
+            // tile's objects only
+            const Segment& sg = kp.segs[cs.seg];
+            const float cd = coarse_sample(kp.td, sg.coarse_ocr, __fsub_rn(wx, sg.pos[0]), __fsub_rn(wy, sg.pos[1]),
+                                           __fsub_rn(wz, sg.pos[2]));
+            best = kMaxFloat;
+            best_un = kMaxFloat;
+            best_i = 0;
+            if (cd > kCoarseNear) {
+              prev_dist = kMaxFloat;
+              t = __fadd_rn(t, cd);
+              step++;
+              skipped = true;
+            } else {
+              for (uint32_t j = 0; j < cs.tile_count; ++j) {
+                const uint32_t oi = __ldg(kp.td.tile_list + cs.tile_base + j);
+                float du;
+                const float d = eval_obj<PREC>(s, sh_objs[oi], wx, wy, wz, &du, lc);
+                if (d < best) {
+                  best = d;
+                  best_un = du;
+                  best_i = oi;
+                }
+              }
+            }
+          } else {
+            best = eval_min<PREC, SINGLE>(s, sh_objs, 0, nobj, wx, wy, wz, best_un, best_i, lc);
+          }
+          if (skipped) {
+          } else if (best < 0.0f && prev_dist > hit_thr) {  // overstep (ray_march.wgsl:816)
             cs.hit_obj = best_i;
             cs.hit = true;
             if (mode == RKF_TRACE_ANY) {
@@ -884,12 +927,22 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   if (c->obj_count() > kMaxObjectsFast)
     return fail(RKF_UNSUPPORTED, "march: more objects than the persistent kernel holds");
   if (c->obj_count() == 0) return fail(RKF_INVALID_ARG, "march: the scene has no objects");
-  const size_t sb = segs_host.size() * sizeof(Segment);
+  const bool tiled = p->strategy == RKF_STRATEGY_TILED;
+  std::vector<Segment> tiled_segs;
+  TiledDev td;
+  std::memset(&td, 0, sizeof(td));
+  if (tiled) {
+    tiled_segs = segs_host;
+    rkf_status s2 = prepare_tiled(c, tiled_segs, st, &td);
+    if (s2 != RKF_OK) return s2;
+  }
+  const std::vector<Segment>& segs_dev = tiled ? tiled_segs : segs_host;
+  const size_t sb = segs_dev.size() * sizeof(Segment);
   if (seg_buf->bytes < sb) {
     rkf_status s2 = seg_buf->alloc(sb);
     if (s2 != RKF_OK) return s2;
   }
-  RKF_CUDA_TRY(cudaMemcpyAsync(seg_buf->p, segs_host.data(), sb, cudaMemcpyHostToDevice, st));
+  RKF_CUDA_TRY(cudaMemcpyAsync(seg_buf->p, segs_dev.data(), sb, cudaMemcpyHostToDevice, st));
   RKF_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
   detail::KParams kp;
   std::memset(&kp, 0, sizeof(kp));
@@ -904,7 +957,9 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   kp.counter = counter;
   kp.p = *p;
   kp.p.scene.num_objects = c->obj_count();
-  const int obj = object_set(c);
+  const int obj = tiled && object_set(c) == detail::OBJ_SINGLE_EMPTY ? detail::OBJ_SINGLE : object_set(c);
+  kp.td = td;
+  kp.tiled = tiled ? 1u : 0u;
   kp.probe_min = obj == detail::OBJ_SINGLE_EMPTY ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
   kp.budget = tu.step_budget ? tu.step_budget : 32;
   kp.refill_active = 32u - std::min<uint32_t>(tu.refill_idle ? tu.refill_idle : 32u, 32u);
@@ -953,6 +1008,8 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
 rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t nseg, uint64_t total,
                                      const rkf_march_params* p, const rkf_batch_tuning& tu,
                                      cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter) {
+  if (p->strategy != RKF_STRATEGY_BRUTE)
+    return fail(RKF_UNSUPPORTED, "march: the tiled strategy needs tile-list scratch this launch path lacks");
   if (c->obj_count() > kMaxObjectsFast)
     return fail(RKF_UNSUPPORTED, "march: more objects than the persistent kernel holds");
   if (c->obj_count() == 0) return fail(RKF_INVALID_ARG, "march: the scene has no objects");

@@ -478,6 +478,8 @@ rkf_status launch_trace_plain(Ctx* c, const float* o, const float* d, const floa
 rkf_status launch_plain(Ctx* c, const rkf_camera* cam, const rkf_march_params* p, uint32_t w,
                         uint32_t h, const rkf_gbuffer& out, cudaStream_t st) {
   if (!c->aos.p) return fail(RKF_UNSUPPORTED, "rkf_march_plain: context keeps no reference (AoS) pool");
+  if (p->strategy != RKF_STRATEGY_BRUTE)
+    return fail(RKF_UNSUPPORTED, "rkf_march_plain: the baseline runs the brute strategy only");
   detail::PlainParams kp;
   kp.s = c->scene_dev();
   kp.p = *p;

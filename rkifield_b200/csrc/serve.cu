@@ -408,6 +408,8 @@ rkf_status rkf_serve_start(rkf_ctx* ctx, const rkf_march_params* p) {
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   if (c->serve) return fail(RKF_BUSY, "rkf_serve_start: already serving");
   if (c->obj_count() == 0) return fail(RKF_INVALID_ARG, "rkf_serve_start: the scene has no objects");
+  if (p->strategy != RKF_STRATEGY_BRUTE)
+    return fail(RKF_UNSUPPORTED, "rkf_serve_start: serving marches with the brute strategy only");
   RKF_CUDA_TRY(cudaSetDevice(c->device));
   RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
   auto* s = new ServeState();
