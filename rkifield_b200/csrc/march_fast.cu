@@ -44,7 +44,9 @@ struct ColdState {
   float lo, hi, mat_t, gpos, shadow;
   uint32_t tile_base, tile_count;  // tiled strategy: the ray's object list (kNoTiles: every object)
   bool hit, bisected, mat_ok;
+  uint32_t pad_;  // an odd number of words per lane: a warp's accesses hit 32 distinct banks
 };
+static_assert(sizeof(ColdState) % 8 == 4, "ColdState must span an odd number of 32-bit words");
 
 struct KParams {
   ObjDev objs[kMaxObjectsFast];  // object table in the constant parameter bank
@@ -402,15 +404,17 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                 oz = sg.pos[2];
                 tmax = p.scene.max_distance;
                 mode = RKF_TRACE_CLOSEST;
-                cs.tile_count = kNoTiles;
-                if (!EMPTY_PATH && kp.tiled) {  // the pixel's tile (ray_march.wgsl:884-893)
-                  const uint32_t tl = sg.tile_off + (py / 16) * ((sg.w + 15) / 16) + px / 16;
-                  cs.tile_base = tl * kTileObjects;
-                  cs.tile_count = __ldg(kp.td.tile_cnt + tl);
+                if (!EMPTY_PATH) {
+                  cs.tile_count = kNoTiles;
+                  if (kp.tiled) {  // the pixel's tile (ray_march.wgsl:884-893)
+                    const uint32_t tl = sg.tile_off + (py / 16) * ((sg.w + 15) / 16) + px / 16;
+                    cs.tile_base = tl * kTileObjects;
+                    cs.tile_count = __ldg(kp.td.tile_cnt + tl);
+                  }
                 }
               }
             } else {
-              cs.tile_count = kNoTiles;
+              if (!EMPTY_PATH) cs.tile_count = kNoTiles;
               cs.idx = static_cast<uint32_t>(local);
               const size_t i3 = 3 * static_cast<size_t>(cs.idx);
               ox = __ldg(sg.origins + i3);
@@ -437,7 +441,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                 prev_t = 0.0f;
                 prev_dist = kMaxFloat;
                 // a tile with no objects is sky (ray_march.wgsl:895-897)
-                state = cs.tile_count == 0 ? ST_EPI : ST_MARCH;
+                state = (!EMPTY_PATH && cs.tile_count == 0) ? ST_EPI : ST_MARCH;
               }
             }
           }
