@@ -551,7 +551,8 @@ rkf_status rkf_objects_import(rkf_ctx* ctx, const rkf_gpu_object* objects, uint3
             if (all_int) {
               entry = RKF_INTERIOR_SLOT;
             } else if (any) {
-              entry = c->n_leaves + static_cast<uint32_t>(leaf_host.size() / 512);
+              // the import replaces the leaf buffer: entries count from 0
+              entry = static_cast<uint32_t>(leaf_host.size() / 512);
               for (uint32_t l = 0; l < 512; ++l) {
                 const uint64_t bx = kx * 8 + (l & 7), by = ky * 8 + ((l >> 3) & 7), bz = kz * 8 + (l >> 6);
                 uint32_t s = RKF_EMPTY_SLOT;

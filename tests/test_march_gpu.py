@@ -85,3 +85,38 @@ def test_soa_import_matches_voxelsample_import(oracle, small_scene, small_ctx, p
     finally:
         a.close()
         b.close()
+
+
+def test_objects_reimport_replaces_the_index(oracle, small_scene):
+    """A second rkf_objects_import builds the index afresh: its top grid names
+    leaf blocks of the new leaf buffer only, and the index and the march equal
+    those of a context that imported the objects once."""
+    from rkifield_b200 import _abi as abi, scenes
+    from rkifield_b200.engine import Context
+    v = small_scene["vox"]
+    cap = v.n_bricks + 1024
+    a = Context(pool_capacity=cap)
+    b = Context(pool_capacity=cap)
+    try:
+        for ctx in (a, b):
+            ctx.set_brick_pool(v.words)
+            ctx.upload_brick_maps(v.map)
+        a.upload_objects([small_scene["obj"]])
+        a.upload_objects([small_scene["obj"]])
+        b.upload_objects([small_scene["obj"]])
+        ia, ib = a.export_index(), b.export_index()
+        n_leaves = a.info()["leaf_blocks"]
+        assert n_leaves == b.info()["leaf_blocks"] > 0
+        leaf = ia["top"][ia["top"] < abi.INTERIOR_SLOT]
+        assert leaf.size and int(leaf.max()) < n_leaves
+        for k in ia:
+            assert_bits_equal(ia[k], ib[k], f"index {k}")
+        spec = small_scene["spec"]
+        cam = scenes.seeded_camera(spec, 128, 96, seed=23)
+        p = scenes.march_params(spec)
+        ga, gb = a.march(cam, p, 128, 96), b.march(cam, p, 128, 96)
+        for k in ga:
+            assert_bits_equal(ga[k], gb[k], f"march {k}")
+    finally:
+        a.close()
+        b.close()

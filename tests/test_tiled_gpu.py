@@ -115,3 +115,28 @@ def test_multi_object_views_bit_exact(oracle, small_scene, strategy, seed):
                 assert_bits_equal(g[kk].download(), ref[kk], f"batched tiled {kk}")
     finally:
         ctx.close()
+
+
+@pytest.mark.gpu
+def test_tiled_after_scene_change_bit_exact(oracle, small_scene):
+    """The coarse field follows the scene: march, add an object, march again."""
+    from rkifield_b200 import _abi as abi
+    from rkifield_b200.engine import Context
+    v = small_scene["vox"]
+    objs = _objects(small_scene)
+    ctx = Context(pool_capacity=v.n_bricks + 1024)
+    try:
+        ctx.set_brick_pool(v.words)
+        ctx.upload_brick_maps(v.map)
+        w, h = 160, 96
+        cam = _camera(5, w, h)
+        p = _params(abi.RKF_STRATEGY_TILED)
+        for k in (3, 5):
+            ctx.upload_objects(objs[:k])
+            sc = oracle.Scene(objs[:k], pool_words=v.words, brick_maps=v.map)
+            ref = oracle.march(sc, cam, p, w, h)
+            got = ctx.march(cam, p, w, h)
+            for name in ("t", "normal", "slot", "material", "flags"):
+                assert_bits_equal(got[name], ref[name], f"{k} objects {name}")
+    finally:
+        ctx.close()
