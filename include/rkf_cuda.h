@@ -119,9 +119,13 @@ typedef struct rkf_gpu_object {
 /* ------------------------------------------------------------------------ */
 typedef enum rkf_strategy {
     RKF_STRATEGY_BRUTE = 0,  /* ray_march_brute (:776-858): every object each */
-                             /* step (the BVH strategy gives the same result) */
-    RKF_STRATEGY_TILED = 1   /* ray_march_tiled (:874-985): coarse-field skips */
+                             /* step, in index order                          */
+    RKF_STRATEGY_TILED = 1,  /* ray_march_tiled (:874-985): coarse-field skips */
                              /* and per-16x16-tile object lists; views only   */
+    RKF_STRATEGY_BVH = 2     /* ray_march_bvh (:641-773): each step walks the  */
+                             /* imported BVH (rkf_bvh_import), skipping nodes */
+                             /* farther than the best distance so far; views  */
+                             /* and closest/any ray batches                   */
 } rkf_strategy;
 
 typedef struct rkf_march_params {
@@ -130,8 +134,8 @@ typedef struct rkf_march_params {
     uint32_t bisect_steps;           /* BISECT_STEPS = 8                   */
     float min_step;                  /* MIN_STEP = 0.0005                  */
     float near_surface_threshold;    /* NEAR_SURFACE_THRESHOLD = 0.02      */
-    uint32_t strategy;               /* rkf_strategy (views; ray batches   */
-                                     /* always march every object)         */
+    uint32_t strategy;               /* rkf_strategy (tiled: views only;   */
+                                     /* shadow rays march every object)    */
     uint32_t reserved;
 } rkf_march_params;
 
@@ -202,6 +206,42 @@ RKF_API rkf_status rkf_brickmap_import(rkf_ctx* ctx, const uint32_t* packed, uin
  * (gpu_scene.rs:141).  Builds the device two-level brick index for every
  * voxelized object from the imported brick maps. */
 RKF_API rkf_status rkf_objects_import(rkf_ctx* ctx, const rkf_gpu_object* objects, uint32_t n);
+
+/* One BVH node as the shader reads it (GpuBvhNode, gpu_bvh.rs:24-41;
+ * BvhNode, ray_march.wgsl:99-108): 32 bytes. */
+#define RKF_BVH_INVALID 0xFFFFFFFFu
+typedef struct rkf_bvh_node {
+    float aabb_min[3];
+    uint32_t left;             /* left child, or RKF_BVH_INVALID for a leaf  */
+    float aabb_max[3];
+    uint32_t right_or_object;  /* right child (internal) or object index     */
+} rkf_bvh_node;
+
+/* Upload BVH nodes, root first.  Replaces GpuScene::upload_bvh
+ * (gpu_scene.rs:186).  The nodes must form one tree: every internal node
+ * names two children with larger indices than its own, and every node but
+ * the root is named exactly once (Bvh::build, bvh.rs:66-260, lays nodes out
+ * this way); anything else returns RKF_INVALID_ARG and keeps the previous
+ * BVH.  Leaves may name any object index: the march skips indices at or
+ * beyond the object count, as the shader does.  n = 0 removes the BVH.  At
+ * most 65,536 nodes. */
+RKF_API rkf_status rkf_bvh_import(rkf_ctx* ctx, const rkf_bvh_node* nodes, uint32_t n);
+
+/* Object AABB for rkf_bvh_build: the (object_id, aabb) pairs of
+ * Bvh::build (bvh.rs:66). */
+typedef struct rkf_bvh_item {
+    uint32_t object_index;
+    float aabb_min[3];
+    float aabb_max[3];
+} rkf_bvh_item;
+
+/* Host-side BVH build with the reference's surface-area heuristic
+ * (Bvh::build, bvh.rs:66-260, converted by GpuBvhNode::from_cpu,
+ * gpu_bvh.rs:45-60): one object per leaf, 2n-1 nodes for n >= 1 items,
+ * 0 for n = 0.  Writes *n_out nodes to out (cap entries available; too few
+ * returns RKF_INVALID_ARG).  Needs no context or device. */
+RKF_API rkf_status rkf_bvh_build(const rkf_bvh_item* items, uint32_t n, rkf_bvh_node* out, uint32_t cap,
+                                 uint32_t* n_out);
 
 /* Counts of what the context holds. */
 typedef struct rkf_scene_info {

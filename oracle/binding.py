@@ -29,7 +29,8 @@ class orc_scene(C.Structure):
                 ("blend_plane", C.c_void_p), ("precision", C.c_uint32),
                 ("brick_maps", C.c_void_p), ("top", C.c_void_p), ("leaves", C.c_void_p),
                 ("obj_top_info", C.c_void_p), ("objects", C.c_void_p),
-                ("num_objects", C.c_uint32), ("dist_f64", C.c_void_p)]
+                ("num_objects", C.c_uint32), ("dist_f64", C.c_void_p),
+                ("bvh", C.c_void_p), ("bvh_nodes", C.c_uint32)]
 
 PRECISION_F64 = 3
 
@@ -154,15 +155,17 @@ class Scene:
     def __init__(self, objects, pool_words=None, brick_maps=None, top=None, leaves=None,
                  obj_top_info=None, dist_f16=None, dist_f32=None, dist_u8=None,
                  brick_scale=None, mat_plane=None, blend_plane=None,
-                 precision=abi.RKF_PRECISION_F16, dist_f64=None):
+                 precision=abi.RKF_PRECISION_F16, dist_f64=None, bvh=None):
         n = len(objects)
         self.objects = (abi.rkf_gpu_object * n)(*objects)
         self._keep = [pool_words, brick_maps, top, leaves, obj_top_info, dist_f16, dist_f32,
-                      dist_u8, brick_scale, mat_plane, blend_plane, dist_f64]
+                      dist_u8, brick_scale, mat_plane, blend_plane, dist_f64, bvh]
         self.s = orc_scene(ptr(pool_words), ptr(dist_f16), ptr(dist_f32), ptr(dist_u8),
                            ptr(brick_scale), ptr(mat_plane), ptr(blend_plane), precision,
                            ptr(brick_maps), ptr(top), ptr(leaves), ptr(obj_top_info),
-                           C.addressof(self.objects), n, ptr(dist_f64))
+                           C.addressof(self.objects), n, ptr(dist_f64),
+                           C.addressof(bvh) if bvh is not None and len(bvh) else None,
+                           len(bvh) if bvh is not None else 0)
 
 
 def march(scene: Scene, cam, params, w: int, h: int, fp64: bool = False, threads: int | None = None,

@@ -762,9 +762,10 @@ struct Marcher {
     uint32_t mat, obj_id, obj_idx;
   };
 
-  // ray_march_brute (:776-858); ray_march_bvh (:641-773) gives the same
-  // result whenever object AABBs bound their SDFs.  any_hit stops at the
-  // first surface contact without bisecting.
+  // ray_march_brute (:776-858), or ray_march_bvh (:641-773) when the
+  // strategy is BVH, or ray_march_tiled (:874-985) when tl is given.  The
+  // three differ only in the objects a step evaluates and their order.
+  // any_hit stops at the first surface contact without bisecting.
   Result march(V3<R> origin, V3<R> dir, const rkf_march_params* p, R max_distance,
                bool any_hit, uint64_t* steps_out, const TiledRay* tl = nullptr) {
     Result r{R(kMaxFloat), false, false, false, 0, 0, 0};
@@ -776,6 +777,7 @@ struct Marcher {
     const R hit_thr = R(p->scene.hit_threshold);
     const R near_thr = R(p->near_surface_threshold);
     const R min_step = R(p->min_step);
+    const bool use_bvh = p->strategy == RKF_STRATEGY_BVH && s->bvh && s->bvh_nodes;
     R t = R(0), prev_t = R(0), prev_dist = R(kMaxFloat);
     uint32_t near_steps = 0;
     uint32_t step = 0;
@@ -796,9 +798,7 @@ struct Marcher {
       }
       R min_dist = R(kMaxFloat);
       uint32_t best_mat = 0, best_id = 0, best_idx = 0;
-      const uint32_t n_eval = tl ? tl->count : s->num_objects;
-      for (uint32_t j = 0; j < n_eval; ++j) {
-        const uint32_t i = tl ? tl->list[j] : j;
+      auto consider = [&](uint32_t i) {
         uint32_t m;
         const R d = evaluate(pos, i, &m, !any_hit);
         if (d < min_dist) {
@@ -807,6 +807,33 @@ struct Marcher {
           best_id = s->objects[i].object_id;
           best_idx = i;
         }
+      };
+      if (!tl && use_bvh) {
+        // BVH traversal (:672-721): skip nodes whose AABB is farther than
+        // the best distance so far; push left then right (right is visited
+        // first) while the 32-entry stack has room for both
+        uint32_t stack[32];
+        uint32_t sp = 1;
+        stack[0] = 0;
+        while (sp > 0) {
+          const uint32_t ni = stack[--sp];
+          if (ni >= s->bvh_nodes) continue;  // the import admits no such tree
+          const rkf_bvh_node& nd = s->bvh[ni];
+          const V3<R> c = v3<R>(std::fmin(std::fmax(pos.x, R(nd.aabb_min[0])), R(nd.aabb_max[0])),
+                                std::fmin(std::fmax(pos.y, R(nd.aabb_min[1])), R(nd.aabb_max[1])),
+                                std::fmin(std::fmax(pos.z, R(nd.aabb_min[2])), R(nd.aabb_max[2])));
+          const R box_dist = length(sub(c, pos));
+          if (box_dist > min_dist) continue;
+          if (nd.left == RKF_BVH_INVALID) {
+            if (nd.right_or_object < s->num_objects) consider(nd.right_or_object);
+          } else if (sp < 31) {
+            stack[sp++] = nd.left;
+            stack[sp++] = nd.right_or_object;
+          }
+        }
+      } else {
+        const uint32_t n_eval = tl ? tl->count : s->num_objects;
+        for (uint32_t j = 0; j < n_eval; ++j) consider(tl ? tl->list[j] : j);
       }
       note(min_dist, R(0));
       note(min_dist, hit_thr);

@@ -5,8 +5,9 @@
  * calls this code.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
  * baseline leg use it, as the checker / timed CPU baseline.
  *
- * It restates crates/rkf-render/shaders/ray_march.wgsl (the march, its
- * samplers, bisection, normals, material and blend lookups),
+ * It restates crates/rkf-render/shaders/ray_march.wgsl (the brute, BVH and
+ * tiled marches, their samplers, bisection, normals, material and blend
+ * lookups),
  * shade_common_shading.wgsl:9-47 (soft shadow), the voxelizer of
  * crates/rkf-core/src/voxelize_object.rs:53-182, the analytic SDFs of
  * crates/rkf-core/src/sdf.rs:12-51, the binary16 conversion of the `half`
@@ -87,6 +88,10 @@ typedef struct orc_scene {
     const rkf_gpu_object* objects;
     uint32_t num_objects;
     const double* dist_f64;        /* analytic distances (precision 3)      */
+    /* BVH strategy (ray_march_bvh): nodes root first, a tree whose children
+     * follow their parent (rkf_bvh_import's rule) */
+    const rkf_bvh_node* bvh;
+    uint32_t bvh_nodes;
 } orc_scene;
 
 /* Distance-plane code for orc_scene.dist_f64. */

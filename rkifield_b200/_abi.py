@@ -33,7 +33,8 @@ RKF_BAND_VOXELS, RKF_BAND_REFERENCE = 0, 1
 RKF_TRACE_CLOSEST, RKF_TRACE_ANY, RKF_TRACE_SHADOW = 0, 1, 2
 RKF_FLAG_HIT, RKF_FLAG_BISECTED, RKF_FLAG_STEPS_OUT = 1, 2, 4
 RKF_REQ_RENDER, RKF_REQ_RAYS, RKF_REQ_POINTS, RKF_REQ_EDIT = 0, 1, 2, 3
-RKF_STRATEGY_BRUTE, RKF_STRATEGY_TILED = 0, 1
+RKF_STRATEGY_BRUTE, RKF_STRATEGY_TILED, RKF_STRATEGY_BVH = 0, 1, 2
+BVH_INVALID = 0xFFFFFFFF
 
 
 class rkf_camera(C.Structure):
@@ -72,6 +73,16 @@ class rkf_config(C.Structure):
                 ("precision", C.c_uint32), ("keep_reference_pool", C.c_uint32),
                 ("mem_budget_bytes", C.c_uint64), ("max_inflight", C.c_uint32),
                 ("reserved", C.c_uint32 * 7)]
+
+
+class rkf_bvh_node(C.Structure):
+    """GpuBvhNode (gpu_bvh.rs:24-41): 32 bytes."""
+    _fields_ = [("aabb_min", C.c_float * 3), ("left", C.c_uint32),
+                ("aabb_max", C.c_float * 3), ("right_or_object", C.c_uint32)]
+
+
+class rkf_bvh_item(C.Structure):
+    _fields_ = [("object_index", C.c_uint32), ("aabb_min", C.c_float * 3), ("aabb_max", C.c_float * 3)]
 
 
 class rkf_scene_info(C.Structure):
@@ -185,6 +196,8 @@ SIGNATURES = {
     "rkf_pool_import_voxelsample": (_I, [_P, _P, _U32, _U32]),
     "rkf_brickmap_import": (_I, [_P, _P, _U64]),
     "rkf_objects_import": (_I, [_P, _P, _U32]),
+    "rkf_bvh_import": (_I, [_P, _P, _U32]),
+    "rkf_bvh_build": (_I, [_P, _U32, _P, _U32, C.POINTER(_U32)]),
     "rkf_scene_info_get": (_I, [_P, C.POINTER(rkf_scene_info)]),
     "rkf_pool_export_voxelsample": (_I, [_P, _U32, _U32, _P]),
     "rkf_brick_lookup": (_I, [_P, _U32, _P, _U32, _P]),

@@ -21,7 +21,7 @@ LIB = os.path.join(OUT_DIR, "librkf_cuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
-         "-ftz=false", "-Xcompiler", "-fPIC,-O2,-fvisibility=hidden", "-Xptxas", "-warn-spills",
+         "-ftz=false", "-Xcompiler", "-fPIC,-O2,-fvisibility=hidden,-ffp-contract=off", "-Xptxas", "-warn-spills",
          "--expt-relaxed-constexpr", "-DRKF_BUILD"]
 
 

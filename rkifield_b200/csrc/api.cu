@@ -63,7 +63,7 @@ rkf_status check_common(rkf_ctx* ctx, const void* a, const rkf_march_params* p, 
   if (p->hard_max_steps == 0 || p->hard_max_steps > (1u << 20))
     return fail(RKF_INVALID_ARG, std::string(fn) + ": hard_max_steps out of range");
   if (p->bisect_steps > 64) return fail(RKF_INVALID_ARG, std::string(fn) + ": bisect_steps out of range");
-  if (p->strategy > RKF_STRATEGY_TILED) return fail(RKF_INVALID_ARG, std::string(fn) + ": unknown strategy");
+  if (p->strategy > RKF_STRATEGY_BVH) return fail(RKF_INVALID_ARG, std::string(fn) + ": unknown strategy");
   return RKF_OK;
 }
 

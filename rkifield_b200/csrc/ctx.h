@@ -99,6 +99,10 @@ struct Ctx {
   uint32_t coarse_dims[3] = {0, 0, 0};
   uint64_t coarse_epoch = ~0ull;
 
+  // BVH of the BVH strategy (bvh.cu): rkf_bvh_node records, root first
+  DevBuf bvh;
+  uint32_t bvh_n = 0;
+
   // objects
   std::vector<rkf_gpu_object> objects;
   std::vector<ObjDev> objdev_host;

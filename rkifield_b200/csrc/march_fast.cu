@@ -2,8 +2,8 @@
 // views (primary rays) and ray batches (closest / any-hit / soft shadow).
 //
 // Reference algorithm: crates/rkf-render/shaders/ray_march.wgsl:776-858
-// (ray_march_brute; ray_march_bvh :641-773 gives the same result whenever
-// the object AABBs bound their SDFs), :941-964 (bisection), :1003-1032
+// (ray_march_brute), :641-773 (ray_march_bvh), :874-985 (ray_march_tiled),
+// :941-964 (bisection), :1003-1032
 // (normals), :1036-1112 (ray generation and G-buffer), and
 // shade_common_shading.wgsl:9-33 (soft_shadow).
 //
@@ -68,7 +68,52 @@ struct KParams {
   float empty_lo;          // empty-space path: lower bound of every EMPTY value
   float empty_lo_t, empty_hi;  // empty-space path: tight bounds of an EMPTY step
   uint32_t settle_links;   // empty-space path: cubes a settling chain may add (0 = off)
+  const rkf_bvh_node* bvh; // BVH strategy: the imported tree, root first
+  uint32_t use_bvh;
 };
+
+// The candidate loop of ray_march_bvh (ray_march.wgsl:672-721): a stack walk
+// of the tree from the root that skips every node whose AABB lies farther
+// from the position than the best distance so far, evaluates the objects of
+// the leaves it reaches (object indices beyond the object count are skipped),
+// and pushes the left then the right child while fewer than 31 entries are on
+// the stack (so the right child is visited first).  The import admits trees
+// only, so the walk visits each node at most once.
+template <int PREC>
+__device__ __forceinline__ float eval_bvh(const SceneDev& s, const ObjDev* objs, const rkf_bvh_node* nodes,
+                                          uint32_t nobj, float wx, float wy, float wz, float& best_un,
+                                          uint32_t& best_i, LaneCache& lc) {
+  uint32_t stack[32];
+  uint32_t sp = 1;
+  stack[0] = 0;
+  float best = kMaxFloat;
+  best_un = kMaxFloat;
+  best_i = 0;
+  while (sp > 0) {
+    const float4* nd = reinterpret_cast<const float4*>(nodes + stack[--sp]);
+    const float4 a = __ldg(nd), b = __ldg(nd + 1);
+    // length(clamp(pos, node_min, node_max) - pos)
+    const float bd = len3(__fsub_rn(fminf(fmaxf(wx, a.x), b.x), wx), __fsub_rn(fminf(fmaxf(wy, a.y), b.y), wy),
+                          __fsub_rn(fminf(fmaxf(wz, a.z), b.z), wz));
+    if (bd > best) continue;
+    const uint32_t left = __float_as_uint(a.w), ro = __float_as_uint(b.w);
+    if (left == RKF_BVH_INVALID) {
+      if (ro < nobj) {
+        float du;
+        const float d = eval_obj<PREC>(s, objs[ro], wx, wy, wz, &du, lc);
+        if (d < best) {
+          best = d;
+          best_un = du;
+          best_i = ro;
+        }
+      }
+    } else if (sp < 31) {
+      stack[sp++] = left;
+      stack[sp++] = ro;
+    }
+  }
+  return best;
+}
 
 // Object set of a launch: several objects, exactly one, or exactly one that
 // qualifies for the empty-space path (voxelized, translation-only
@@ -569,6 +614,8 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                 }
               }
             }
+          } else if (!EMPTY_PATH && kp.use_bvh) {
+            best = eval_bvh<PREC>(s, sh_objs, kp.bvh, nobj, wx, wy, wz, best_un, best_i, lc);
           } else {
             best = eval_min<PREC, SINGLE>(s, sh_objs, 0, nobj, wx, wy, wz, best_un, best_i, lc);
           }
@@ -932,6 +979,8 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
     return fail(RKF_UNSUPPORTED, "march: more objects than the persistent kernel holds");
   if (c->obj_count() == 0) return fail(RKF_INVALID_ARG, "march: the scene has no objects");
   const bool tiled = p->strategy == RKF_STRATEGY_TILED;
+  const bool use_bvh = p->strategy == RKF_STRATEGY_BVH;
+  if (use_bvh && c->bvh_n == 0) return fail(RKF_INVALID_ARG, "march: the BVH strategy needs an imported BVH");
   std::vector<Segment> tiled_segs;
   TiledDev td;
   std::memset(&td, 0, sizeof(td));
@@ -961,9 +1010,12 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   kp.counter = counter;
   kp.p = *p;
   kp.p.scene.num_objects = c->obj_count();
-  const int obj = tiled && object_set(c) == detail::OBJ_SINGLE_EMPTY ? detail::OBJ_SINGLE : object_set(c);
+  const int obj =
+      (tiled || use_bvh) && object_set(c) == detail::OBJ_SINGLE_EMPTY ? detail::OBJ_SINGLE : object_set(c);
   kp.td = td;
   kp.tiled = tiled ? 1u : 0u;
+  kp.bvh = use_bvh ? c->bvh.as<rkf_bvh_node>() : nullptr;
+  kp.use_bvh = use_bvh ? 1u : 0u;
   kp.probe_min = obj == detail::OBJ_SINGLE_EMPTY ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
   kp.budget = tu.step_budget ? tu.step_budget : 32;
   kp.refill_active = 32u - std::min<uint32_t>(tu.refill_idle ? tu.refill_idle : 32u, 32u);
@@ -1013,7 +1065,7 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
                                      const rkf_march_params* p, const rkf_batch_tuning& tu,
                                      cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter) {
   if (p->strategy != RKF_STRATEGY_BRUTE)
-    return fail(RKF_UNSUPPORTED, "march: the tiled strategy needs tile-list scratch this launch path lacks");
+    return fail(RKF_UNSUPPORTED, "march: this launch path runs the brute strategy only");
   if (c->obj_count() > kMaxObjectsFast)
     return fail(RKF_UNSUPPORTED, "march: more objects than the persistent kernel holds");
   if (c->obj_count() == 0) return fail(RKF_INVALID_ARG, "march: the scene has no objects");

@@ -24,6 +24,31 @@ def _p(a):
     return None if a is None else a.ctypes.data
 
 
+def build_bvh(pairs) -> C.Array:
+    """``Bvh::build`` (crates/rkf-core/src/bvh.rs:66-260) over ``(object_index,
+    aabb_min, aabb_max)`` triples, as the GPU node array ``upload_bvh`` takes
+    (``GpuBvhNode::from_cpu``, gpu_bvh.rs:45-60); built on the host by the
+    library."""
+    pairs = list(pairs)
+    items = (abi.rkf_bvh_item * max(1, len(pairs)))()
+    for k, (oi, lo, hi) in enumerate(pairs):
+        items[k].object_index = int(oi)
+        for a in range(3):
+            items[k].aabb_min[a] = float(lo[a])
+            items[k].aabb_max[a] = float(hi[a])
+    cap = max(1, 2 * len(pairs) - 1)
+    nodes = (abi.rkf_bvh_node * cap)()
+    n = C.c_uint32()
+    check(abi.load_library().rkf_bvh_build(items, len(pairs), nodes, cap, C.byref(n)), "rkf_bvh_build")
+    return (abi.rkf_bvh_node * n.value).from_buffer_copy(nodes, 0) if n.value else (abi.rkf_bvh_node * 0)()
+
+
+def object_bvh(objects) -> C.Array:
+    """The BVH the runtime uploads with its objects: one leaf per object
+    index over the object's AABB (render.rs:79-140)."""
+    return build_bvh((i, o.aabb_min, o.aabb_max) for i, o in enumerate(objects))
+
+
 def gbuffer_host(n: int, reference_planes: bool = False) -> dict:
     out = {"t": np.zeros(n, np.float32), "normal": np.zeros(3 * n, np.float32),
            "slot": np.zeros(n, np.uint32), "material": np.zeros(n, np.uint16),
@@ -106,6 +131,10 @@ class Context:
     def upload_objects(self, objects):
         arr = (abi.rkf_gpu_object * len(objects))(*objects)
         check(self.lib.rkf_objects_import(self.h, arr, len(objects)), "rkf_objects_import")
+
+    def upload_bvh(self, nodes):
+        """BVH nodes, root first (an ``rkf_bvh_node`` array); an empty one removes the BVH."""
+        check(self.lib.rkf_bvh_import(self.h, nodes if len(nodes) else None, len(nodes)), "rkf_bvh_import")
 
     def voxelize(self, prims: np.ndarray, vp: abi.rkf_voxelize_params) -> int:
         prims = np.ascontiguousarray(prims)
@@ -334,6 +363,9 @@ class GpuScene:
 
     def upload_objects(self, objects):
         self.ctx.upload_objects(objects)
+
+    def upload_bvh(self, nodes):
+        self.ctx.upload_bvh(nodes)
 
 
 class RayMarchPass:
