@@ -238,6 +238,7 @@ SIGNATURES = {
     "rkf_pool_import_soa": (_I, [_P, _P, _P, _P, _U32, _U32]),
     "rkf_testing_fail_allocation_after": (None, [C.c_longlong]),
     "rkf_testing_export_empty_dist": (_I, [_P, _P, C.POINTER(C.c_uint64)]),
+    "rkf_testing_set_host_bands": (None, [C.c_int]),
     "rkf_world_relative": (None, [C.POINTER(rkf_world_pos), C.POINTER(rkf_world_pos),
                                   C.POINTER(C.c_double), C.POINTER(C.c_float)]),
 }

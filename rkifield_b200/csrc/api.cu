@@ -2,16 +2,23 @@
 //
 // Host-pointer outputs are staged in a context-owned device buffer and copied
 // back on the context stream; device-pointer outputs are written in place.
+// A large view with host outputs is marched in bands of tile rows, each
+// band's rows copied back on a second stream while the next band marches.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <vector>
 
+#include "../../include/rkf_cuda_testing.h"
 #include "ctx.h"
 #include "march.h"
 
 using namespace rkf;
 
 namespace detail {
+
+// Band count of host-output views: < 0 chooses by size (rkf_testing_*).
+std::atomic<int> g_host_bands{-1};
 
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
@@ -55,6 +62,91 @@ rkf_status copy_back_gbuffer(Ctx* c, const rkf_gbuffer& host, const rkf_gbuffer&
   RKF_CUDA_TRY(cp(host.position, dev.position, n * 16));
   RKF_CUDA_TRY(cp(host.packed_material, dev.packed_material, n * 4));
   RKF_CUDA_TRY(cp(host.motion, dev.motion, n * 16));
+  return RKF_OK;
+}
+
+// Bands of a host-output view of n rays: band b's copy overlaps the march
+// of the bands after it; only the last band's copy stays exposed.
+int host_bands(uint64_t n) {
+  const int forced = g_host_bands.load();
+  if (forced >= 0) return std::min(std::max(forced, 1), Ctx::kMaxBands);
+  return n >= (1u << 20) ? 3 : n >= (1u << 18) ? 2 : 1;  // measured best on a 1080p view
+}
+
+// rkf_march into host planes, band by band: tile rows [r0, r1) of the view
+// are the work ids [r0, r1) x tiles_x x tile area and write pixel rows
+// [r0 * tile_h, min(r1 * tile_h, h)), contiguous in every plane.  Bands
+// weigh 2 : 2 : ... : 1, so the last (exposed) copy is the smallest.  Bands
+// alternate between two streams with a work counter each: the launches do
+// not wait on one another, so band b + 1's blocks take the SMs that band
+// b's blocks free while its last rays finish.
+rkf_status march_host_banded(Ctx* c, const rkf_camera* cam, const rkf_march_params* p, uint32_t w,
+                             uint32_t h, const rkf_gbuffer& host, int bands) {
+  const uint64_t n = static_cast<uint64_t>(w) * h;
+  rkf_gbuffer dev;
+  rkf_status st = stage_gbuffer(c, host, n, &dev);
+  if (st != RKF_OK) return st;
+  for (cudaStream_t* s : {&c->copy_stream, &c->band_stream})
+    if (!*s) RKF_CUDA_TRY(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
+  for (int b = 0; b < bands; ++b)
+    if (!c->band_ev[b]) RKF_CUDA_TRY(cudaEventCreateWithFlags(&c->band_ev[b], cudaEventDisableTiming));
+  if (!c->segs_ev) RKF_CUDA_TRY(cudaEventCreateWithFlags(&c->segs_ev, cudaEventDisableTiming));
+  const rkf_batch_tuning& tu = c->tuning;
+  std::vector<Segment> segs{view_segment(cam, w, h, tu.tile_w, tu.tile_h, dev)};
+  segs[0].first = 0;
+  const size_t sb = sizeof(Segment);
+  if (c->seg_buf.bytes < sb && (st = c->seg_buf.alloc(sb)) != RKF_OK) return st;
+  RKF_CUDA_TRY(cudaMemcpyAsync(c->seg_buf.p, segs.data(), sb, cudaMemcpyHostToDevice, c->stream));
+  RKF_CUDA_TRY(cudaEventRecord(c->segs_ev, c->stream));
+  RKF_CUDA_TRY(cudaStreamWaitEvent(c->band_stream, c->segs_ev, 0));
+  const uint32_t tile_w = tu.tile_w ? tu.tile_w : 8, tile_h = tu.tile_h ? tu.tile_h : 4;
+  const uint64_t row_ids = static_cast<uint64_t>(segs[0].tiles_x) * tile_w * tile_h;
+  const uint32_t rows = (h + tile_h - 1) / tile_h;
+  const uint32_t weight = 2u * static_cast<uint32_t>(bands) - 1u;
+  // on an error, work already queued must finish before the caller's
+  // buffers are handed back
+  struct Drain {
+    Ctx* c;
+    ~Drain() {
+      cudaStreamSynchronize(c->copy_stream);
+      cudaStreamSynchronize(c->band_stream);
+      cudaStreamSynchronize(c->stream);
+    }
+  } drain{c};
+  // one counter per band, 64 bytes apart, past the counters other launches use
+  unsigned long long* counters = reinterpret_cast<unsigned long long*>(c->counters.as<char>() + 1024);
+  uint32_t r0 = 0;
+  for (int b = 0; b < bands && r0 < rows; ++b) {
+    const uint32_t r1 = b == bands - 1 ? rows
+                                       : std::min(rows, static_cast<uint32_t>(
+                                                            (static_cast<uint64_t>(rows) * 2u * (b + 1)) / weight));
+    if (r1 <= r0) continue;
+    cudaStream_t bs = (b & 1) ? c->band_stream : c->stream;
+    st = launch_persistent(c, segs, (r1 - r0) * row_ids, p, tu, bs, &c->seg_buf, counters + 8 * b,
+                           r0 * row_ids, true);
+    if (st != RKF_OK) return st;
+    RKF_CUDA_TRY(cudaEventRecord(c->band_ev[b], bs));
+    RKF_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, c->band_ev[b], 0));
+    const uint64_t p0 = static_cast<uint64_t>(r0) * tile_h * w;
+    const uint64_t p1 = std::min<uint64_t>(static_cast<uint64_t>(r1) * tile_h, h) * w;
+    auto cp = [&](void* dst, const void* src, size_t elem) -> cudaError_t {
+      if (!dst || !src) return cudaSuccess;
+      return cudaMemcpyAsync(static_cast<char*>(dst) + p0 * elem, static_cast<const char*>(src) + p0 * elem,
+                             (p1 - p0) * elem, cudaMemcpyDeviceToHost, c->copy_stream);
+    };
+    RKF_CUDA_TRY(cp(host.t, dev.t, 4));
+    RKF_CUDA_TRY(cp(host.normal, dev.normal, 12));
+    RKF_CUDA_TRY(cp(host.slot, dev.slot, 4));
+    RKF_CUDA_TRY(cp(host.material, dev.material, 2));
+    RKF_CUDA_TRY(cp(host.flags, dev.flags, 2));
+    RKF_CUDA_TRY(cp(host.position, dev.position, 16));
+    RKF_CUDA_TRY(cp(host.packed_material, dev.packed_material, 4));
+    RKF_CUDA_TRY(cp(host.motion, dev.motion, 16));
+    r0 = r1;
+  }
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->band_stream));
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return RKF_OK;
 }
 
@@ -109,6 +201,9 @@ rkf_status rkf_march(rkf_ctx* ctx, const rkf_camera* cam, const rkf_march_params
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   RKF_CUDA_TRY(cudaSetDevice(c->device));
   const uint64_t n = static_cast<uint64_t>(width) * height;
+  const int bands = host_bands(n);
+  if (out->mem == RKF_MEM_HOST && bands > 1 && p->strategy != RKF_STRATEGY_TILED)
+    return march_host_banded(c, cam, p, width, height, *out, bands);
   return run_gbuffer(c, out, n, [&](const rkf_gbuffer& dev) {
     const rkf_batch_tuning& tu = c->tuning;
     std::vector<Segment> segs{view_segment(cam, width, height, tu.tile_w, tu.tile_h, dev)};
@@ -347,5 +442,7 @@ rkf_status rkf_march_batch_async(rkf_ctx* ctx, const rkf_view* views, uint32_t n
   if (segs.empty()) return RKF_OK;
   return launch_persistent(c, segs, first, p, tu, strm, &c->seg_buf, c->counters.as<unsigned long long>());
 }
+
+void rkf_testing_set_host_bands(int bands) { detail::g_host_bands.store(bands < 0 ? -1 : bands); }
 
 }  // extern "C"

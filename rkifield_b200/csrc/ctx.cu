@@ -406,6 +406,14 @@ rkf_status rkf_destroy(rkf_ctx* ctx) {
   if (c->serve) rkf_serve_stop(ctx);
   cudaStreamSynchronize(c->stream);
   cudaStreamDestroy(c->stream);
+  for (cudaStream_t s : {c->copy_stream, c->band_stream})
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  for (cudaEvent_t e : c->band_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->segs_ev) cudaEventDestroy(c->segs_ev);
   delete c;
   return RKF_OK;
 }

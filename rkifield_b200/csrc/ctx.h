@@ -112,6 +112,14 @@ struct Ctx {
 
   // scratch reused by march calls (host-pointer outputs staged here)
   DevBuf stage;
+  // host-output views: band b marches on band_stream[b % 2] (so a band's
+  // launch fills the SMs its predecessor's last rays leave idle), and its
+  // rows go back on copy_stream once band_ev[b] has completed
+  static constexpr int kMaxBands = 8;
+  cudaStream_t copy_stream = nullptr;
+  cudaStream_t band_stream = nullptr;  // the second band stream; the first is `stream`
+  cudaEvent_t band_ev[kMaxBands] = {};
+  cudaEvent_t segs_ev = nullptr;
   DevBuf counters;   // work counters of the persistent kernels
   DevBuf seg_buf;    // segment table of the persistent kernel
   DevBuf l2_flush;

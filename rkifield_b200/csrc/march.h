@@ -37,9 +37,15 @@ Segment view_segment(const rkf_camera* cam, uint32_t w, uint32_t h, uint32_t til
                      uint32_t tile_h, const rkf_gbuffer& out);
 Segment ray_segment(const float* o, const float* d, const float* tmax, uint32_t n, uint32_t mode,
                     const rkf_hits& out);
+// Marches work ids id0 .. id0 + total - 1 of the segments (id0 > 0: a part
+// of the work, e.g. one band of tile rows of a view; not with the tiled
+// strategy, whose tile lists cover whole views).  segs_resident: seg_buf
+// already holds this segment table (a later part of the same work), so it
+// is not uploaded again.
 rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs, uint64_t total,
                              const rkf_march_params* p, const rkf_batch_tuning& tu,
-                             cudaStream_t st, DevBuf* seg_buf, unsigned long long* counter);
+                             cudaStream_t st, DevBuf* seg_buf, unsigned long long* counter,
+                             uint64_t id0 = 0, bool segs_resident = false);
 // Same launch as launch_persistent, with the segment table and work counter
 // in caller-provided device memory (it allocates nothing).
 rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t nseg, uint64_t total,

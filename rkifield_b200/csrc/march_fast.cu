@@ -55,7 +55,8 @@ struct KParams {
   uint32_t nseg;
   uint32_t tile_w, tile_h;
   uint32_t interval;
-  uint64_t total;
+  uint64_t total;          // work ids of this launch: id0 .. id0 + total - 1
+  uint64_t id0;
   unsigned long long* counter;
   rkf_march_params p;
   float probe_min;  // empty-space path: probe for a cube once a sample was at least this
@@ -415,8 +416,9 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
         base = __shfl_sync(kFull, base, leader);
         if (base + __popc(need) >= kp.total) exhausted = true;
         if (idle) {
-          const uint64_t id = base + __popc(need & ((1u << lane) - 1u));
-          if (id < kp.total) {
+          const uint64_t k = base + __popc(need & ((1u << lane) - 1u));
+          if (k < kp.total) {
+            const uint64_t id = kp.id0 + k;
             cs.seg = find_segment(kp.segs, kp.nseg, id);
             const Segment& sg = kp.segs[cs.seg];
             const uint64_t local = id - sg.first;
@@ -974,7 +976,8 @@ int object_set(const Ctx* c) {
 
 rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint64_t total,
                              const rkf_march_params* p, const rkf_batch_tuning& tu,
-                             cudaStream_t st, DevBuf* seg_buf, unsigned long long* counter) {
+                             cudaStream_t st, DevBuf* seg_buf, unsigned long long* counter, uint64_t id0,
+                             bool segs_resident) {
   if (c->obj_count() > kMaxObjectsFast)
     return fail(RKF_UNSUPPORTED, "march: more objects than the persistent kernel holds");
   if (c->obj_count() == 0) return fail(RKF_INVALID_ARG, "march: the scene has no objects");
@@ -991,11 +994,14 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   }
   const std::vector<Segment>& segs_dev = tiled ? tiled_segs : segs_host;
   const size_t sb = segs_dev.size() * sizeof(Segment);
-  if (seg_buf->bytes < sb) {
-    rkf_status s2 = seg_buf->alloc(sb);
-    if (s2 != RKF_OK) return s2;
+  if (!segs_resident || seg_buf->bytes < sb) {
+    if (seg_buf->bytes < sb) {
+      rkf_status s2 = seg_buf->alloc(sb);
+      if (s2 != RKF_OK) return s2;
+    }
+    // a pageable source: the call returns once the stream has taken the data
+    RKF_CUDA_TRY(cudaMemcpyAsync(seg_buf->p, segs_dev.data(), sb, cudaMemcpyHostToDevice, st));
   }
-  RKF_CUDA_TRY(cudaMemcpyAsync(seg_buf->p, segs_dev.data(), sb, cudaMemcpyHostToDevice, st));
   RKF_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
   detail::KParams kp;
   std::memset(&kp, 0, sizeof(kp));
@@ -1007,6 +1013,7 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   kp.tile_h = tu.tile_h ? tu.tile_h : 4;
   kp.interval = tu.compact_interval ? tu.compact_interval : 64;
   kp.total = total;
+  kp.id0 = id0;
   kp.counter = counter;
   kp.p = *p;
   kp.p.scene.num_objects = c->obj_count();

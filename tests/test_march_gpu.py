@@ -120,3 +120,27 @@ def test_objects_reimport_replaces_the_index(oracle, small_scene):
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("bands", [1, 2, 3, 8])
+def test_host_output_bands_bit_exact(oracle, small_scene, small_ctx, bands):
+    """rkf_march with host outputs marches large views in bands of tile rows
+    whose copies overlap the next band: every band count gives the oracle's
+    planes, on a height that is not a multiple of the tile height."""
+    from rkifield_b200 import _abi as abi, scenes
+    lib = abi.load_library()
+    spec = small_scene["spec"]
+    v = small_scene["vox"]
+    sc = oracle.Scene([small_scene["obj"]], pool_words=v.words, brick_maps=v.map)
+    w, h = 640, 429
+    cam = scenes.seeded_camera(spec, w, h, seed=31)
+    p = scenes.march_params(spec)
+    lib.rkf_testing_set_host_bands(bands)
+    try:
+        got = small_ctx.march(cam, p, w, h, reference_planes=True)
+    finally:
+        lib.rkf_testing_set_host_bands(-1)
+    ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+    assert ((ref["flags"] & 1) != 0).sum() > 1000
+    for k in PLANES:
+        assert_bits_equal(got[k], ref[k], f"{bands} bands {k}")
