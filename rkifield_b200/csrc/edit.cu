@@ -186,7 +186,27 @@ __global__ void k_scatter_top(uint32_t* top, const uint32_t* blocks, const uint3
 
 }  // namespace detail
 
-rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcome* out) {
+namespace {
+// A temporary device buffer: caller scratch when given, else an allocation.
+struct Temp {
+  DevBuf own;
+  void* p = nullptr;
+  rkf_status get(const EditScratch* scratch, size_t bytes) {
+    if (scratch) {
+      p = (*scratch)(bytes);
+      return p ? RKF_OK : fail(RKF_OOM, "rkf_edit_csg: no scratch room for the edit");
+    }
+    rkf_status st = own.alloc(bytes);
+    p = own.p;
+    return st;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+};
+}  // namespace
+
+rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcome* out,
+                      const EditScratch* scratch) {
   out->changed_bricks = 0;
   out->new_top.release();
   out->retired.clear();
@@ -239,8 +259,8 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   // current slots through the device index
   std::vector<uint32_t> cur(ncand_all);
   {
-    DevBuf b;
-    rkf_status s2 = b.alloc(static_cast<size_t>(ncand_all) * 16);
+    Temp b;
+    rkf_status s2 = b.get(scratch, static_cast<size_t>(ncand_all) * 16);
     if (s2 != RKF_OK) return s2;
     RKF_CUDA_TRY(cudaMemcpyAsync(b.p, bxyz.data(), bxyz.size() * 4, cudaMemcpyHostToDevice, st));
     rkf_status s3 = lookup_bricks(c, op.object_index, b.as<uint32_t>(), ncand_all,
@@ -283,8 +303,8 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
     out->new_top.release();
     out->new_empty_dist.release();
   });
-  DevBuf dargs;
-  rkf_status s2 = dargs.alloc(static_cast<size_t>(n) * 24 + 256);
+  Temp dargs;
+  rkf_status s2 = dargs.get(scratch, static_cast<size_t>(n) * 24 + 256);
   if (s2 != RKF_OK) return s2;
   uint32_t* d_src = dargs.as<uint32_t>();
   uint32_t* d_dst = d_src + n;
@@ -345,8 +365,8 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   }
   const uint32_t nb = static_cast<uint32_t>(blocks.size());
   if ((s2 = c->ensure_leaf_capacity(c->n_leaves + nb)) != RKF_OK) return s2;
-  DevBuf g;
-  if ((s2 = g.alloc(static_cast<size_t>(nb) * (4 + 4 + 2048) + 256)) != RKF_OK) return s2;
+  Temp g;
+  if ((s2 = g.get(scratch, static_cast<size_t>(nb) * (4 + 4 + 2048) + 256)) != RKF_OK) return s2;
   uint32_t* d_blocks = g.as<uint32_t>();
   uint32_t* d_topv = d_blocks + nb;
   uint32_t* d_leafs = d_topv + nb;

@@ -1,6 +1,7 @@
 // edit.h — device CSG edits (edit.cu) and the brick lookup they use.
 #pragma once
 
+#include <functional>
 #include <vector>
 
 #include "ctx.h"
@@ -14,10 +15,17 @@ struct EditOutcome {
   std::vector<uint32_t> retired;  // slots the new epoch no longer references
 };
 
+// Device scratch for an edit's temporaries (nullptr: none left).  The memory
+// must stay untouched by other work until the edit's stream is synchronised.
+using EditScratch = std::function<void*(size_t bytes)>;
+
 // Applies one edit; on success with changed bricks, out->new_top holds the
 // new epoch's top grid (the caller publishes it) and out->retired the slots
-// to free once no work reads the previous epoch.  Synchronises `st`.
-rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcome* out);
+// to free once no work reads the previous epoch.  Synchronises `st`.  With
+// scratch, the temporaries come from it instead of device allocations (whose
+// release would wait for every stream of the device).
+rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcome* out,
+                      const EditScratch* scratch = nullptr);
 
 // Slots (or sentinels) of n bricks (bxyz: 3 u32 each, device) of object obj
 // through the current index, into d_out (device).  Enqueued on st.

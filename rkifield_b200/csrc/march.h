@@ -47,10 +47,13 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs, uint64_t 
                              cudaStream_t st, DevBuf* seg_buf, unsigned long long* counter,
                              uint64_t id0 = 0, bool segs_resident = false);
 // Same launch as launch_persistent, with the segment table and work counter
-// in caller-provided device memory (it allocates nothing).
+// in caller-provided device memory (it allocates nothing).  segs_uploaded:
+// the caller has already queued the copy of the table into dev_segs on st
+// (from page-locked memory, so that enqueueing never waits on the stream).
 rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t nseg, uint64_t total,
                                      const rkf_march_params* p, const rkf_batch_tuning& tu,
-                                     cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter);
+                                     cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter,
+                                     bool segs_uploaded = false);
 rkf_status launch_trace_plain(Ctx* c, const float* o, const float* d, const float* tmax, uint32_t n,
                               uint32_t mode, const rkf_march_params* p, const rkf_hits& out,
                               cudaStream_t st);

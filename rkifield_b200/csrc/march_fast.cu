@@ -1070,13 +1070,15 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
 
 rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t nseg, uint64_t total,
                                      const rkf_march_params* p, const rkf_batch_tuning& tu,
-                                     cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter) {
+                                     cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter,
+                                     bool segs_uploaded) {
   if (p->strategy != RKF_STRATEGY_BRUTE)
     return fail(RKF_UNSUPPORTED, "march: this launch path runs the brute strategy only");
   if (c->obj_count() > kMaxObjectsFast)
     return fail(RKF_UNSUPPORTED, "march: more objects than the persistent kernel holds");
   if (c->obj_count() == 0) return fail(RKF_INVALID_ARG, "march: the scene has no objects");
-  RKF_CUDA_TRY(cudaMemcpyAsync(dev_segs, segs_host, sizeof(Segment) * nseg, cudaMemcpyHostToDevice, st));
+  if (!segs_uploaded)
+    RKF_CUDA_TRY(cudaMemcpyAsync(dev_segs, segs_host, sizeof(Segment) * nseg, cudaMemcpyHostToDevice, st));
   RKF_CUDA_TRY(cudaMemsetAsync(dev_counter, 0, sizeof(unsigned long long), st));
   detail::KParams kp;
   std::memset(&kp, 0, sizeof(kp));

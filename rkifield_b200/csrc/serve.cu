@@ -17,6 +17,7 @@
 // ticks are never disturbed.  During a session retired brick slots are not
 // reused (they return to the pool at rkf_serve_stop), which keeps slot numbers
 // -- and so every output -- a function of the request and its epoch alone.
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <map>
@@ -87,6 +88,48 @@ struct Tick {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<uint64_t> ids;
   std::vector<std::pair<size_t, size_t>> blocks;
+  int pinned = -1;  // page-locked staging block of the segment table
+};
+
+// Page-locked host blocks for segment tables: a copy from pageable memory
+// may wait for the stream to drain before it is queued, which would hold the
+// worker until an earlier tick on that stream finished.  A block returns to
+// the pool when its tick completes.
+struct PinnedPool {
+  struct Block {
+    void* p = nullptr;
+    size_t cap = 0;
+    bool used = false;
+  };
+  std::vector<Block> blocks;
+  int get(size_t bytes) {
+    for (size_t i = 0; i < blocks.size(); ++i)
+      if (!blocks[i].used && blocks[i].cap >= bytes) {
+        blocks[i].used = true;
+        return static_cast<int>(i);
+      }
+    Block b;
+    b.cap = std::max<size_t>(bytes, 64 << 10);
+    if (cudaHostAlloc(&b.p, b.cap, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      return -1;
+    }
+    b.used = true;
+    blocks.push_back(b);
+    return static_cast<int>(blocks.size() - 1);
+  }
+  void put(int i) {
+    if (i >= 0) blocks[static_cast<size_t>(i)].used = false;
+  }
+  // page-locked allocation waits for the device: make the usual blocks when
+  // the session starts
+  void reserve(int n, size_t bytes) {
+    for (int i = 0; i < n; ++i) put(get(bytes));
+  }
+  void release() {  // every stream that read the blocks has been synchronised
+    for (Block& b : blocks) cudaFreeHost(b.p);
+    blocks.clear();
+  }
 };
 
 double now_us(std::chrono::steady_clock::time_point t0) {
@@ -127,6 +170,7 @@ struct ServeState {
   cudaStream_t edit_stream = nullptr;
   int next_stream = 0;
   Arena arena;
+  PinnedPool pinned;
   std::deque<Tick> ticks;
   std::vector<DevBuf*> old_tops;
   std::vector<uint32_t> retired;
@@ -148,7 +192,18 @@ void ServeState::do_edit(uint64_t id) {
     tickets[id].state = 1;
   }
   EditOutcome out;
-  rkf_status st = apply_edit(c, op, edit_stream, &out);
+  // temporaries from the arena: freeing device memory would wait for every
+  // tick in flight
+  std::vector<std::pair<size_t, size_t>> taken;
+  const EditScratch scratch = [&](size_t bytes) -> void* {
+    size_t off;
+    if (!arena.alloc(bytes, &off)) return nullptr;
+    taken.emplace_back(off, bytes);
+    return arena.at(off);
+  };
+  rkf_status st = apply_edit(c, op, edit_stream, &out, &scratch);
+  cudaStreamSynchronize(edit_stream);  // error paths may return with work queued
+  for (auto& t : taken) arena.release(t.first, t.second);
   if (st == RKF_OK && out.new_top.p) {
     DevBuf* old = new DevBuf();
     std::swap(old->p, c->top.p);
@@ -282,9 +337,18 @@ bool ServeState::launch_tick(std::vector<uint64_t>& ids) {
     const size_t need = sizeof(Segment) * segs.size() + 256;
     if (arena.alloc(need, &off)) {
       tick.blocks.emplace_back(off, need);
+      Segment* dev_segs = reinterpret_cast<Segment*>(arena.at(off) + 256);
+      const size_t sb = sizeof(Segment) * segs.size();
+      tick.pinned = pinned.get(sb);
+      bool uploaded = false;
+      if (tick.pinned >= 0) {
+        void* hp = pinned.blocks[static_cast<size_t>(tick.pinned)].p;
+        std::memcpy(hp, segs.data(), sb);
+        uploaded = cudaMemcpyAsync(dev_segs, hp, sb, cudaMemcpyHostToDevice, st) == cudaSuccess;
+      }
       lst = launch_persistent_scratch(c, segs.data(), static_cast<uint32_t>(segs.size()), first, &p, c->tuning,
-                                      st, reinterpret_cast<Segment*>(arena.at(off) + 256),
-                                      reinterpret_cast<unsigned long long*>(arena.at(off)));
+                                      st, dev_segs, reinterpret_cast<unsigned long long*>(arena.at(off)),
+                                      uploaded);
     } else {
       lst = fail(RKF_OOM, "serve: no arena room for the segment table");
     }
@@ -340,6 +404,7 @@ void ServeState::poll_ticks() {
       cudaEventElapsedTime(&ms, it->ev0, it->ev1);
       const double done = now_us(t0);
       for (auto& bl : it->blocks) arena.release(bl.first, bl.second);
+      pinned.put(it->pinned);
       {
         std::lock_guard<std::mutex> lk(mu);
         for (uint64_t id : it->ids) {
@@ -428,6 +493,7 @@ rkf_status rkf_serve_start(rkf_ctx* ctx, const rkf_march_params* p) {
   }
   for (auto& strm : s->streams) cudaStreamCreateWithFlags(&strm, cudaStreamNonBlocking);
   cudaStreamCreateWithFlags(&s->edit_stream, cudaStreamNonBlocking);
+  s->pinned.reserve(2 * ServeState::kStreams, 256 << 10);
   c->leaves_frozen = true;
   c->serve = s;
   s->worker = std::thread([s] { s->run(); });
@@ -451,6 +517,7 @@ rkf_status rkf_serve_stop(rkf_ctx* ctx) {
   }
   cudaStreamSynchronize(s->edit_stream);
   cudaStreamDestroy(s->edit_stream);
+  s->pinned.release();
   for (DevBuf* d : s->old_tops) delete d;
   for (uint32_t slot : s->retired) c->free_slots.push_back(slot);
   c->used_slots -= static_cast<uint32_t>(s->retired.size());
