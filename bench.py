@@ -165,6 +165,12 @@ def barrier(dist):
         dist.barrier()
 
 
+def job_mrays(dist, world: int, rays_per_rank: int, steps: int, seconds: float) -> float:
+    """Whole-job rate of replicas: every rank marches rays_per_rank rays per
+    step; the job takes as long as its slowest rank."""
+    return world * rays_per_rank * steps / dist_max(dist, seconds) / 1e6
+
+
 def oracle_scene_from_ctx(ctx, oracle):
     info = ctx.info()
     words = ctx.export_pool(0, info["pool_bricks_used"])
@@ -744,9 +750,7 @@ def run_b200(args, world, rank, local, dist):
     clk = ClockSampler(local)
     with clk:
         ms, wall = timed(False, args.steps, args.warmup)
-    dev_s = sum(ms) / 1e3
-    dev_s_max = dist_max(dist, dev_s)
-    value = world * n * args.steps / dev_s_max / 1e6
+    value = job_mrays(dist, world, n, args.steps, sum(ms) / 1e3)
     lat = {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99)),
            "max": float(np.max(ms))}
 
@@ -754,8 +758,7 @@ def run_b200(args, world, rank, local, dist):
     if not args.no_plain:
         psteps = max(3, args.steps // 4)
         pms, _ = timed(True, psteps, 1)
-        pdev = dist_max(dist, sum(pms) / 1e3)
-        pval = world * n * psteps / pdev / 1e6
+        pval = job_mrays(dist, world, n, psteps, sum(pms) / 1e3)
         plain = {"value": pval, "unit": "Mrays/s", "steps": psteps,
                  "latency_ms": {"p50": float(np.percentile(pms, 50)), "p99": float(np.percentile(pms, 99))},
                  "kernel": "k_march_plain (reference AoS pool, one thread per ray, one launch per view)"}
@@ -769,8 +772,7 @@ def run_b200(args, world, rank, local, dist):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         ctx.march(cam, p, w, h, out=host_out)
-    e2e_s = dist_max(dist, time.perf_counter() - t0)
-    e2e_val = world * n * args.steps / e2e_s / 1e6
+    e2e_val = job_mrays(dist, world, n, args.steps, time.perf_counter() - t0)
     d2h = sum(v.nbytes for v in host_out.values())
     h2d = 144 + 32  # camera uniforms + march parameters
 
