@@ -22,6 +22,7 @@ without a graphics stack) on all host threads, on a bounded ray sample.
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import os
 import subprocess
@@ -85,7 +86,9 @@ def camera_for(spec, w, h, rank):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """nvidia-smi clocks and throttle reasons during the timed regions:
+    polled every 20 ms from before the first timed region to after the last;
+    the summary counts the samples taken inside a window()."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -94,22 +97,35 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.lines = []
+        self.lines = []    # (arrival time, csv line)
+        self.windows = []  # timed regions (perf_counter start, end)
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the first query takes a while: start timing once samples flow
+            t_end = time.perf_counter() + 5.0
+            while not self.lines and time.perf_counter() < t_end and self.proc.poll() is None:
+                time.sleep(0.005)
         except FileNotFoundError:
             self.proc = None
         return self
 
     def _read(self):
         for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
+            self.lines.append((time.perf_counter(), ln.strip()))
+
+    @contextlib.contextmanager
+    def window(self):
+        t0 = time.perf_counter()
+        try:
+            yield
+        finally:
+            self.windows.append((t0, time.perf_counter()))
 
     def __exit__(self, *a):
         if self.proc:
@@ -122,7 +138,10 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        # a line arrives up to one query (a few ms) after its sample was taken
+        inside = [ln for t, ln in self.lines
+                  if not self.windows or any(a <= t <= b + 0.02 for a, b in self.windows)]
+        for ln in inside:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -747,32 +766,37 @@ def run_b200(args, world, rank, local, dist):
         ms = [a.elapsed_ms(b) for a, b in ev]
         return ms, wall
 
-    clk = ClockSampler(local)
-    with clk:
-        ms, wall = timed(False, args.steps, args.warmup)
-    value = job_mrays(dist, world, n, args.steps, sum(ms) / 1e3)
-    lat = {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99)),
-           "max": float(np.max(ms))}
-
-    plain = None
-    if not args.no_plain:
-        psteps = max(3, args.steps // 4)
-        pms, _ = timed(True, psteps, 1)
-        pval = job_mrays(dist, world, n, psteps, sum(pms) / 1e3)
-        plain = {"value": pval, "unit": "Mrays/s", "steps": psteps,
-                 "latency_ms": {"p50": float(np.percentile(pms, 50)), "p99": float(np.percentile(pms, 99))},
-                 "kernel": "k_march_plain (reference AoS pool, one thread per ray, one launch per view)"}
-
     # e2e: public host-buffer call; pinned host G-buffer copied back each step
     pin = {k: cudart.PinnedArray(v.size, v.dtype) for k, v in gbuffer_host(n).items()}
     host_out = {k: v.array for k, v in pin.items()}
-    for _ in range(args.warmup):
-        ctx.march(cam, p, w, h, out=host_out)
-    barrier(dist)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        ctx.march(cam, p, w, h, out=host_out)
-    e2e_val = job_mrays(dist, world, n, args.steps, time.perf_counter() - t0)
+
+    clk = ClockSampler(local)
+    plain = None
+    with clk:
+        with clk.window():
+            ms, wall = timed(False, args.steps, args.warmup)
+        value = job_mrays(dist, world, n, args.steps, sum(ms) / 1e3)
+        lat = {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99)),
+               "max": float(np.max(ms))}
+
+        if not args.no_plain:
+            psteps = max(3, args.steps // 4)
+            with clk.window():
+                pms, _ = timed(True, psteps, 1)
+            pval = job_mrays(dist, world, n, psteps, sum(pms) / 1e3)
+            plain = {"value": pval, "unit": "Mrays/s", "steps": psteps,
+                     "latency_ms": {"p50": float(np.percentile(pms, 50)), "p99": float(np.percentile(pms, 99))},
+                     "kernel": "k_march_plain (reference AoS pool, one thread per ray, one launch per view)"}
+
+        for _ in range(args.warmup):
+            ctx.march(cam, p, w, h, out=host_out)
+        barrier(dist)
+        with clk.window():
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                ctx.march(cam, p, w, h, out=host_out)
+            e2e_s = time.perf_counter() - t0
+        e2e_val = job_mrays(dist, world, n, args.steps, e2e_s)
     d2h = sum(v.nbytes for v in host_out.values())
     h2d = 144 + 32  # camera uniforms + march parameters
 
