@@ -492,7 +492,11 @@ rkf_status rkf_serve_start(rkf_ctx* ctx, const rkf_march_params* p) {
     return st;
   }
   for (auto& strm : s->streams) cudaStreamCreateWithFlags(&strm, cudaStreamNonBlocking);
-  cudaStreamCreateWithFlags(&s->edit_stream, cudaStreamNonBlocking);
+  // edits hold up every request behind them: their small kernels take free
+  // SM slots ahead of queued ticks
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  cudaStreamCreateWithPriority(&s->edit_stream, cudaStreamNonBlocking, prio_high);
   s->pinned.reserve(2 * ServeState::kStreams, 256 << 10);
   c->leaves_frozen = true;
   c->serve = s;

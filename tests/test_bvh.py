@@ -346,3 +346,50 @@ def test_bvh_import_checks(small_scene):
         assert e.value.status == abi.RKF_INVALID_ARG
     finally:
         ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f32", "u8"])
+@pytest.mark.parametrize("strategy", ["bvh", "tiled"])
+def test_strategies_over_precision_planes_bit_exact(oracle, small_scene, precision, strategy):
+    """The BVH and tiled marches over the f32 and u8 distance planes, against
+    the oracle reading the same planes and index; the BVH march also through
+    three bands of host-output rows."""
+    from rkifield_b200 import _abi as abi
+    from rkifield_b200.engine import Context
+    v = small_scene["vox"]
+    objs = _objects(small_scene)
+    bvh = _scene_bvh(objs)
+    ctx = Context(pool_capacity=v.n_bricks + 1024, precision=precision)
+    try:
+        ctx.set_brick_pool(v.words)
+        ctx.upload_brick_maps(v.map)
+        ctx.upload_objects(objs)
+        ctx.upload_bvh(bvh)
+        pl = ctx.export_planes(0, v.n_bricks)
+        idx = ctx.export_index()
+        if precision == "f32":
+            kw = {"dist_f32": pl["dist"], "precision": abi.RKF_PRECISION_F32}
+        else:
+            kw = {"dist_u8": pl["dist"], "brick_scale": pl["step"], "precision": abi.RKF_PRECISION_U8}
+        sc = oracle.Scene(objs, top=idx["top"], leaves=idx["leaves"], obj_top_info=idx["obj_top_info"],
+                          mat_plane=pl["mat"], blend_plane=pl["blend"], bvh=bvh, **kw)
+        w, h = 200, 136
+        cam = _camera(4, w, h)
+        p = _params(abi.RKF_STRATEGY_BVH if strategy == "bvh" else abi.RKF_STRATEGY_TILED)
+        ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+        got = ctx.march(cam, p, w, h, reference_planes=True)
+        assert ((ref["flags"] & 1) != 0).sum() > 500
+        for k in PLANES:
+            assert_bits_equal(got[k], ref[k], f"{strategy} {precision} {k}")
+        if strategy == "bvh":
+            lib = abi.load_library()
+            lib.rkf_testing_set_host_bands(3)
+            try:
+                banded = ctx.march(cam, p, w, h, reference_planes=True)
+            finally:
+                lib.rkf_testing_set_host_bands(-1)
+            for k in PLANES:
+                assert_bits_equal(banded[k], ref[k], f"banded {strategy} {precision} {k}")
+    finally:
+        ctx.close()
