@@ -745,6 +745,20 @@ def run_b200(args, world, rank, local, dist):
     g = cudart.device_gbuffer(n)
     gp = cudart.gbuffer_ptrs(g)
     flush = cudart.DeviceArray(256 << 20, np.uint8)
+    # set-up, untimed: the autotuner picks the launch tuning for this view and
+    # stores it in the context, as a renderer would do once
+    import ctypes as C
+    vw = (abi.rkf_view * 1)()
+    vw[0].camera = cam
+    vw[0].width, vw[0].height = w, h
+    for k, a in g.items():
+        setattr(vw[0].out, k, a.ptr)
+    vw[0].out.mem = abi.RKF_MEM_DEVICE
+    tu = abi.rkf_batch_tuning()
+    t0 = time.perf_counter()
+    abi.check(ctx.lib.rkf_autotune(ctx.h, vw, 1, None, 0, C.byref(p), C.byref(tu)), "autotune")
+    tuning = {k: getattr(tu, k) for k, _ in abi.rkf_batch_tuning._fields_}
+    tuning["tune_s"] = time.perf_counter() - t0
 
     def timed(plain: bool, steps: int, warmup: int):
         for _ in range(warmup):
@@ -866,7 +880,7 @@ def run_b200(args, world, rank, local, dist):
                        "bricks": info["pool_bricks_used"], "leaf_blocks": info["leaf_blocks"],
                        "build_s": build_s, "hit_fraction": hits / n,
                        "l2": "256 MiB flush between steps, outside the timed events",
-                       "parallelism": f"replicas x{world}"},
+                       "tuning": tuning, "parallelism": f"replicas x{world}"},
             "latency_ms": lat,
             "plain": plain,
             "vs_plain": (value / plain["value"]) if plain else None,
