@@ -208,6 +208,7 @@ struct Temp {
 rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcome* out,
                       const EditScratch* scratch) {
   out->changed_bricks = 0;
+  out->new_epoch = false;
   out->new_top.release();
   out->retired.clear();
   if (op.object_index >= c->obj_count()) return fail(RKF_INVALID_ARG, "rkf_edit_csg: object index out of range");
@@ -386,15 +387,18 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   for (uint32_t i = 0; i < nb; ++i) newtop[i] = c->n_leaves + i;
   RKF_CUDA_TRY(cudaMemcpyAsync(c->leaves.as<uint32_t>() + static_cast<size_t>(c->n_leaves) * 512, leafv.data(),
                                leafv.size() * 4, cudaMemcpyHostToDevice, st));
-  if ((s2 = out->new_top.alloc(std::max<uint64_t>(c->top_len, 1) * 4)) != RKF_OK) return s2;
-  RKF_CUDA_TRY(cudaMemcpyAsync(out->new_top.p, c->top.p, c->top_len * 4, cudaMemcpyDeviceToDevice, st));
+  const bool into = out->top_dst && out->field_dst;
+  if (!into && (s2 = out->new_top.alloc(std::max<uint64_t>(c->top_len, 1) * 4)) != RKF_OK) return s2;
+  uint32_t* ntop = into ? out->top_dst : out->new_top.as<uint32_t>();
+  RKF_CUDA_TRY(cudaMemcpyAsync(ntop, c->top.p, c->top_len * 4, cudaMemcpyDeviceToDevice, st));
   RKF_CUDA_TRY(cudaMemcpyAsync(d_topv, newtop.data(), nb * 4ull, cudaMemcpyHostToDevice, st));
-  detail::k_scatter_top<<<(nb + 127) / 128, 128, 0, st>>>(out->new_top.as<uint32_t>(), d_blocks, d_topv, nb);
+  detail::k_scatter_top<<<(nb + 127) / 128, 128, 0, st>>>(ntop, d_blocks, d_topv, nb);
   RKF_CUDA_TRY(cudaGetLastError());
   // the touched blocks are leaf blocks now: lower the field around them
-  if ((s2 = out->new_empty_dist.alloc(std::max<uint64_t>(c->top_len, 1))) != RKF_OK) return s2;
-  RKF_CUDA_TRY(cudaMemcpyAsync(out->new_empty_dist.p, c->empty_dist.p, c->top_len, cudaMemcpyDeviceToDevice, st));
-  if ((s2 = lower_empty_dist(od, out->new_empty_dist.as<uint8_t>(), d_blocks, blocks, st)) != RKF_OK) return s2;
+  if (!into && (s2 = out->new_empty_dist.alloc(std::max<uint64_t>(c->top_len, 1))) != RKF_OK) return s2;
+  uint8_t* nfield = into ? out->field_dst : out->new_empty_dist.as<uint8_t>();
+  RKF_CUDA_TRY(cudaMemcpyAsync(nfield, c->empty_dist.p, c->top_len, cudaMemcpyDeviceToDevice, st));
+  if ((s2 = lower_empty_dist(od, nfield, d_blocks, blocks, st)) != RKF_OK) return s2;
   c->n_leaves += nb;
   // the reference flat map (read only by the plain march) is updated in place
   if (od.has_flat && !c->flat_host.empty()) {
@@ -408,6 +412,7 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   }
   RKF_CUDA_TRY(cudaStreamSynchronize(st));
   undo.dismiss();
+  out->new_epoch = true;
   return RKF_OK;
 }
 

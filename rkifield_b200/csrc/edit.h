@@ -10,9 +10,14 @@ namespace rkf {
 
 struct EditOutcome {
   uint32_t changed_bricks = 0;
-  DevBuf new_top;                 // top grid of the new epoch (empty: no change)
-  DevBuf new_empty_dist;          // its empty-space distance field
+  bool new_epoch = false;         // the edit changed bricks: a new top grid and field exist
+  DevBuf new_top;                 // top grid of the new epoch (unless written to top_dst)
+  DevBuf new_empty_dist;          // its empty-space distance field (unless field_dst)
   std::vector<uint32_t> retired;  // slots the new epoch no longer references
+  // optional caller memory for the new epoch (top_len u32 / top_len bytes);
+  // when both are set nothing is allocated for it
+  uint32_t* top_dst = nullptr;
+  uint8_t* field_dst = nullptr;
 };
 
 // Device scratch for an edit's temporaries (nullptr: none left).  The memory

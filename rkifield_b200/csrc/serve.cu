@@ -89,6 +89,7 @@ struct Tick {
   std::vector<uint64_t> ids;
   std::vector<std::pair<size_t, size_t>> blocks;
   int pinned = -1;  // page-locked staging block of the segment table
+  uint64_t epoch = 0;  // index epoch the tick's launches read
 };
 
 // Page-locked host blocks for segment tables: a copy from pageable memory
@@ -173,6 +174,13 @@ struct ServeState {
   PinnedPool pinned;
   std::deque<Tick> ticks;
   std::vector<DevBuf*> old_tops;
+  // Top grid + field pairs for new epochs.  An edit writes its epoch into a
+  // spare pair (a device allocation could wait for the ticks in flight); the
+  // pair it replaces retires with the old epoch number and becomes a spare
+  // once no tick of that epoch or earlier is in flight.
+  std::vector<std::pair<DevBuf*, DevBuf*>> spares;
+  std::vector<std::pair<uint64_t, std::pair<DevBuf*, DevBuf*>>> retiring;
+  void recycle();
   std::vector<uint32_t> retired;
   rkf_status error = RKF_OK;
   std::string error_msg;
@@ -192,6 +200,13 @@ void ServeState::do_edit(uint64_t id) {
     tickets[id].state = 1;
   }
   EditOutcome out;
+  std::pair<DevBuf*, DevBuf*> spare{nullptr, nullptr};
+  if (!spares.empty()) {
+    spare = spares.back();
+    spares.pop_back();
+    out.top_dst = spare.first->as<uint32_t>();
+    out.field_dst = spare.second->as<uint8_t>();
+  }
   // temporaries from the arena: freeing device memory would wait for every
   // tick in flight
   std::vector<std::pair<size_t, size_t>> taken;
@@ -204,7 +219,17 @@ void ServeState::do_edit(uint64_t id) {
   rkf_status st = apply_edit(c, op, edit_stream, &out, &scratch);
   cudaStreamSynchronize(edit_stream);  // error paths may return with work queued
   for (auto& t : taken) arena.release(t.first, t.second);
-  if (st == RKF_OK && out.new_top.p) {
+  if (st == RKF_OK && out.new_epoch && spare.first) {
+    // the spare pair becomes the index; the old pair retires at this epoch
+    std::swap(c->top.p, spare.first->p);
+    std::swap(c->top.bytes, spare.first->bytes);
+    std::swap(c->empty_dist.p, spare.second->p);
+    std::swap(c->empty_dist.bytes, spare.second->bytes);
+    retiring.push_back({c->epoch, spare});
+    spare = {nullptr, nullptr};
+    retired.insert(retired.end(), out.retired.begin(), out.retired.end());
+    c->epoch++;
+  } else if (st == RKF_OK && out.new_epoch) {
     DevBuf* old = new DevBuf();
     std::swap(old->p, c->top.p);
     std::swap(old->bytes, c->top.bytes);
@@ -220,6 +245,7 @@ void ServeState::do_edit(uint64_t id) {
     retired.insert(retired.end(), out.retired.begin(), out.retired.end());
     c->epoch++;
   }
+  if (spare.first) spares.push_back(spare);  // unused: no new epoch
   std::lock_guard<std::mutex> lk(mu);
   TicketRec& t = tickets[id];
   t.res.status = st;
@@ -242,6 +268,7 @@ bool ServeState::launch_tick(std::vector<uint64_t>& ids) {
   std::vector<std::pair<const rkf_request*, rkf_gbuffer>> renders;
   std::vector<std::pair<const rkf_request*, rkf_hits>> rays;
   const uint64_t epoch = c->epoch;
+  tick.epoch = epoch;
   const double start = now_us(t0);
   for (uint64_t id : ids) {
     TicketRec* tr;
@@ -426,6 +453,20 @@ void ServeState::poll_ticks() {
     }
     if (!progressed) break;
   }
+  recycle();
+}
+
+void ServeState::recycle() {
+  uint64_t oldest = ~0ull;
+  for (const Tick& t : ticks) oldest = std::min(oldest, t.epoch);
+  for (auto it = retiring.begin(); it != retiring.end();) {
+    if (it->first < oldest) {
+      spares.push_back(it->second);
+      it = retiring.erase(it);
+    } else {
+      ++it;
+    }
+  }
 }
 
 void ServeState::run() {
@@ -498,6 +539,18 @@ rkf_status rkf_serve_start(rkf_ctx* ctx, const rkf_march_params* p) {
   cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   cudaStreamCreateWithPriority(&s->edit_stream, cudaStreamNonBlocking, prio_high);
   s->pinned.reserve(2 * ServeState::kStreams, 256 << 10);
+  for (int i = 0; i < 2; ++i) {
+    auto* tp = new DevBuf();
+    auto* fp = new DevBuf();
+    if (tp->alloc(std::max<uint64_t>(c->top_len, 1) * 4) == RKF_OK &&
+        fp->alloc(std::max<uint64_t>(c->top_len, 1)) == RKF_OK) {
+      s->spares.push_back({tp, fp});
+    } else {  // no spares: edits allocate their epochs
+      delete tp;
+      delete fp;
+      cudaGetLastError();
+    }
+  }
   c->leaves_frozen = true;
   c->serve = s;
   s->worker = std::thread([s] { s->run(); });
@@ -523,6 +576,14 @@ rkf_status rkf_serve_stop(rkf_ctx* ctx) {
   cudaStreamDestroy(s->edit_stream);
   s->pinned.release();
   for (DevBuf* d : s->old_tops) delete d;
+  for (auto& pr : s->spares) {
+    delete pr.first;
+    delete pr.second;
+  }
+  for (auto& r : s->retiring) {
+    delete r.second.first;
+    delete r.second.second;
+  }
   for (uint32_t slot : s->retired) c->free_slots.push_back(slot);
   c->used_slots -= static_cast<uint32_t>(s->retired.size());
   c->leaves_frozen = false;
