@@ -352,9 +352,10 @@ typedef struct rkf_gbuffer {
 /* The B200 march: SoA distance plane at the context precision, two-level
  * brick index with empty-brick read skipping, warp-compacted persistent
  * kernel.  Bit-identical results to the reference algorithm in FP32.  With
- * host outputs, a view of 256K rays or more (brute and BVH strategies) is
- * marched in bands of rows whose copies to the host overlap the next band's
- * march; the call returns once every output is written. */
+ * host outputs, a view of 256K rays or more (brute and BVH strategies) in
+ * page-locked host planes is marched in bands of rows whose copies to the
+ * host overlap the next band's march; the call returns once every output is
+ * written. */
 RKF_API rkf_status rkf_march(rkf_ctx* ctx, const rkf_camera* cam, const rkf_march_params* p,
                      uint32_t width, uint32_t height, rkf_gbuffer* out);
 

@@ -25,8 +25,9 @@ RKF_API void rkf_testing_fail_allocation_after(long long n);
 RKF_API rkf_status rkf_testing_export_empty_dist(rkf_ctx* ctx, uint8_t* out, uint64_t* n);
 
 /* Number of bands rkf_march uses for a view with host outputs (1 = one
- * launch, then the copies; at most 8); bands < 0 restores the choice by
- * view size.  Process-wide. */
+ * launch, then the copies; at most 8), whatever the view's size and whether
+ * or not its planes are page-locked; bands < 0 restores the choice by view
+ * size (page-locked planes only).  Process-wide. */
 RKF_API void rkf_testing_set_host_bands(int bands);
 
 #ifdef __cplusplus

@@ -20,6 +20,23 @@ namespace detail {
 // Band count of host-output views: < 0 chooses by size (rkf_testing_*).
 std::atomic<int> g_host_bands{-1};
 
+// Whether every given host plane is page-locked: only then do the banded
+// copies run asynchronously (a copy into pageable memory holds the host until
+// it is done, which would hold back the next band's launch).
+bool all_page_locked(const rkf_gbuffer& g) {
+  const void* planes[] = {g.t, g.normal, g.slot, g.material, g.flags, g.position, g.packed_material, g.motion};
+  for (const void* p : planes) {
+    if (!p) continue;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if (a.type != cudaMemoryTypeHost) return false;
+  }
+  return true;
+}
+
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
 // Device staging for a G-buffer of n elements; fills dev with device pointers.
@@ -202,7 +219,8 @@ rkf_status rkf_march(rkf_ctx* ctx, const rkf_camera* cam, const rkf_march_params
   RKF_CUDA_TRY(cudaSetDevice(c->device));
   const uint64_t n = static_cast<uint64_t>(width) * height;
   const int bands = host_bands(n);
-  if (out->mem == RKF_MEM_HOST && bands > 1 && p->strategy != RKF_STRATEGY_TILED)
+  if (out->mem == RKF_MEM_HOST && bands > 1 && p->strategy != RKF_STRATEGY_TILED &&
+      (g_host_bands.load() >= 0 || all_page_locked(*out)))
     return march_host_banded(c, cam, p, width, height, *out, bands);
   return run_gbuffer(c, out, n, [&](const rkf_gbuffer& dev) {
     const rkf_batch_tuning& tu = c->tuning;
