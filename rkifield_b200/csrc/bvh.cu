@@ -2,11 +2,20 @@
 // gpu_scene.rs:186) and a host-side build with the reference's surface-area
 // heuristic (Bvh::build, crates/rkf-core/src/bvh.rs:66-260).
 //
-// The march walks the tree once per step with a 32-entry stack
-// (ray_march.wgsl:676-721).  On a tree whose children follow their parent
-// and whose nodes have one parent each, that walk visits every node at most
-// once per step; the import admits nothing else, so no imported BVH can make
-// the walk loop.
+// The shader walks the tree once per step with a 32-entry stack
+// (ray_march.wgsl:676-721): pop a node, skip it if its box is farther than
+// the best distance so far, else evaluate its object (a leaf) or push its left
+// then its right child while fewer than 31 entries are on the stack.  On a
+// tree whose children follow their parent and whose nodes have one parent
+// each -- the only kind the import admits -- that walk visits every node at
+// most once, and the stack's content when a node is popped depends on the
+// tree alone: the left children of the ancestors whose right subtree holds
+// the node.  So the walk is the fixed order "node, right subtree, left
+// subtree", with a node's children dropped when 31 or more entries lie
+// below it, and the march replays it without a stack: per node the import
+// stores the node that follows its subtree in that order (bvh_next, bits
+// 0-30; kBvhEnd after the last) and whether the walk descends into it
+// (bit 31).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -19,6 +28,7 @@ namespace rkf {
 namespace {
 
 constexpr uint32_t kMaxBvhNodes = 65536;
+constexpr uint32_t kBvhEnd = 0x7FFFFFFFu;
 
 struct Box {
   float lo[3], hi[3];
@@ -120,6 +130,21 @@ struct Builder {
 };
 
 // One tree, children after their parent, every node but the root named once.
+// The walk's links (see the file comment); nodes must be a valid tree.
+std::vector<uint32_t> walk_links(const rkf_bvh_node* nodes, uint32_t n) {
+  std::vector<uint32_t> next(n, kBvhEnd), below(n, 0);
+  for (uint32_t i = 0; i < n; ++i) {  // parents come before their children
+    if (nodes[i].left == RKF_BVH_INVALID) continue;
+    const uint32_t l = nodes[i].left, r = nodes[i].right_or_object;
+    if (below[i] < 31) next[i] |= 0x80000000u;
+    next[r] = l;                      // the right subtree is followed by the left child
+    below[r] = below[i] + 1;          // ... which waits on the stack meanwhile
+    next[l] = next[i] & ~0x80000000u;  // the left subtree by what follows the parent's
+    below[l] = below[i];
+  }
+  return next;
+}
+
 bool valid_tree(const rkf_bvh_node* nodes, uint32_t n) {
   std::vector<uint8_t> named(n, 0);
   for (uint32_t i = 0; i < n; ++i) {
@@ -152,15 +177,21 @@ rkf_status rkf_bvh_import(rkf_ctx* ctx, const rkf_bvh_node* nodes, uint32_t n) {
   RKF_CUDA_TRY(cudaSetDevice(c->device));
   if (n == 0) {
     c->bvh.release();
+    c->bvh_next.release();
     c->bvh_n = 0;
     return RKF_OK;
   }
-  DevBuf nb;
+  const std::vector<uint32_t> next = walk_links(nodes, n);
+  DevBuf nb, nn;
   rkf_status st = nb.alloc(static_cast<size_t>(n) * sizeof(rkf_bvh_node));
+  if (st == RKF_OK) st = nn.alloc(static_cast<size_t>(n) * 4);
   if (st != RKF_OK) return st;
   RKF_CUDA_TRY(cudaMemcpy(nb.p, nodes, static_cast<size_t>(n) * sizeof(rkf_bvh_node), cudaMemcpyHostToDevice));
+  RKF_CUDA_TRY(cudaMemcpy(nn.p, next.data(), static_cast<size_t>(n) * 4, cudaMemcpyHostToDevice));
   std::swap(c->bvh.p, nb.p);
   std::swap(c->bvh.bytes, nb.bytes);
+  std::swap(c->bvh_next.p, nn.p);
+  std::swap(c->bvh_next.bytes, nn.bytes);
   c->bvh_n = n;
   return RKF_OK;
 }

@@ -99,8 +99,9 @@ struct Ctx {
   uint32_t coarse_dims[3] = {0, 0, 0};
   uint64_t coarse_epoch = ~0ull;
 
-  // BVH of the BVH strategy (bvh.cu): rkf_bvh_node records, root first
-  DevBuf bvh;
+  // BVH of the BVH strategy (bvh.cu): rkf_bvh_node records, root first, and
+  // per node the walk's next node and whether it descends (bvh.cu)
+  DevBuf bvh, bvh_next;
   uint32_t bvh_n = 0;
 
   // objects

@@ -70,6 +70,7 @@ struct KParams {
   float empty_lo_t, empty_hi;  // empty-space path: tight bounds of an EMPTY step
   uint32_t settle_links;   // empty-space path: cubes a settling chain may add (0 = off)
   const rkf_bvh_node* bvh; // BVH strategy: the imported tree, root first
+  const uint32_t* bvh_next;  // per node: the walk's next node (bits 0-30), descend (bit 31)
   uint32_t use_bvh;
 };
 
@@ -78,25 +79,38 @@ struct KParams {
 // from the position than the best distance so far, evaluates the objects of
 // the leaves it reaches (object indices beyond the object count are skipped),
 // and pushes the left then the right child while fewer than 31 entries are on
-// the stack (so the right child is visited first).  The import admits trees
-// only, so the walk visits each node at most once.
+// the stack (so the right child is visited first).  On the trees the import
+// admits the stack's content at each node is fixed by the tree, so the same
+// walk runs from the per-node links bvh.cu derives (next node after the
+// subtree, whether to descend), without a stack.  The distance to a box is
+// length(clamp(pos, min, max) - pos); its square root is taken only where the
+// comparison needs it (an exact zero stays zero, and any length exceeds a
+// negative best).
 template <int PREC>
 __device__ __forceinline__ float eval_bvh(const SceneDev& s, const ObjDev* objs, const rkf_bvh_node* nodes,
-                                          uint32_t nobj, float wx, float wy, float wz, float& best_un,
-                                          uint32_t& best_i, LaneCache& lc) {
-  uint32_t stack[32];
-  uint32_t sp = 1;
-  stack[0] = 0;
+                                          const uint32_t* __restrict__ next, uint32_t nobj, float wx, float wy,
+                                          float wz, float& best_un, uint32_t& best_i, LaneCache& lc) {
+  constexpr uint32_t kEnd = 0x7FFFFFFFu;
   float best = kMaxFloat;
   best_un = kMaxFloat;
   best_i = 0;
-  while (sp > 0) {
-    const float4* nd = reinterpret_cast<const float4*>(nodes + stack[--sp]);
+  uint32_t i = 0;
+  while (i != kEnd) {
+    const float4* nd = reinterpret_cast<const float4*>(nodes + i);
     const float4 a = __ldg(nd), b = __ldg(nd + 1);
-    // length(clamp(pos, node_min, node_max) - pos)
-    const float bd = len3(__fsub_rn(fminf(fmaxf(wx, a.x), b.x), wx), __fsub_rn(fminf(fmaxf(wy, a.y), b.y), wy),
-                          __fsub_rn(fminf(fmaxf(wz, a.z), b.z), wz));
-    if (bd > best) continue;
+    const uint32_t link = __ldg(next + i);
+    const float ex = __fsub_rn(fminf(fmaxf(wx, a.x), b.x), wx);
+    const float ey = __fsub_rn(fminf(fmaxf(wy, a.y), b.y), wy);
+    const float ez = __fsub_rn(fminf(fmaxf(wz, a.z), b.z), wz);
+    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez));
+    bool skip;
+    if (d2 == 0.0f) skip = 0.0f > best;
+    else if (best < 0.0f && d2 == d2) skip = true;
+    else skip = __fsqrt_rn(d2) > best;
+    if (skip) {
+      i = link & kEnd;
+      continue;
+    }
     const uint32_t left = __float_as_uint(a.w), ro = __float_as_uint(b.w);
     if (left == RKF_BVH_INVALID) {
       if (ro < nobj) {
@@ -108,9 +122,9 @@ __device__ __forceinline__ float eval_bvh(const SceneDev& s, const ObjDev* objs,
           best_i = ro;
         }
       }
-    } else if (sp < 31) {
-      stack[sp++] = left;
-      stack[sp++] = ro;
+      i = link & kEnd;
+    } else {
+      i = (link >> 31) ? ro : (link & kEnd);
     }
   }
   return best;
@@ -617,7 +631,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
               }
             }
           } else if (!EMPTY_PATH && kp.use_bvh) {
-            best = eval_bvh<PREC>(s, sh_objs, kp.bvh, nobj, wx, wy, wz, best_un, best_i, lc);
+            best = eval_bvh<PREC>(s, sh_objs, kp.bvh, kp.bvh_next, nobj, wx, wy, wz, best_un, best_i, lc);
           } else {
             best = eval_min<PREC, SINGLE>(s, sh_objs, 0, nobj, wx, wy, wz, best_un, best_i, lc);
           }
@@ -1022,6 +1036,7 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   kp.td = td;
   kp.tiled = tiled ? 1u : 0u;
   kp.bvh = use_bvh ? c->bvh.as<rkf_bvh_node>() : nullptr;
+  kp.bvh_next = use_bvh ? c->bvh_next.as<uint32_t>() : nullptr;
   kp.use_bvh = use_bvh ? 1u : 0u;
   kp.probe_min = obj == detail::OBJ_SINGLE_EMPTY ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
   kp.budget = tu.step_budget ? tu.step_budget : 32;
