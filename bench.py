@@ -380,6 +380,14 @@ def run_batching(ctx, spec, prims, p, args, stream):
 
     steps = args.cb_steps
     mb = timed(batched, steps)
+    # the same batch captured once as a CUDA graph and replayed
+    from rkifield_b200.engine import BatchGraph
+    graph = BatchGraph(ctx, vs, bs, p)
+    try:
+        mg = timed(lambda: graph.launch(stream.ptr), steps)
+    finally:
+        stream.synchronize()
+        graph.close()
     mp = timed(lambda: per_request(True), max(1, steps - 1))
     mf = timed(lambda: per_request(False), max(1, steps - 1))
     rays = wl["n_primary"] + wl["n_secondary_live"]
@@ -391,6 +399,7 @@ def run_batching(ctx, spec, prims, p, args, stream):
                        "probe_in_run": tu.probe_in_run,
                        "threads_per_block": tu.threads_per_block, "tune_s": tune_s},
             "batched": {"value": val(mb), "unit": "Mrays/s", "ms": float(np.mean(mb)), "launches": 1},
+            "batched_graph": {"value": val(mg), "unit": "Mrays/s", "ms": float(np.mean(mg)), "launches": 1},
             "plain_per_request": {"value": val(mp), "unit": "Mrays/s", "ms": float(np.mean(mp)),
                                   "launches": 3 * nv},
             "b200_per_request": {"value": val(mf), "unit": "Mrays/s", "ms": float(np.mean(mf)),

@@ -550,6 +550,30 @@ RKF_API rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t n_
                         const rkf_march_params* p, rkf_batch_tuning* out);
 
 /* ------------------------------------------------------------------------ */
+/* A batched march captured as a CUDA graph (no counterpart in the          */
+/* reference, which records its passes into a wgpu command encoder)         */
+/* ------------------------------------------------------------------------ */
+/* For work that repeats every frame with the same sizes and output buffers:
+ * rkf_batch_graph_create captures one rkf_march_batch of these views and ray
+ * batches (device outputs, brute strategy) into a CUDA graph -- the segment
+ * table's copy from page-locked memory the graph owns, the work counter's
+ * reset, the persistent march kernel -- and rkf_batch_graph_launch replays it
+ * on a stream (NULL = the context stream).  rkf_batch_graph_set_cameras
+ * gives the views new cameras for the next launch (one per view given at
+ * creation, in order; it waits for the previous launch to finish).  The graph
+ * holds the scene as it was when made: after an object import, a
+ * voxelization or an edit, rkf_batch_graph_launch returns RKF_EPOCH_STALE and
+ * the caller makes a new graph.  Destroy graphs before their context. */
+typedef struct rkf_batch_graph rkf_batch_graph;
+RKF_API rkf_status rkf_batch_graph_create(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views,
+                                          const rkf_ray_batch* batches, uint32_t n_batches,
+                                          const rkf_march_params* p, const rkf_batch_tuning* tuning,
+                                          rkf_batch_graph** out);
+RKF_API rkf_status rkf_batch_graph_set_cameras(rkf_batch_graph* graph, const rkf_camera* cameras, uint32_t n);
+RKF_API rkf_status rkf_batch_graph_launch(rkf_batch_graph* graph, void* stream);
+RKF_API rkf_status rkf_batch_graph_destroy(rkf_batch_graph* graph);
+
+/* ------------------------------------------------------------------------ */
 /* Serving: resident request loop with continuous batching                  */
 /* ------------------------------------------------------------------------ */
 typedef enum rkf_request_kind {

@@ -197,6 +197,11 @@ SIGNATURES = {
     "rkf_brickmap_import": (_I, [_P, _P, _U64]),
     "rkf_objects_import": (_I, [_P, _P, _U32]),
     "rkf_bvh_import": (_I, [_P, _P, _U32]),
+    "rkf_batch_graph_create": (_I, [_P, C.POINTER(rkf_view), _U32, C.POINTER(rkf_ray_batch), _U32,
+                                    C.POINTER(rkf_march_params), C.POINTER(rkf_batch_tuning), C.POINTER(_P)]),
+    "rkf_batch_graph_set_cameras": (_I, [_P, C.POINTER(rkf_camera), _U32]),
+    "rkf_batch_graph_launch": (_I, [_P, _P]),
+    "rkf_batch_graph_destroy": (_I, [_P]),
     "rkf_bvh_build": (_I, [_P, _U32, _P, _U32, C.POINTER(_U32)]),
     "rkf_scene_info_get": (_I, [_P, C.POINTER(rkf_scene_info)]),
     "rkf_pool_export_voxelsample": (_I, [_P, _U32, _U32, _P]),

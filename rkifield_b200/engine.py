@@ -368,6 +368,36 @@ class GpuScene:
         self.ctx.upload_bvh(nodes)
 
 
+class BatchGraph:
+    """A batched march captured once as a CUDA graph (rkf_batch_graph_*): the
+    same views and ray batches (device outputs) launched again every frame,
+    with new cameras set between launches.  Stale after a scene change
+    (RkfError RKF_EPOCH_STALE on launch): make a new one."""
+
+    def __init__(self, ctx: Context, views, batches, params, tuning=None):
+        self.ctx = ctx
+        self.h = C.c_void_p()
+        self._keep = (views, batches, params, tuning)
+        nv = len(views) if views is not None else 0
+        nb = len(batches) if batches is not None else 0
+        check(ctx.lib.rkf_batch_graph_create(ctx.h, views, nv, batches, nb, C.byref(params),
+                                             C.byref(tuning) if tuning is not None else None, C.byref(self.h)),
+              "rkf_batch_graph_create")
+        self.n_views = nv
+
+    def set_cameras(self, cams):
+        arr = (abi.rkf_camera * len(cams))(*cams)
+        check(self.ctx.lib.rkf_batch_graph_set_cameras(self.h, arr, len(cams)), "rkf_batch_graph_set_cameras")
+
+    def launch(self, stream_ptr: int | None = None):
+        check(self.ctx.lib.rkf_batch_graph_launch(self.h, stream_ptr), "rkf_batch_graph_launch")
+
+    def close(self):
+        if self.h.value:
+            self.ctx.lib.rkf_batch_graph_destroy(self.h)
+            self.h = C.c_void_p()
+
+
 class RayMarchPass:
     """``RayMarchPass`` (ray_march.rs:29-119): dispatch marches one view into
     a G-buffer (SoA numpy planes)."""
