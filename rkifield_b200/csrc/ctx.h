@@ -95,6 +95,10 @@ struct Ctx {
 
   // tiled strategy (tiled.h): coarse field (rebuilt when epoch changes) and tile lists
   DevBuf coarse_tex, tile_buf;
+  // empty-space field of the tiled strategy for a single object: EMPTY
+  // blocks that no coarse skip can reach (tiled.cu); built for tiled_epoch
+  DevBuf tiled_empty_dist;
+  uint64_t tiled_epoch = ~0ull;
   float coarse_origin[3] = {0.0f, 0.0f, 0.0f};
   uint32_t coarse_dims[3] = {0, 0, 0};
   uint64_t coarse_epoch = ~0ull;
@@ -103,6 +107,7 @@ struct Ctx {
   // per node the walk's next node and whether it descends (bvh.cu)
   DevBuf bvh, bvh_next;
   uint32_t bvh_n = 0;
+  bool bvh_one_leaf0 = false;  // the tree is one leaf naming object 0
 
   // objects
   std::vector<rkf_gpu_object> objects;

@@ -133,7 +133,9 @@ __device__ __forceinline__ float eval_bvh(const SceneDev& s, const ObjDev* objs,
 // Object set of a launch: several objects, exactly one, or exactly one that
 // qualifies for the empty-space path (voxelized, translation-only
 // inverse_world, verified exact quotient, fewer than 2^20 voxels per axis).
-enum : int { OBJ_MULTI = 0, OBJ_SINGLE = 1, OBJ_SINGLE_EMPTY = 2 };
+// OBJ_SINGLE_EMPTY_TILED: the empty-space path of a tiled launch (EMPTY runs
+// on the tiled empty-space field, tiled full steps elsewhere).
+enum : int { OBJ_MULTI = 0, OBJ_SINGLE = 1, OBJ_SINGLE_EMPTY = 2, OBJ_SINGLE_EMPTY_TILED = 3 };
 
 // Grid coordinate (position + half grid size, object-local) of the ray at t,
 // rounded exactly as eval_obj -> sample_vox round it for a translation-only
@@ -397,7 +399,8 @@ __device__ __forceinline__ uint32_t empty_run_x2(const ObjDev& o, const uint8_t*
 template <int PREC, int OBJ>
 __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_constant__ KParams kp) {
   constexpr bool SINGLE = OBJ != OBJ_MULTI;
-  constexpr bool EMPTY_PATH = OBJ == OBJ_SINGLE_EMPTY;
+  constexpr bool EMPTY_PATH = OBJ == OBJ_SINGLE_EMPTY || OBJ == OBJ_SINGLE_EMPTY_TILED;
+  constexpr bool TILES = OBJ != OBJ_SINGLE_EMPTY;  // tile bookkeeping of tiled launches
   const ObjDev* sh_objs = kp.objs;
   const SceneDev& s = kp.s;
   const rkf_march_params& p = kp.p;
@@ -465,7 +468,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                 oz = sg.pos[2];
                 tmax = p.scene.max_distance;
                 mode = RKF_TRACE_CLOSEST;
-                if (!EMPTY_PATH) {
+                if (TILES) {
                   cs.tile_count = kNoTiles;
                   if (kp.tiled) {  // the pixel's tile (ray_march.wgsl:884-893)
                     const uint32_t tl = sg.tile_off + (py / 16) * ((sg.w + 15) / 16) + px / 16;
@@ -475,7 +478,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                 }
               }
             } else {
-              if (!EMPTY_PATH) cs.tile_count = kNoTiles;
+              if (TILES) cs.tile_count = kNoTiles;
               cs.idx = static_cast<uint32_t>(local);
               const size_t i3 = 3 * static_cast<size_t>(cs.idx);
               ox = __ldg(sg.origins + i3);
@@ -502,7 +505,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                 prev_t = 0.0f;
                 prev_dist = kMaxFloat;
                 // a tile with no objects is sky (ray_march.wgsl:895-897)
-                state = (!EMPTY_PATH && cs.tile_count == 0) ? ST_EPI : ST_MARCH;
+                state = (TILES && cs.tile_count == 0) ? ST_EPI : ST_MARCH;
               }
             }
           }
@@ -604,7 +607,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                       wz = __fadd_rn(oz, __fmul_rn(qdz, t));
           float best;
           bool skipped = false;
-          if (!EMPTY_PATH && kp.tiled && cs.tile_count != kNoTiles) {
+          if (TILES && kp.tiled && cs.tile_count != kNoTiles) {
             // ray_march_tiled (:899-938): a coarse empty-space skip, else the
             // tile's objects only
             const Segment& sg = kp.segs[cs.seg];
@@ -970,6 +973,8 @@ __global__ void k_sdf_ao(SceneDev s, const float* __restrict__ pos, const float*
 template <int PREC>
 const void* persistent_fn(int obj) {
   if (obj == OBJ_SINGLE_EMPTY) return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_SINGLE_EMPTY>);
+  if (obj == OBJ_SINGLE_EMPTY_TILED)
+    return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_SINGLE_EMPTY_TILED>);
   if (obj == OBJ_SINGLE) return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_SINGLE>);
   return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_MULTI>);
 }
@@ -1001,10 +1006,12 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   std::vector<Segment> tiled_segs;
   TiledDev td;
   std::memset(&td, 0, sizeof(td));
+  const int objs = object_set(c);
   if (tiled) {
     tiled_segs = segs_host;
     rkf_status s2 = prepare_tiled(c, tiled_segs, st, &td);
     if (s2 != RKF_OK) return s2;
+    if (objs == detail::OBJ_SINGLE_EMPTY && (s2 = prepare_tiled_empty(c, st)) != RKF_OK) return s2;
   }
   const std::vector<Segment>& segs_dev = tiled ? tiled_segs : segs_host;
   const size_t sb = segs_dev.size() * sizeof(Segment);
@@ -1031,24 +1038,34 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   kp.counter = counter;
   kp.p = *p;
   kp.p.scene.num_objects = c->obj_count();
-  const int obj =
-      (tiled || use_bvh) && object_set(c) == detail::OBJ_SINGLE_EMPTY ? detail::OBJ_SINGLE : object_set(c);
+  // A BVH of one leaf naming the only, voxelized, object makes every step
+  // evaluate exactly what the brute step evaluates (the one box test passes
+  // for every finite distance, and where it would not, the object's own
+  // distance is not finite either), so that walk is the brute march.
+  const bool walk = use_bvh && !(objs == detail::OBJ_SINGLE_EMPTY && c->bvh_one_leaf0);
+  int obj = objs;
+  if (objs == detail::OBJ_SINGLE_EMPTY && walk) obj = detail::OBJ_SINGLE;
+  if (objs == detail::OBJ_SINGLE_EMPTY && tiled) {
+    obj = detail::OBJ_SINGLE_EMPTY_TILED;
+    kp.s.empty_dist = c->tiled_empty_dist.as<uint8_t>();
+  }
+  const bool empty = obj == detail::OBJ_SINGLE_EMPTY || obj == detail::OBJ_SINGLE_EMPTY_TILED;
   kp.td = td;
   kp.tiled = tiled ? 1u : 0u;
-  kp.bvh = use_bvh ? c->bvh.as<rkf_bvh_node>() : nullptr;
-  kp.bvh_next = use_bvh ? c->bvh_next.as<uint32_t>() : nullptr;
-  kp.use_bvh = use_bvh ? 1u : 0u;
-  kp.probe_min = obj == detail::OBJ_SINGLE_EMPTY ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
+  kp.bvh = walk ? c->bvh.as<rkf_bvh_node>() : nullptr;
+  kp.bvh_next = walk ? c->bvh_next.as<uint32_t>() : nullptr;
+  kp.use_bvh = walk ? 1u : 0u;
+  kp.probe_min = empty ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
   kp.budget = tu.step_budget ? tu.step_budget : 32;
   kp.refill_active = 32u - std::min<uint32_t>(tu.refill_idle ? tu.refill_idle : 32u, 32u);
   kp.run_probe = tu.probe_in_run ? 1u : 0u;
   // mix(c, c, t) three times stays within 12 roundings of c (relative 2^-24
   // each); 0.999 leaves a wide margin
-  kp.empty_lo = obj == detail::OBJ_SINGLE_EMPTY ? 0.999f * kp.objs[0].be * kp.objs[0].min_scale : 0.0f;
+  kp.empty_lo = empty ? 0.999f * kp.objs[0].be * kp.objs[0].min_scale : 0.0f;
   // twelve roundings of 2^-24 stay far inside 2^-16
   kp.empty_lo_t = kp.objs[0].be * kp.objs[0].min_scale * (1.0f - 1.52587890625e-5f);
   kp.empty_hi = kp.objs[0].be * kp.objs[0].min_scale * (1.0f + 1.52587890625e-5f);
-  kp.settle_links = obj == detail::OBJ_SINGLE_EMPTY ? 48u : 0u;
+  kp.settle_links = empty ? 48u : 0u;
   kp.plain_obj = (kp.objs[0].m[12] == 0.0f && kp.objs[0].m[13] == 0.0f && kp.objs[0].m[14] == 0.0f &&
                   kp.objs[0].min_scale == 1.0f)
                      ? 1u

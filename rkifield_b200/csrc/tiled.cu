@@ -20,6 +20,7 @@
 
 #include "ctx.h"
 #include "march.h"
+#include "empty_dist.h"
 #include "tiled.h"
 
 namespace rkf {
@@ -196,6 +197,136 @@ rkf_status prepare_tiled(Ctx* c, std::vector<Segment>& segs, cudaStream_t st, Ti
   out->cinv_vs = 1.0f / vs;
   out->tile_cnt = cnt;
   out->tile_list = list;
+  return RKF_OK;
+}
+
+namespace detail {
+
+// 1 for a texel whose value exceeds kCoarseSafe
+__global__ void k_coarse_unsafe(const uint16_t* __restrict__ tex, uint32_t n, uint32_t* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = __half2float(__ushort_as_half(tex[i])) > kCoarseSafe ? 1u : 0u;
+}
+
+// inclusive prefix sum along one axis of a dx x dy x dz array (one thread per line)
+__global__ void k_prefix_axis(uint32_t* __restrict__ a, uint32_t dx, uint32_t dy, uint32_t dz, uint32_t axis) {
+  const uint32_t line = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t len = axis == 0 ? dx : axis == 1 ? dy : dz;
+  const uint32_t lines = axis == 0 ? dy * dz : axis == 1 ? dx * dz : dx * dy;
+  if (line >= lines) return;
+  size_t base, stride;
+  if (axis == 0) {
+    base = static_cast<size_t>(line) * dx;
+    stride = 1;
+  } else if (axis == 1) {
+    base = static_cast<size_t>(line % dx) + static_cast<size_t>(line / dx) * dx * dy;
+    stride = dx;
+  } else {
+    base = line;
+    stride = static_cast<size_t>(dx) * dy;
+  }
+  uint32_t acc = 0;
+  for (uint32_t k = 0; k < len; ++k) {
+    acc += a[base + k * stride];
+    a[base + k * stride] = acc;
+  }
+}
+
+struct SafeArgs {
+  const uint32_t* top;   // the object's top grid (global indices)
+  const uint32_t* pre;   // 3D prefix count of unsafe texels
+  uint32_t* masked;      // out: top with unsafe EMPTY blocks made INTERIOR
+  uint32_t off, tx, ty, tz;
+  uint32_t cd[3];        // coarse field dims
+  double lo[3];          // world position of grid coordinate 0 (-half_gs - translation)
+  double block;          // block edge (64 voxels)
+  double corg[3];        // coarse field origin
+  double cvs;            // coarse cell
+};
+
+__device__ __forceinline__ uint32_t pre_at(const SafeArgs& a, int x, int y, int z) {
+  if (x < 0 || y < 0 || z < 0) return 0u;
+  return a.pre[static_cast<size_t>(x) + static_cast<size_t>(y) * a.cd[0] +
+               static_cast<size_t>(z) * a.cd[0] * a.cd[1]];
+}
+
+// One thread per top block: the texels a sample in the block (widened by a
+// voxel) can interpolate lie in [floor(xmin) - 1, floor(xmax) + 2] per axis
+// of x = (world - origin) / cell - 0.5 (one texel of margin each side covers
+// the float rounding of the camera-relative coordinates); the block stays
+// EMPTY only if none of them is unsafe.  Positions outside the field sample 0.
+__global__ void k_tiled_mask(const __grid_constant__ SafeArgs a) {
+  const uint64_t n = static_cast<uint64_t>(a.tx) * a.ty * a.tz;
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t k[3] = {static_cast<uint32_t>(i % a.tx), static_cast<uint32_t>((i / a.tx) % a.ty),
+                         static_cast<uint32_t>(i / (static_cast<uint64_t>(a.tx) * a.ty))};
+  const uint32_t v = a.top[a.off + i];
+  uint32_t out = v;
+  if (v == RKF_EMPTY_SLOT) {
+    int r0[3], r1[3];
+    bool any = true;
+    for (int d = 0; d < 3; ++d) {
+      const double vox = a.block / 64.0;
+      const double w0 = a.lo[d] + k[d] * a.block - vox, w1 = a.lo[d] + (k[d] + 1) * a.block + vox;
+      const double x0 = (w0 - a.corg[d]) / a.cvs - 0.5, x1 = (w1 - a.corg[d]) / a.cvs - 0.5;
+      r0[d] = max(static_cast<int>(floor(x0)) - 1, 0);
+      r1[d] = min(static_cast<int>(floor(x1)) + 2, static_cast<int>(a.cd[d]) - 1);
+      if (r1[d] < r0[d]) any = false;  // the block lies wholly outside the field
+    }
+    uint32_t cnt = 0;
+    if (any) {
+      const int x0 = r0[0] - 1, y0 = r0[1] - 1, z0 = r0[2] - 1, x1 = r1[0], y1 = r1[1], z1 = r1[2];
+      cnt = pre_at(a, x1, y1, z1) - pre_at(a, x0, y1, z1) - pre_at(a, x1, y0, z1) - pre_at(a, x1, y1, z0) +
+            pre_at(a, x0, y0, z1) + pre_at(a, x0, y1, z0) + pre_at(a, x1, y0, z0) - pre_at(a, x0, y0, z0);
+    }
+    if (cnt) out = RKF_INTERIOR_SLOT;
+  }
+  a.masked[a.off + i] = out;
+}
+
+}  // namespace detail
+
+rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st) {
+  if (c->tiled_epoch == c->epoch && c->tiled_empty_dist.p) return RKF_OK;
+  if (c->coarse_epoch != c->epoch || !c->coarse_tex.p)
+    return fail(RKF_CUDA_ERROR, "tiled march: coarse field missing for the empty-space field");
+  const ObjDev& o = c->objdev_host[0];
+  const uint32_t cd[3] = {c->coarse_dims[0], c->coarse_dims[1], c->coarse_dims[2]};
+  const uint32_t nt = cd[0] * cd[1] * cd[2];
+  DevBuf pre, masked, field;
+  rkf_status s2 = pre.alloc(static_cast<size_t>(nt) * 4);
+  if (s2 == RKF_OK) s2 = masked.alloc(std::max<uint64_t>(c->top_len, 1) * 4);
+  if (s2 == RKF_OK) s2 = field.alloc(std::max<uint64_t>(c->top_len, 1));
+  if (s2 != RKF_OK) return s2;
+  detail::k_coarse_unsafe<<<(nt + 255) / 256, 256, 0, st>>>(c->coarse_tex.as<uint16_t>(), nt, pre.as<uint32_t>());
+  for (uint32_t axis = 0; axis < 3; ++axis) {
+    const uint32_t lines = axis == 0 ? cd[1] * cd[2] : axis == 1 ? cd[0] * cd[2] : cd[0] * cd[1];
+    detail::k_prefix_axis<<<(lines + 127) / 128, 128, 0, st>>>(pre.as<uint32_t>(), cd[0], cd[1], cd[2], axis);
+  }
+  detail::SafeArgs a;
+  a.top = c->top.as<uint32_t>();
+  a.pre = pre.as<uint32_t>();
+  a.masked = masked.as<uint32_t>();
+  a.off = o.top_off;
+  a.tx = o.tdim[0];
+  a.ty = o.tdim[1];
+  a.tz = o.tdim[2];
+  for (int d = 0; d < 3; ++d) {
+    a.cd[d] = cd[d];
+    a.lo[d] = -static_cast<double>(o.half_gs[d]) - static_cast<double>(o.m[12 + d]);
+    a.corg[d] = c->coarse_origin[d];
+  }
+  a.block = 64.0 * static_cast<double>(o.vs);
+  a.cvs = 0.32;
+  const uint64_t nb = static_cast<uint64_t>(a.tx) * a.ty * a.tz;
+  detail::k_tiled_mask<<<static_cast<unsigned>((nb + 255) / 256), 256, 0, st>>>(a);
+  RKF_CUDA_TRY(cudaGetLastError());
+  if ((s2 = build_empty_dist(o, masked.as<uint32_t>(), field.as<uint8_t>(), st)) != RKF_OK) return s2;
+  RKF_CUDA_TRY(cudaStreamSynchronize(st));
+  std::swap(c->tiled_empty_dist.p, field.p);
+  std::swap(c->tiled_empty_dist.bytes, field.bytes);
+  c->tiled_epoch = c->epoch;
   return RKF_OK;
 }
 

@@ -393,3 +393,34 @@ def test_strategies_over_precision_planes_bit_exact(oracle, small_scene, precisi
                 assert_bits_equal(banded[k], ref[k], f"banded {strategy} {precision} {k}")
     finally:
         ctx.close()
+
+
+@pytest.mark.gpu
+def test_bvh_single_leaf_bit_exact(oracle, small_scene):
+    """A BVH of one leaf over the one voxelized object (which the library
+    marches as the brute march it equals), against the oracle's stack walk."""
+    from rkifield_b200 import _abi as abi, engine, scenes
+    from rkifield_b200.engine import Context
+    v = small_scene["vox"]
+    spec = small_scene["spec"]
+    obj = small_scene["obj"]
+    bvh = engine.object_bvh([obj])
+    assert len(bvh) == 1 and bvh[0].left == INVALID and bvh[0].right_or_object == 0
+    sc = oracle.Scene([obj], pool_words=v.words, brick_maps=v.map, bvh=bvh)
+    ctx = Context(pool_capacity=v.n_bricks + 1024)
+    try:
+        ctx.set_brick_pool(v.words)
+        ctx.upload_brick_maps(v.map)
+        ctx.upload_objects([obj])
+        ctx.upload_bvh(bvh)
+        w, h = 160, 128
+        cam = scenes.seeded_camera(spec, w, h, seed=13)
+        p = scenes.march_params(spec)
+        p.strategy = abi.RKF_STRATEGY_BVH
+        ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+        got = ctx.march(cam, p, w, h, reference_planes=True)
+        assert ((ref["flags"] & 1) != 0).sum() > 300
+        for k in PLANES:
+            assert_bits_equal(got[k], ref[k], f"one-leaf bvh {k}")
+    finally:
+        ctx.close()

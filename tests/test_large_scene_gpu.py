@@ -91,3 +91,18 @@ def test_large_rays_around_the_step_budget_bit_exact(oracle, large, large_oracle
         if mode == abi.RKF_TRACE_CLOSEST:
             steps_out = (ref["flags"] & 4) != 0
             assert steps_out.sum() > 200 and (ref["flags"] == 0).sum() > 200, "both miss endings must occur"
+
+
+def test_large_view_tiled_rows_bit_exact(oracle, large, large_oracle):
+    """The tiled strategy on the single-object scene (EMPTY runs on the field
+    of blocks no coarse skip can reach, tiled steps elsewhere): sampled rows
+    bit-exact against the oracle's tiled march."""
+    from rkifield_b200 import _abi as abi, scenes
+    ctx, spec, cam, _ = large
+    p = scenes.march_params(spec)
+    p.strategy = abi.RKF_STRATEGY_TILED
+    got = ctx.march(cam, p, W, H, reference_planes=True)
+    for r in (0, 389, 541, 1079):
+        ref = oracle.march(large_oracle, cam, p, W, H, rows=(r, r + 1), with_reference_planes=True)
+        for k in PLANES:
+            assert_bits_equal(got[k].reshape(H, -1)[r], ref[k].reshape(1, -1)[0], f"tiled row {r} {k}")

@@ -140,3 +140,28 @@ def test_tiled_after_scene_change_bit_exact(oracle, small_scene):
                 assert_bits_equal(got[name], ref[name], f"{k} objects {name}")
     finally:
         ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [11, 12])
+def test_single_object_tiled_bit_exact(oracle, small_scene, small_ctx, seed):
+    """One voxelized object seen from outside its box: the tiled march takes
+    coarse-field skips outside the box and EMPTY runs inside it (on the field
+    of blocks no coarse skip can reach), bit-exact against the oracle's tiled
+    march, which differs from the brute march in the low bits of t."""
+    from rkifield_b200 import _abi as abi, scenes
+    spec = small_scene["spec"]
+    v = small_scene["vox"]
+    sc = oracle.Scene([small_scene["obj"]], pool_words=v.words, brick_maps=v.map)
+    w, h = 192, 160
+    cam = scenes.seeded_camera(spec, w, h, seed=seed)
+    p = scenes.march_params(spec)
+    p.strategy = abi.RKF_STRATEGY_TILED
+    ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+    got = small_ctx.march(cam, p, w, h, reference_planes=True)
+    hit = (ref["flags"] & 1) != 0
+    assert hit.sum() > 500
+    for k in PLANES:
+        assert_bits_equal(got[k], ref[k], f"single-object tiled {k}")
+    brute = oracle.march(sc, cam, scenes.march_params(spec), w, h)
+    assert (brute["t"][hit] != ref["t"][hit]).any(), "the coarse field should move some sample points"
