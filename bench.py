@@ -718,6 +718,17 @@ def run_extras(args, spec, prims, p, ctx, stream):
     prec = {}
     cam = camera_for(spec, args.width, args.height, 0)
     n = args.width * args.height
+    # the headline view under the shader's other strategies (the runtime binds
+    # tile lists every frame, so its shader marches with the tiled one)
+    from rkifield_b200 import engine
+    ctx.upload_bvh(engine.object_bvh([ctx.object(i) for i in range(ctx.info()["num_objects"])]))
+    strat = {}
+    for name, code in (("tiled", abi.RKF_STRATEGY_TILED), ("bvh", abi.RKF_STRATEGY_BVH)):
+        ps = scenes.march_params(spec)
+        ps.strategy = code
+        ms = time_view(ctx, cam, ps, args.width, args.height, stream, 5)
+        strat[name] = {"mrays": n / ms / 1e3, "ms": ms}
+    out["strategies"] = strat
     for name in ("f32", "u8"):
         c2 = Context(pool_capacity=ctx.info()["pool_bricks_used"] + 4096, precision=name, keep_reference_pool=False)
         try:
