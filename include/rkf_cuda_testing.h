@@ -30,6 +30,13 @@ RKF_API rkf_status rkf_testing_export_empty_dist(rkf_ctx* ctx, uint8_t* out, uin
  * size (page-locked planes only).  Process-wide. */
 RKF_API void rkf_testing_set_host_bands(int bands);
 
+/* The tiled strategy's coarse field for the context's current objects (built
+ * if needed): its origin, dims and, when tex is not NULL, its dims[0] x
+ * dims[1] x dims[2] binary16 texels (x + y*dx + z*dx*dy); *n receives the
+ * texel count. */
+RKF_API rkf_status rkf_testing_export_coarse(rkf_ctx* ctx, float origin[3], uint32_t dims[3], uint16_t* tex,
+                                             uint64_t* n);
+
 #ifdef __cplusplus
 }
 #endif

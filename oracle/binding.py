@@ -53,6 +53,8 @@ def lib() -> C.CDLL:
         P, U32, I = C.c_void_p, C.c_uint32, C.c_int
         L.orc_f16_from_f32.restype = C.c_uint16
         L.orc_f16_from_f32.argtypes = [C.c_float]
+        L.orc_coarse_field.restype = C.c_uint64
+        L.orc_coarse_field.argtypes = [P, U32, P, P, P, C.c_uint64]
         L.orc_f16_to_f32.restype = C.c_float
         L.orc_f16_to_f32.argtypes = [C.c_uint16]
         L.orc_prim_sdf.restype = C.c_float
@@ -166,6 +168,18 @@ class Scene:
                            C.addressof(self.objects), n, ptr(dist_f64),
                            C.addressof(bvh) if bvh is not None and len(bvh) else None,
                            len(bvh) if bvh is not None else 0)
+
+
+def coarse_field(objects):
+    """orc_coarse_field: (origin float32[3], dims uint32[3], texels uint16[])."""
+    n = len(objects)
+    arr = (abi.rkf_gpu_object * max(n, 1))(*objects)
+    origin = np.zeros(3, np.float32)
+    dims = np.zeros(3, np.uint32)
+    cnt = lib().orc_coarse_field(arr, n, ptr(origin), ptr(dims), None, 0)
+    tex = np.zeros(cnt, np.uint16)
+    lib().orc_coarse_field(arr, n, ptr(origin), ptr(dims), ptr(tex), cnt)
+    return origin, dims, tex
 
 
 def march(scene: Scene, cam, params, w: int, h: int, fp64: bool = False, threads: int | None = None,

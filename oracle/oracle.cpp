@@ -1565,6 +1565,21 @@ float orc_sample_brick_trilinear(const uint32_t* words, const float lp[3], float
 }
 
 // Reference defaults (gpu_scene.rs:34-43, ray_march.wgsl:28-41).
+uint64_t orc_coarse_field(const rkf_gpu_object* objects, uint32_t n, float origin[3], uint32_t dims[3],
+                          uint16_t* tex, uint64_t cap) {
+  orc_scene sc;
+  std::memset(&sc, 0, sizeof(sc));
+  sc.objects = objects;
+  sc.num_objects = n;
+  const CoarseField c = coarse_build(&sc);
+  for (int a = 0; a < 3; ++a) {
+    origin[a] = c.origin[a];
+    dims[a] = c.dims[a];
+  }
+  if (tex && cap >= c.tex.size()) std::memcpy(tex, c.tex.data(), c.tex.size() * 2);
+  return c.tex.size();
+}
+
 void orc_march_params_default(rkf_march_params* p) {
   p->scene.num_objects = 0;
   p->scene.max_steps = 128;

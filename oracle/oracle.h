@@ -38,6 +38,13 @@ extern "C" {
 
 void orc_march_params_default(rkf_march_params* p);
 
+/* The tiled strategy's coarse field over these objects' AABBs (0.32 m cells
+ * over the union grown by 1 m, at most 128 per axis; binary16 texels of the
+ * distance to the nearest AABB, x + y*dx + z*dx*dy).  Writes origin and
+ * dims, and the texels when cap holds them; returns the texel count. */
+uint64_t orc_coarse_field(const rkf_gpu_object* objects, uint32_t n, float origin[3], uint32_t dims[3],
+                          uint16_t* tex, uint64_t cap);
+
 /* ---- binary16 ---------------------------------------------------------- */
 uint16_t orc_f16_from_f32(float f);
 float orc_f16_to_f32(uint16_t h);

@@ -20,6 +20,7 @@
 
 #include "ctx.h"
 #include "march.h"
+#include "../../include/rkf_cuda_testing.h"
 #include "empty_dist.h"
 #include "tiled.h"
 
@@ -331,3 +332,23 @@ rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st) {
 }
 
 }  // namespace rkf
+
+extern "C" rkf_status rkf_testing_export_coarse(rkf_ctx* ctx, float origin[3], uint32_t dims[3], uint16_t* tex,
+                                                 uint64_t* n) {
+  using namespace rkf;
+  if (!ctx || !origin || !dims || !n) return fail(RKF_INVALID_ARG, "rkf_testing_export_coarse: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  std::vector<Segment> none;
+  TiledDev td;
+  rkf_status st = prepare_tiled(c, none, c->stream, &td);  // builds the field for the current epoch
+  if (st != RKF_OK) return st;
+  RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 3; ++k) {
+    origin[k] = c->coarse_origin[k];
+    dims[k] = c->coarse_dims[k];
+  }
+  *n = static_cast<uint64_t>(dims[0]) * dims[1] * dims[2];
+  if (tex) RKF_CUDA_TRY(cudaMemcpy(tex, c->coarse_tex.p, *n * 2, cudaMemcpyDeviceToHost));
+  return RKF_OK;
+}

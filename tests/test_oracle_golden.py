@@ -11,6 +11,8 @@ import math
 import numpy as np
 import pytest
 
+from conftest import assert_bits_equal
+
 from rkifield_b200 import _abi as abi
 
 
@@ -265,3 +267,62 @@ def test_voxelizer_grid_is_centred_and_band_limited(oracle):
                 assert math.isinf(d[s, x + 8 * y + 64 * zz])
             else:
                 assert abs(d[s, x + 8 * y + 64 * zz] - (r - 1.0)) < 1e-5
+
+
+# ---- coarse field of the tiled strategy (coarse_field.rs) -------------------
+def _aabb_distance(q, lo, hi):
+    """aabb_unsigned_distance (coarse_field.rs): length of max(lo - q, q - hi, 0), in float32."""
+    F = np.float32
+    d = np.maximum(np.maximum(F(lo) - F(q), F(q) - F(hi)), F(0))
+    return np.sqrt((d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2]).astype(F)
+
+
+def _box(lo, hi):
+    from rkifield_b200 import _abi as abi
+    o = abi.rkf_gpu_object()
+    for a in range(3):
+        o.aabb_min[a], o.aabb_max[a] = lo[a], hi[a]
+        o.accumulated_scale[a] = 1.0
+    o.sdf_type = abi.RKF_SDF_ANALYTICAL
+    return o
+
+
+def test_coarse_aabb_distance_matches_reference_tests():
+    """aabb_distance_outside / _inside / _corner (coarse_field.rs:471-500)."""
+    F = np.float32
+    assert abs(_aabb_distance(np.array([3, 0, 0], F), [-1] * 3, [1] * 3) - 2.0) < 1e-5
+    assert _aabb_distance(np.zeros(3, F), [-1] * 3, [1] * 3) == 0.0
+    assert abs(_aabb_distance(np.array([2, 2, 2], F), [0] * 3, [1] * 3) - np.sqrt(F(3))) < 1e-5
+
+
+def test_coarse_field_dims_match_reference_test(oracle):
+    """dims_calculation (coarse_field.rs:502-527): an extent of (4, 2, 6) at
+    0.32 m cells is 13 x 7 x 19 = 1729 cells; here it is an object box of
+    (2, 0, 4) grown by the 1 m margin, origin (-2, -1, -3) as in that test."""
+    origin, dims, tex = oracle.coarse_field([_box((-1.0, 0.0, -2.0), (1.0, 0.0, 2.0))])
+    assert origin.tolist() == [-2.0, -1.0, -3.0]
+    assert dims.tolist() == [13, 7, 19] and tex.size == 1729
+    assert all(dims[a] * np.float32(0.32) >= [4.0, 2.0, 6.0][a] for a in range(3))
+
+
+@pytest.mark.parametrize("boxes", [
+    [((-0.5, -0.5, -0.5), (0.5, 0.5, 0.5))],
+    [((-3.0, 0.0, 1.0), (-1.0, 2.5, 4.0)), ((2.0, -1.0, -1.0), (5.0, 0.5, 0.25)), ((0.0, 3.0, -2.0), (0.5, 3.5, 6.0))],
+])
+def test_coarse_field_texels_match_populate(oracle, boxes):
+    """populate (coarse_field.rs:240-266, as its populate_one_object test runs
+    it): each texel is the binary16 of the smallest distance from the cell
+    centre to an object AABB, starting from cell size x the largest dim."""
+    F = np.float32
+    origin, dims, tex = oracle.coarse_field([_box(lo, hi) for lo, hi in boxes])
+    vs = F(0.32)
+    start = vs * F(dims.max())
+    z, y, x = np.meshgrid(*[np.arange(d, dtype=F) for d in dims[::-1]], indexing="ij")
+    q = np.stack([origin[0] + (x + F(0.5)) * vs, origin[1] + (y + F(0.5)) * vs, origin[2] + (z + F(0.5)) * vs],
+                 axis=-1).astype(F)
+    best = np.full(q.shape[:-1], start, F)
+    for lo, hi in boxes:
+        best = np.minimum(best, _aabb_distance(q, lo, hi))
+    want = best.astype(np.float16).view(np.uint16).ravel()
+    assert_bits_equal(tex, want, "coarse texels")
+    assert (tex == 0).any(), "cells inside a box hold 0"

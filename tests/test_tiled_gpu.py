@@ -165,3 +165,34 @@ def test_single_object_tiled_bit_exact(oracle, small_scene, small_ctx, seed):
         assert_bits_equal(got[k], ref[k], f"single-object tiled {k}")
     brute = oracle.march(sc, cam, scenes.march_params(spec), w, h)
     assert (brute["t"][hit] != ref["t"][hit]).any(), "the coarse field should move some sample points"
+
+
+@pytest.mark.gpu
+def test_device_coarse_field_equals_oracle(oracle, small_scene):
+    """The coarse field the device builds (one thread per cell) is the
+    oracle's, which the golden tests pin to coarse_field.rs: same origin,
+    dims and binary16 texels."""
+    import ctypes as C
+    from rkifield_b200 import _abi as abi
+    from rkifield_b200.engine import Context
+    v = small_scene["vox"]
+    ctx = Context(pool_capacity=v.n_bricks + 1024)
+    try:
+        ctx.set_brick_pool(v.words)
+        ctx.upload_brick_maps(v.map)
+        for objs in (_objects(small_scene), [small_scene["obj"]]):
+            ctx.upload_objects(objs)
+            origin = np.zeros(3, np.float32)
+            dims = np.zeros(3, np.uint32)
+            n = C.c_uint64()
+            abi.check(ctx.lib.rkf_testing_export_coarse(ctx.h, origin.ctypes.data, dims.ctypes.data, None,
+                                                        C.byref(n)), "export coarse")
+            tex = np.zeros(n.value, np.uint16)
+            abi.check(ctx.lib.rkf_testing_export_coarse(ctx.h, origin.ctypes.data, dims.ctypes.data,
+                                                        tex.ctypes.data, C.byref(n)), "export coarse")
+            o_ref, d_ref, t_ref = oracle.coarse_field(objs)
+            assert_bits_equal(origin, o_ref, "coarse origin")
+            assert dims.tolist() == d_ref.tolist()
+            assert_bits_equal(tex, t_ref, "coarse texels")
+    finally:
+        ctx.close()
