@@ -207,6 +207,17 @@ RKF_API rkf_status rkf_brickmap_import(rkf_ctx* ctx, const uint32_t* packed, uin
  * voxelized object from the imported brick maps. */
 RKF_API rkf_status rkf_objects_import(rkf_ctx* ctx, const rkf_gpu_object* objects, uint32_t n);
 
+/* Replace the object records and keep the brick index: the per-frame
+ * GpuScene::upload_objects of the runtime (render.rs:135-137), where
+ * transforms, materials and the set of analytic objects change but the
+ * voxelized objects' brick maps do not.  For a voxelized record i,
+ * index_source[i] names the current object whose index it uses (same
+ * brick_map_dims and voxel_size; NULL: object i's own); other records need
+ * no index.  Works on objects made by rkf_voxelize_prims, which have no
+ * flat brick map to re-import.  On a refused record nothing changes. */
+RKF_API rkf_status rkf_objects_update(rkf_ctx* ctx, const rkf_gpu_object* objects, uint32_t n,
+                                      const int32_t* index_source);
+
 /* One BVH node as the shader reads it (GpuBvhNode, gpu_bvh.rs:24-41;
  * BvhNode, ray_march.wgsl:99-108): 32 bytes. */
 #define RKF_BVH_INVALID 0xFFFFFFFFu

@@ -197,6 +197,7 @@ SIGNATURES = {
     "rkf_brickmap_import": (_I, [_P, _P, _U64]),
     "rkf_objects_import": (_I, [_P, _P, _U32]),
     "rkf_bvh_import": (_I, [_P, _P, _U32]),
+    "rkf_objects_update": (_I, [_P, _P, _U32, _P]),
     "rkf_batch_graph_create": (_I, [_P, C.POINTER(rkf_view), _U32, C.POINTER(rkf_ray_batch), _U32,
                                     C.POINTER(rkf_march_params), C.POINTER(rkf_batch_tuning), C.POINTER(_P)]),
     "rkf_batch_graph_set_cameras": (_I, [_P, C.POINTER(rkf_camera), _U32]),

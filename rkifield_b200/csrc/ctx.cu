@@ -610,6 +610,46 @@ rkf_status rkf_objects_import(rkf_ctx* ctx, const rkf_gpu_object* objects, uint3
   return RKF_OK;
 }
 
+rkf_status rkf_objects_update(rkf_ctx* ctx, const rkf_gpu_object* objects, uint32_t n,
+                              const int32_t* index_source) {
+  if (!ctx || (!objects && n)) return fail(RKF_INVALID_ARG, "rkf_objects_update: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (c->serve) return fail(RKF_BUSY, "rkf_objects_update: the context is serving");
+  RKF_CUDA_TRY(cudaSetDevice(c->device));
+  std::vector<rkf_gpu_object> recs(objects, objects + n);
+  std::vector<ObjDev> od;
+  od.reserve(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    rkf_gpu_object& o = recs[i];
+    if (o.sdf_type > RKF_SDF_VOXELIZED) return fail(RKF_INVALID_ARG, "rkf_objects_update: bad sdf_type");
+    if (o.sdf_type != RKF_SDF_VOXELIZED) {
+      od.push_back(make_objdev(o, 0, 0));
+      continue;
+    }
+    const int64_t s = index_source ? index_source[i] : static_cast<int64_t>(i);
+    if (s < 0 || s >= static_cast<int64_t>(c->obj_count()) ||
+        c->objects[static_cast<size_t>(s)].sdf_type != RKF_SDF_VOXELIZED)
+      return fail(RKF_INVALID_ARG, "rkf_objects_update: a voxelized record names no voxelized object's index");
+    const rkf_gpu_object& e = c->objects[static_cast<size_t>(s)];
+    const ObjDev& ed = c->objdev_host[static_cast<size_t>(s)];
+    if (o.brick_map_dims[0] != e.brick_map_dims[0] || o.brick_map_dims[1] != e.brick_map_dims[1] ||
+        o.brick_map_dims[2] != e.brick_map_dims[2] || o.voxel_size != e.voxel_size)
+      return fail(RKF_INVALID_ARG, "rkf_objects_update: the record's grid differs from its index source");
+    o.brick_map_offset = e.brick_map_offset;  // the brick map the index was built from
+    od.push_back(make_objdev(o, ed.top_off, ed.has_flat));
+  }
+  std::swap(c->objects, recs);
+  std::swap(c->objdev_host, od);
+  rkf_status st = c->upload_objects();
+  if (st != RKF_OK) {
+    std::swap(c->objects, recs);
+    std::swap(c->objdev_host, od);
+    return st;
+  }
+  c->epoch++;
+  return RKF_OK;
+}
+
 rkf_status rkf_object_get(rkf_ctx* ctx, uint32_t i, rkf_gpu_object* out) {
   if (!ctx || !out) return fail(RKF_INVALID_ARG, "rkf_object_get: null argument");
   Ctx* c = reinterpret_cast<Ctx*>(ctx);

@@ -132,6 +132,12 @@ class Context:
         arr = (abi.rkf_gpu_object * len(objects))(*objects)
         check(self.lib.rkf_objects_import(self.h, arr, len(objects)), "rkf_objects_import")
 
+    def update_objects(self, objects, index_source=None):
+        """Replace the object records, keeping the brick index (rkf_objects_update)."""
+        arr = (abi.rkf_gpu_object * max(1, len(objects)))(*objects)
+        src = None if index_source is None else np.ascontiguousarray(index_source, np.int32)
+        check(self.lib.rkf_objects_update(self.h, arr, len(objects), _p(src)), "rkf_objects_update")
+
     def upload_bvh(self, nodes):
         """BVH nodes, root first (an ``rkf_bvh_node`` array); an empty one removes the BVH."""
         check(self.lib.rkf_bvh_import(self.h, nodes if len(nodes) else None, len(nodes)), "rkf_bvh_import")
