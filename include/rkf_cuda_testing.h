@@ -37,6 +37,12 @@ RKF_API void rkf_testing_set_host_bands(int bands);
 RKF_API rkf_status rkf_testing_export_coarse(rkf_ctx* ctx, float origin[3], uint32_t dims[3], uint16_t* tex,
                                              uint64_t* n);
 
+/* Kernel variant of the context's last march launch through rkf_march,
+ * rkf_march_rays or rkf_march_batch: 0 several objects, 1 one object, 2 one
+ * object on the empty-space path, 3 the same under the tiled strategy, 4
+ * several objects on the multi-object empty-space path; -1 before the first. */
+RKF_API int rkf_testing_last_variant(rkf_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -99,6 +99,7 @@ struct Ctx {
   // blocks that no coarse skip can reach (tiled.cu); built for tiled_epoch
   DevBuf tiled_empty_dist;
   uint64_t tiled_epoch = ~0ull;
+  int last_variant = -1;  // kernel variant of the last persistent march launch
   float coarse_origin[3] = {0.0f, 0.0f, 0.0f};
   uint32_t coarse_dims[3] = {0, 0, 0};
   uint64_t coarse_epoch = ~0ull;

@@ -20,9 +20,12 @@
 // idling it until the slowest ray of the warp finishes.  The hit material is
 // read once, from the position that decided it.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <limits>
 #include <vector>
 
+#include "../../include/rkf_cuda_testing.h"
 #include "ctx.h"
 #include "march.h"
 #include "f32x2.cuh"
@@ -48,6 +51,24 @@ struct ColdState {
 };
 static_assert(sizeof(ColdState) % 8 == 4, "ColdState must span an odd number of 32-bit words");
 
+// Multi-object empty-space path.  Each analytic primitive lies inside a ball
+// of radius R around its local origin (sphere r, box |b|, capsule |r|+|h|,
+// torus |R|+|r|, cylinder |(r, h)|), and its exact distance is at least |l|-R
+// at a local position l.  With c the local origin in world space, sigma a
+// lower bound of the smallest singular value of inverse_world's linear part
+// and s the object's min_scale, the FP32 value of evaluate_object at a world
+// position p is at least (sigma*|p - c| - R - rounding)*s.  The host folds
+// the voxelized object's largest EMPTY value and bounds of every rounding
+// (the object's own evaluation, the ray's position, this centre's rounding)
+// into a radius a + b*P, P = |o| + |d|*|tmax| bounding the magnitude of a
+// ray's positions: outside that ball the object's value exceeds every EMPTY
+// value, so wherever the voxelized object samples EMPTY, the minimum over
+// the scene is that sample, bit for bit.
+struct FarBall {
+  float c[3];  // world-space centre
+  float a, b;  // radius a + b * P
+};
+
 struct KParams {
   ObjDev objs[kMaxObjectsFast];  // object table in the constant parameter bank
   SceneDev s;
@@ -72,6 +93,9 @@ struct KParams {
   const rkf_bvh_node* bvh; // BVH strategy: the imported tree, root first
   const uint32_t* bvh_next;  // per node: the walk's next node (bits 0-30), descend (bit 31)
   uint32_t use_bvh;
+  ObjDev vox;                     // multi-object empty-space path: the voxelized object
+  FarBall far[kMaxObjectsFast];   // multi-object empty-space path: the analytic objects' balls
+  uint32_t n_far;
 };
 
 // The candidate loop of ray_march_bvh (ray_march.wgsl:672-721): a stack walk
@@ -135,7 +159,43 @@ __device__ __forceinline__ float eval_bvh(const SceneDev& s, const ObjDev* objs,
 // inverse_world, verified exact quotient, fewer than 2^20 voxels per axis).
 // OBJ_SINGLE_EMPTY_TILED: the empty-space path of a tiled launch (EMPTY runs
 // on the tiled empty-space field, tiled full steps elsewhere).
-enum : int { OBJ_MULTI = 0, OBJ_SINGLE = 1, OBJ_SINGLE_EMPTY = 2, OBJ_SINGLE_EMPTY_TILED = 3 };
+// OBJ_MULTI_EMPTY: one object that qualifies for the empty-space path plus
+// analytic objects that each fit a ball (FarBall) and objects of no type; its
+// EMPTY runs and settling chains stay outside every ball.
+enum : int { OBJ_MULTI = 0, OBJ_SINGLE = 1, OBJ_SINGLE_EMPTY = 2, OBJ_SINGLE_EMPTY_TILED = 3, OBJ_MULTI_EMPTY = 4 };
+
+// Largest t' >= t such that every position of the ray o + d*u, u in [t, t'],
+// lies outside every ball (kMaxFloat when no ball lies ahead); -1 when the
+// position at t may lie inside one.  In double precision: differences and
+// products of floats are exact there, and the rest rounds at 2^-53, whose
+// effect on the entry time (at most ~1e-8 |o - c| / |d| where the ray grazes
+// a ball) the 2^-20 |o - c| widening of each radius covers many times over.
+// A non-finite ray (or a zero direction) makes every ball near.
+__device__ __noinline__ float far_limit(const FarBall* __restrict__ far, uint32_t n, float ox, float oy, float oz,
+                                        float dx, float dy, float dz, float tmax, float t) {
+  const double Dx = dx, Dy = dy, Dz = dz;
+  const double dd = Dx * Dx + Dy * Dy + Dz * Dz;
+  const double P = sqrt(static_cast<double>(ox) * ox + static_cast<double>(oy) * oy + static_cast<double>(oz) * oz) +
+                   sqrt(dd) * fabs(static_cast<double>(tmax));
+  const double td = t;
+  double lim = 1e300;
+  for (uint32_t j = 0; j < n; ++j) {
+    const FarBall& f = far[j];
+    const double wx = static_cast<double>(ox) - f.c[0], wy = static_cast<double>(oy) - f.c[1],
+                 wz = static_cast<double>(oz) - f.c[2];
+    const double rho = (static_cast<double>(f.a) + static_cast<double>(f.b) * P) * (1.0 + 0x1p-20) +
+                       0x1p-20 * sqrt(wx * wx + wy * wy + wz * wz);
+    const double tc = -(Dx * wx + Dy * wy + Dz * wz) / dd;  // closest approach
+    const double qx = wx + Dx * tc, qy = wy + Dy * tc, qz = wz + Dz * tc;
+    const double h2 = qx * qx + qy * qy + qz * qz;
+    if (h2 > rho * rho) continue;  // the line never comes within rho (NaN: not skipped)
+    const double half = sqrt((rho * rho - h2) / dd);
+    const double e = tc - half, x = tc + half;
+    if (td < e) lim = fmin(lim, e);
+    else if (!(td > x)) return -1.0f;  // inside the ball now (or NaN)
+  }
+  return lim >= 3.4028234663852886e38 ? kMaxFloat : __double2float_rd(lim);
+}
 
 // Grid coordinate (position + half grid size, object-local) of the ray at t,
 // rounded exactly as eval_obj -> sample_vox round it for a translation-only
@@ -287,18 +347,19 @@ __device__ __forceinline__ float eval_min(const SceneDev& s, const ObjDev* objs,
 // whose t is past tmax (the full step decides those), after the step that
 // makes max_near samples below near_thr, and where the ray leaves its cube
 // (t > box_t).  INRUN: a lane whose cube ends probes the next cube in place
-// and runs on; stop_full tells whether the next step must be a full one.
+// and runs on (FAR: clipped at far_t, the end of the positions outside every
+// ball); stop_full tells whether the next step must be a full one.
 // PLAIN: the object's translation is zero and its scale one, where adding the
 // translation and multiplying by the scale are exact identities.  CLEAN: every
 // EMPTY value is at least brk, near_thr and min_step (the caller checks this
 // against a lower bound), so those comparisons are known and skipped.
 // Returns the number of steps taken.
-template <bool PLAIN, bool CLEAN, bool INRUN>
+template <bool PLAIN, bool CLEAN, bool INRUN, bool FAR>
 __device__ __forceinline__ uint32_t empty_run(const ObjDev& o, const uint8_t* __restrict__ field, float ox,
                                               float oy, float oz, float dx, float dy, float dz, float tmax,
                                               uint32_t n, float brk, float near_thr, float min_step,
-                                              uint32_t max_near, float& t, float& box_t, float& prev_t,
-                                              float& prev_dist, uint32_t& near, bool& stop_full) {
+                                              uint32_t max_near, float far_t, float& t, float& box_t,
+                                              float& prev_t, float& prev_dist, uint32_t& near, bool& stop_full) {
   uint32_t c = 0;
   float lim = fminf(box_t, tmax);
   stop_full = false;
@@ -310,6 +371,7 @@ __device__ __forceinline__ uint32_t empty_run(const ObjDev& o, const uint8_t* __
         break;
       }
       box_t = probe_empty(o, field, ox, oy, oz, dx, dy, dz, t);
+      if (FAR) box_t = fminf(box_t, far_t);
       lim = fminf(box_t, tmax);
       if (t > lim) {
         stop_full = true;
@@ -353,10 +415,10 @@ __device__ __forceinline__ uint32_t empty_run(const ObjDev& o, const uint8_t* __
 // empty_run<PLAIN=true, CLEAN=true> with the x and y chains of a step packed
 // into two-wide FP32 instructions (z stays scalar): the same operations on
 // the same values, so the same bits.
-template <bool INRUN>
+template <bool INRUN, bool FAR>
 __device__ __forceinline__ uint32_t empty_run_x2(const ObjDev& o, const uint8_t* __restrict__ field, float ox,
                                                  float oy, float oz, float dx, float dy, float dz, float tmax,
-                                                 uint32_t n, float& t, float& box_t, float& prev_t,
+                                                 uint32_t n, float far_t, float& t, float& box_t, float& prev_t,
                                                  float& prev_dist, bool& stop_full) {
   uint32_t c = 0;
   float lim = fminf(box_t, tmax);
@@ -372,6 +434,7 @@ __device__ __forceinline__ uint32_t empty_run_x2(const ObjDev& o, const uint8_t*
         break;
       }
       box_t = probe_empty(o, field, ox, oy, oz, dx, dy, dz, t);
+      if (FAR) box_t = fminf(box_t, far_t);
       lim = fminf(box_t, tmax);
       if (t > lim) {
         stop_full = true;
@@ -398,9 +461,11 @@ __device__ __forceinline__ uint32_t empty_run_x2(const ObjDev& o, const uint8_t*
 
 template <int PREC, int OBJ>
 __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_constant__ KParams kp) {
-  constexpr bool SINGLE = OBJ != OBJ_MULTI;
-  constexpr bool EMPTY_PATH = OBJ == OBJ_SINGLE_EMPTY || OBJ == OBJ_SINGLE_EMPTY_TILED;
-  constexpr bool TILES = OBJ != OBJ_SINGLE_EMPTY;  // tile bookkeeping of tiled launches
+  constexpr bool MULTI_EMPTY = OBJ == OBJ_MULTI_EMPTY;
+  constexpr bool SINGLE = OBJ != OBJ_MULTI && !MULTI_EMPTY;
+  constexpr bool EMPTY_PATH = OBJ == OBJ_SINGLE_EMPTY || OBJ == OBJ_SINGLE_EMPTY_TILED || MULTI_EMPTY;
+  // tile bookkeeping of tiled launches
+  constexpr bool TILES = OBJ != OBJ_SINGLE_EMPTY && !MULTI_EMPTY;
   const ObjDev* sh_objs = kp.objs;
   const SceneDev& s = kp.s;
   const rkf_march_params& p = kp.p;
@@ -418,6 +483,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
   float ox = 0, oy = 0, oz = 0, rdx = 0, rdy = 0, rdz = 0;
   float t = 0, prev_t = 0, prev_dist = kMaxFloat, tmax = 0;
   float box_t = -1.0f;  // empty-space path: positions up to here sample the EMPTY value
+  float far_t = -1.0f;  // multi-object empty-space path: positions up to here lie outside every ball
   uint32_t near = 0, step = 0;
   bool exhausted = false;
 
@@ -494,6 +560,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
               near = 0;
               step = 0;
               box_t = -1.0f;
+              if (MULTI_EMPTY) far_t = -1.0f;
               prev_dist = kMaxFloat;
               cs.hit = cs.bisected = cs.mat_ok = false;
               if (mode == RKF_TRACE_SHADOW) {
@@ -529,7 +596,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
       if (EMPTY_PATH && (state == ST_MARCH || state == ST_SHADOW)) {
         // empty-space run: inside a cube of EMPTY blocks every sample is
         // empty_value(), so up to kp.budget steps run without the sampler
-        const ObjDev& o0 = sh_objs[0];
+        const ObjDev& o0 = MULTI_EMPTY ? kp.vox : sh_objs[0];
         const bool sh = state == ST_SHADOW;
         const float dx = sh ? rdx : qdx, dy = sh ? rdy : qdy, dz = sh ? rdz : qdz;
         const uint32_t max_step = sh ? 256u : p.hard_max_steps;
@@ -541,6 +608,11 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
         const bool clean = kp.empty_lo >= brk && kp.empty_lo >= near_thr && kp.empty_lo >= min_step;
         if (t > box_t && prev_dist >= kp.probe_min) {
           box_t = probe_empty(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, t);
+          const float cube_t = box_t;
+          if (MULTI_EMPTY) {  // only positions outside every ball sample the EMPTY value
+            if (t <= box_t) far_t = far_limit(kp.far, kp.n_far, ox, oy, oz, dx, dy, dz, tmax, t);
+            box_t = fminf(box_t, far_t);
+          }
           if (t <= box_t && clean && kp.settle_links && step < max_step && near < max_near) {
             // Settle the ray if every sample it has left is the EMPTY value:
             // then no threshold acts on it, it misses, and its outputs do not
@@ -559,7 +631,12 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
             const bool out_of_steps = t_hi <= tmax;
             if (out_of_steps || t_lo > tmax) {
               const float need = out_of_steps ? t_hi : tmax;
-              box_t = extend_cover(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, box_t, need, kp.settle_links);
+              if (!MULTI_EMPTY) {
+                box_t = extend_cover(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, box_t, need, kp.settle_links);
+              } else if (far_t >= need) {
+                box_t = fminf(extend_cover(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, cube_t, need, kp.settle_links),
+                              far_t);
+              }
               if (box_t >= need) {
                 if (sh) cs.shadow = clampf(cs.shadow, 0.0f, 1.0f);
                 else if (out_of_steps) step = max_step;
@@ -575,13 +652,13 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
           bool stop_full = true;
           if (near < max_near) {
 #define RKF_RUN(P, CL, IN)                                                                                   \
-  empty_run<P, CL, IN>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n, brk, near_thr, min_step, max_near, t, \
-                       box_t, prev_t, prev_dist, near, stop_full)
+  empty_run<P, CL, IN, MULTI_EMPTY>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n, brk, near_thr, min_step, \
+                                    max_near, far_t, t, box_t, prev_t, prev_dist, near, stop_full)
             if (kp.plain_obj && clean)
-              c = kp.run_probe ? empty_run_x2<true>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n, t, box_t,
-                                                    prev_t, prev_dist, stop_full)
-                               : empty_run_x2<false>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n, t, box_t,
-                                                     prev_t, prev_dist, stop_full);
+              c = kp.run_probe ? empty_run_x2<true, MULTI_EMPTY>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n,
+                                                                 far_t, t, box_t, prev_t, prev_dist, stop_full)
+                               : empty_run_x2<false, MULTI_EMPTY>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n,
+                                                                  far_t, t, box_t, prev_t, prev_dist, stop_full);
             else if (kp.plain_obj)
               c = kp.run_probe ? RKF_RUN(true, false, true) : RKF_RUN(true, false, false);
             else
@@ -972,6 +1049,7 @@ __global__ void k_sdf_ao(SceneDev s, const float* __restrict__ pos, const float*
 
 template <int PREC>
 const void* persistent_fn(int obj) {
+  if (obj == OBJ_MULTI_EMPTY) return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_MULTI_EMPTY>);
   if (obj == OBJ_SINGLE_EMPTY) return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_SINGLE_EMPTY>);
   if (obj == OBJ_SINGLE_EMPTY_TILED)
     return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_SINGLE_EMPTY_TILED>);
@@ -982,14 +1060,127 @@ const void* persistent_fn(int obj) {
 }  // namespace detail
 
 namespace {
+// A voxelized object the empty-space path can march: translation-only
+// inverse_world, verified exact quotient, fewer than 2^20 voxels per axis.
+bool empty_object(const Ctx* c, const ObjDev& o) {
+  return o.sdf_type == RKF_SDF_VOXELIZED && o.translate_only && o.div_ok && c->empty_dist.p != nullptr &&
+         o.tv[0] < (1 << 20) && o.tv[1] < (1 << 20) && o.tv[2] < (1 << 20);
+}
+
+// Upper bound of every EMPTY value of a voxelized object: mix(c, c, t) three
+// times stays within 12 roundings of c = brick extent * min_scale (relative
+// 2^-24 each), far inside 2^-16.
+float empty_hi_of(const ObjDev& o) { return o.be * o.min_scale * (1.0f + 1.52587890625e-5f); }
+
+// Radius of the ball around the local origin that holds an analytic
+// primitive (analytic_sdf, ray_march.wgsl:182-264): its value is at least
+// |l| - R everywhere.  -1 for a plane (unbounded) or non-finite parameters.
+double prim_radius(const ObjDev& o) {
+  const double a0 = std::fabs(static_cast<double>(o.params[0])), a1 = std::fabs(static_cast<double>(o.params[1])),
+               a2 = std::fabs(static_cast<double>(o.params[2]));
+  double r = -1.0;
+  switch (o.prim_type) {
+    case RKF_PRIM_SPHERE: r = a0; break;
+    case RKF_PRIM_BOX: r = std::sqrt(a0 * a0 + a1 * a1 + a2 * a2); break;
+    case RKF_PRIM_CAPSULE: r = a0 + a1; break;
+    case RKF_PRIM_TORUS: r = a0 + a1; break;
+    case RKF_PRIM_CYLINDER: r = std::sqrt(a0 * a0 + a1 * a1); break;
+    default: return -1.0;
+  }
+  return std::isfinite(r) ? r : -1.0;
+}
+
+double up_float(double v) {  // a float >= v
+  const float f = static_cast<float>(v);
+  return static_cast<double>(f) >= v ? f : std::nextafter(f, std::numeric_limits<float>::infinity());
+}
+
+// The FarBall of an analytic object for EMPTY values up to empty_hi (the
+// bound FarBall describes, with every FP32 rounding of evaluate_object held
+// to 2^-16 of the magnitudes involved, a wide margin over the few 2^-24
+// roundings each step makes).  false when the object has no usable ball.
+bool far_ball(const ObjDev& o, float empty_hi, detail::FarBall* out) {
+  const double R = prim_radius(o);
+  const double s = o.min_scale;
+  if (R < 0.0 || !(s > 0.0) || !std::isfinite(s)) return false;
+  double A[3][3], t[3];  // l_i = sum_k A[i][k] p_k + t_i (to_local)
+  for (int i = 0; i < 3; ++i) {
+    for (int k = 0; k < 3; ++k) A[i][k] = o.m[4 * k + i];
+    t[i] = o.m[12 + i];
+  }
+  const double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                     A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                     A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+  if (!std::isfinite(det) || det == 0.0) return false;
+  double inv[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int k = 0; k < 3; ++k) {
+      const int i1 = (k + 1) % 3, i2 = (k + 2) % 3, k1 = (i + 1) % 3, k2 = (i + 2) % 3;
+      inv[i][k] = (A[i1][k1] * A[i2][k2] - A[i1][k2] * A[i2][k1]) / det;
+    }
+  double nf = 0.0, nif = 0.0, tn = 0.0, c[3], cn = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    c[i] = -(inv[i][0] * t[0] + inv[i][1] * t[1] + inv[i][2] * t[2]);
+    cn += c[i] * c[i];
+    tn += t[i] * t[i];
+    for (int k = 0; k < 3; ++k) {
+      nf += A[i][k] * A[i][k];
+      nif += inv[i][k] * inv[i][k];
+    }
+  }
+  const double N = std::sqrt(nf), sigma = 1.0 / std::sqrt(nif);  // |A x| >= sigma |x|
+  const double e16 = 0x1p-16, e20 = 0x1p-20;
+  if (!(sigma > 0.0) || !(N / sigma <= 1024.0)) return false;
+  const double a = (R * (1.0 + e16) + e16 * std::sqrt(tn) + static_cast<double>(empty_hi) * (1.0 + e16) / s) / sigma +
+                   e20 * std::sqrt(cn);
+  const double b = e16 * N / sigma + e20;
+  for (int i = 0; i < 3; ++i) out->c[i] = static_cast<float>(c[i]);
+  out->a = static_cast<float>(up_float(a));
+  out->b = static_cast<float>(up_float(b));
+  return std::isfinite(out->c[0]) && std::isfinite(out->c[1]) && std::isfinite(out->c[2]) && std::isfinite(out->a) &&
+         std::isfinite(out->b);
+}
+
+// A scene of several objects the multi-object empty-space path can march:
+// exactly one object that is not analytic or of no type, which qualifies for
+// the empty-space path, and analytic objects that each have a ball (or whose
+// every value exceeds the EMPTY values).  Fills the voxelized object's index
+// and the balls when the pointers are given.
+bool multi_empty_scene(const Ctx* c, uint32_t* vi_out, detail::FarBall* far, uint32_t* n_far) {
+  const uint32_t n = c->obj_count();
+  if (n < 2 || n > kMaxObjectsFast) return false;
+  uint32_t vi = n;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t ty = c->objdev_host[i].sdf_type;
+    if (ty == RKF_SDF_NONE || ty == RKF_SDF_ANALYTICAL) continue;
+    if (vi != n) return false;
+    vi = i;
+  }
+  if (vi == n || !empty_object(c, c->objdev_host[vi])) return false;
+  const float hi = empty_hi_of(c->objdev_host[vi]);
+  uint32_t nb = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const ObjDev& o = c->objdev_host[i];
+    if (i == vi || o.sdf_type == RKF_SDF_NONE) continue;  // no type: kMaxFloat
+    if (o.prim_type > RKF_PRIM_PLANE) {  // an unknown primitive: kMaxFloat * min_scale
+      if (static_cast<double>(kMaxFloat) * o.min_scale * (1.0 - 0x1p-20) >= hi) continue;
+      return false;
+    }
+    detail::FarBall b;
+    if (!far_ball(o, hi, &b)) return false;
+    if (far) far[nb] = b;
+    ++nb;
+  }
+  if (vi_out) *vi_out = vi;
+  if (n_far) *n_far = nb;
+  return true;
+}
+
 // Which kernel variant a launch over this context's objects uses.
 int object_set(const Ctx* c) {
-  if (c->obj_count() != 1) return detail::OBJ_MULTI;
-  const ObjDev& o = c->objdev_host[0];
-  const bool empty_path = o.sdf_type == RKF_SDF_VOXELIZED && o.translate_only && o.div_ok &&
-                          c->empty_dist.p != nullptr && o.tv[0] < (1 << 20) && o.tv[1] < (1 << 20) &&
-                          o.tv[2] < (1 << 20);
-  return empty_path ? detail::OBJ_SINGLE_EMPTY : detail::OBJ_SINGLE;
+  if (c->obj_count() != 1)
+    return multi_empty_scene(c, nullptr, nullptr, nullptr) ? detail::OBJ_MULTI_EMPTY : detail::OBJ_MULTI;
+  return empty_object(c, c->objdev_host[0]) ? detail::OBJ_SINGLE_EMPTY : detail::OBJ_SINGLE;
 }
 }  // namespace
 
@@ -1049,27 +1240,35 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
     obj = detail::OBJ_SINGLE_EMPTY_TILED;
     kp.s.empty_dist = c->tiled_empty_dist.as<uint8_t>();
   }
-  const bool empty = obj == detail::OBJ_SINGLE_EMPTY || obj == detail::OBJ_SINGLE_EMPTY_TILED;
+  // the multi-object empty-space path marches the brute strategy only
+  if (objs == detail::OBJ_MULTI_EMPTY && (tiled || walk)) obj = detail::OBJ_MULTI;
+  if (obj == detail::OBJ_MULTI_EMPTY) {
+    uint32_t vi = 0;
+    multi_empty_scene(c, &vi, kp.far, &kp.n_far);
+    kp.vox = c->objdev_host[vi];
+  } else {
+    kp.vox = kp.objs[0];
+  }
+  const bool empty = obj == detail::OBJ_SINGLE_EMPTY || obj == detail::OBJ_SINGLE_EMPTY_TILED ||
+                     obj == detail::OBJ_MULTI_EMPTY;
   kp.td = td;
   kp.tiled = tiled ? 1u : 0u;
   kp.bvh = walk ? c->bvh.as<rkf_bvh_node>() : nullptr;
   kp.bvh_next = walk ? c->bvh_next.as<uint32_t>() : nullptr;
   kp.use_bvh = walk ? 1u : 0u;
-  kp.probe_min = empty ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
+  const ObjDev& e0 = kp.vox;  // the object of the empty-space path
+  kp.probe_min = empty ? 0.99f * e0.be * e0.min_scale : kMaxFloat;
   kp.budget = tu.step_budget ? tu.step_budget : 32;
   kp.refill_active = 32u - std::min<uint32_t>(tu.refill_idle ? tu.refill_idle : 32u, 32u);
   kp.run_probe = tu.probe_in_run ? 1u : 0u;
   // mix(c, c, t) three times stays within 12 roundings of c (relative 2^-24
   // each); 0.999 leaves a wide margin
-  kp.empty_lo = empty ? 0.999f * kp.objs[0].be * kp.objs[0].min_scale : 0.0f;
+  kp.empty_lo = empty ? 0.999f * e0.be * e0.min_scale : 0.0f;
   // twelve roundings of 2^-24 stay far inside 2^-16
-  kp.empty_lo_t = kp.objs[0].be * kp.objs[0].min_scale * (1.0f - 1.52587890625e-5f);
-  kp.empty_hi = kp.objs[0].be * kp.objs[0].min_scale * (1.0f + 1.52587890625e-5f);
+  kp.empty_lo_t = e0.be * e0.min_scale * (1.0f - 1.52587890625e-5f);
+  kp.empty_hi = empty_hi_of(e0);
   kp.settle_links = empty ? 48u : 0u;
-  kp.plain_obj = (kp.objs[0].m[12] == 0.0f && kp.objs[0].m[13] == 0.0f && kp.objs[0].m[14] == 0.0f &&
-                  kp.objs[0].min_scale == 1.0f)
-                     ? 1u
-                     : 0u;
+  kp.plain_obj = (e0.m[12] == 0.0f && e0.m[13] == 0.0f && e0.m[14] == 0.0f && e0.min_scale == 1.0f) ? 1u : 0u;
   const void* fn = nullptr;
   switch (c->cfg.precision) {
     case RKF_PRECISION_F32:
@@ -1081,6 +1280,7 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
     default:
       fn = detail::persistent_fn<RKF_PRECISION_F16>(obj);
   }
+  c->last_variant = obj;
   const uint32_t threads = tu.threads_per_block ? tu.threads_per_block : 256;
   if (threads > 256 || threads % 32)
     return fail(RKF_INVALID_ARG, "march: threads_per_block must be a multiple of 32 <= 256");
@@ -1125,7 +1325,10 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
   kp.counter = dev_counter;
   kp.p = *p;
   kp.p.scene.num_objects = c->obj_count();
-  const int obj = object_set(c);
+  // this launch path keeps the variants it had: several objects march the
+  // plain multi-object kernel
+  int obj = object_set(c);
+  if (obj == detail::OBJ_MULTI_EMPTY) obj = detail::OBJ_MULTI;
   kp.probe_min = obj == detail::OBJ_SINGLE_EMPTY ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
   kp.budget = tu.step_budget ? tu.step_budget : 32;
   kp.refill_active = 32u - std::min<uint32_t>(tu.refill_idle ? tu.refill_idle : 32u, 32u);
@@ -1258,3 +1461,7 @@ Segment ray_segment(const float* o, const float* d, const float* tmax, uint32_t 
 }
 
 }  // namespace rkf
+
+extern "C" int rkf_testing_last_variant(rkf_ctx* ctx) {
+  return ctx ? reinterpret_cast<rkf::Ctx*>(ctx)->last_variant : -1;
+}

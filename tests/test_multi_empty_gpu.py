@@ -1,0 +1,177 @@
+"""The multi-object empty-space path: one voxelized object beside analytic
+objects and objects of no type.  EMPTY runs and settling chains stay outside
+each analytic object's ball (its primitive's bounding radius mapped to world
+space, widened by the largest EMPTY value and every rounding bound), so the
+minimum over the scene there is the voxelized object's EMPTY value, and every
+output stays bit-exact against the oracle: views, and ray casts in the three
+modes (closest, any hit, soft shadow), with analytic objects outside the
+grid, just beyond it and inside it, rotated and non-uniformly scaled, and the
+voxelized object not first in the list.  Scenes the path does not cover (a
+plane; the tiled strategy) march the plain multi-object kernel."""
+import numpy as np
+import pytest
+
+from conftest import assert_bits_equal
+from test_tiled_gpu import PLANES, _analytic, _camera, _params
+from test_trace_gpu import _rays
+
+pytestmark = pytest.mark.gpu
+
+
+VARIANT_MULTI, VARIANT_MULTI_EMPTY = 0, 4
+
+
+def _rotation(axis, angle):
+    a = np.asarray(axis, np.float64)
+    a /= np.linalg.norm(a)
+    k = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+    return np.eye(3) + np.sin(angle) * k + (1 - np.cos(angle)) * (k @ k)
+
+
+def _transformed(ptype, centre, params, rot, scale, mat, oid):
+    """An analytic object whose local frame is scaled by `scale`, rotated by
+    `rot` and moved to `centre`: inverse_world maps world to local,
+    l = S^-1 R^T (p - c)."""
+    o = _analytic(ptype, centre, params, (1.0, 1.0, 1.0), mat, oid)
+    a = np.diag(1.0 / np.asarray(scale, np.float64)) @ rot.T
+    t = -a @ np.asarray(centre, np.float64)
+    for i in range(3):
+        for k in range(3):
+            o.inverse_world[4 * k + i] = float(a[i, k])
+        o.inverse_world[12 + i] = float(t[i])
+        o.accumulated_scale[i] = float(scale[i])
+    ext = float(np.linalg.norm(params[:3])) * float(max(scale)) + 1.0
+    for i in range(3):
+        o.aabb_min[i] = float(centre[i] - ext)
+        o.aabb_max[i] = float(centre[i] + ext)
+    return o
+
+
+def _none_object(oid):
+    o = _analytic(0, (0.0, 0.0, 0.0), (1.0,), (1.0, 1.0, 1.0), 0, oid)
+    from rkifield_b200 import _abi as abi
+    o.sdf_type = abi.RKF_SDF_NONE
+    return o
+
+
+def _scene_objects(small_scene):
+    return [_analytic(0, (30.0, 0.0, 0.0), (3.0,), (3.0, 3.0, 3.0), 5, 2),                     # sphere beyond the grid
+            small_scene["obj"],                                                                 # voxelized (index 1)
+            _analytic(3, (0.0, 19.5, 0.0), (4.0, 1.0), (5.0, 1.0, 5.0), 6, 3),                  # torus just above it
+            _transformed(1, (-10.0, 2.0, 8.0), (2.0, 1.0, 1.5), _rotation((1, 2, 3), 0.7),
+                         (1.5, 0.7, 1.2), 7, 4),                                                # rotated, scaled box
+            _none_object(5),
+            _analytic(2, (12.0, -5.0, -9.0), (1.0, 2.5), (1.0, 3.5, 1.0), 8, 6),                # capsule inside the grid
+            _analytic(4, (-5.0, 12.0, -14.0), (2.0, 1.5), (2.0, 1.5, 2.0), 9, 7)]               # cylinder inside the grid
+
+
+def _context(small_scene, objs):
+    from rkifield_b200.engine import Context
+    v = small_scene["vox"]
+    ctx = Context(pool_capacity=v.n_bricks + 1024)
+    ctx.set_brick_pool(v.words)
+    ctx.upload_brick_maps(v.map)
+    ctx.upload_objects(objs)
+    return ctx
+
+
+@pytest.mark.parametrize("seed", [3, 5, 8])
+def test_views_bit_exact(oracle, small_scene, seed):
+    v = small_scene["vox"]
+    objs = _scene_objects(small_scene)
+    sc = oracle.Scene(objs, pool_words=v.words, brick_maps=v.map)
+    ctx = _context(small_scene, objs)
+    try:
+        w, h = 200, 136
+        cam = _camera(seed, w, h)
+        p = _params(0)
+        ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+        got = ctx.march(cam, p, w, h, reference_planes=True)
+        assert ctx.lib.rkf_testing_last_variant(ctx.h) == VARIANT_MULTI_EMPTY
+        hit = (ref["flags"] & 1) != 0
+        assert hit.sum() > 500
+        for k in PLANES:
+            assert_bits_equal(got[k], ref[k], f"seed {seed}: {k}")
+    finally:
+        ctx.close()
+
+
+def test_views_see_the_analytic_objects(oracle, small_scene):
+    """A camera close to the torus and the box: rays graze the balls."""
+    from rkifield_b200 import scenes
+    v = small_scene["vox"]
+    objs = _scene_objects(small_scene)
+    sc = oracle.Scene(objs, pool_words=v.words, brick_maps=v.map)
+    ctx = _context(small_scene, objs)
+    try:
+        w, h = 160, 120
+        p = _params(0)
+        seen = set()
+        for eye, target in (((0.0, 32.0, 18.0), (0.0, 19.5, 0.0)), ((-22.0, 6.0, 24.0), (-10.0, 2.0, 8.0))):
+            cam = scenes.camera_uniforms(eye, target, w, h)
+            ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+            got = ctx.march(cam, p, w, h, reference_planes=True)
+            assert ctx.lib.rkf_testing_last_variant(ctx.h) == VARIANT_MULTI_EMPTY
+            for k in PLANES:
+                assert_bits_equal(got[k], ref[k], f"eye {eye}: {k}")
+            hit = (ref["flags"] & 1) != 0
+            seen |= set(((ref["packed_material"][hit] >> 24) & 0xFF).tolist())
+        assert {3, 4} <= seen, f"object ids seen: {sorted(seen)}"
+    finally:
+        ctx.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2], ids=["closest", "any", "shadow"])
+def test_rays_bit_exact(oracle, small_scene, mode):
+    from rkifield_b200 import scenes
+    v = small_scene["vox"]
+    objs = _scene_objects(small_scene)
+    sc = oracle.Scene(objs, pool_words=v.words, brick_maps=v.map)
+    ctx = _context(small_scene, objs)
+    try:
+        o, d, tmax = _rays(20000, seed=40 + mode, box=24.0)
+        p = scenes.march_params(small_scene["spec"])
+        ref = oracle.trace(sc, o.ravel(), d.ravel(), tmax, mode, p)
+        got = ctx.trace(o, d, tmax, mode, p)
+        assert ctx.lib.rkf_testing_last_variant(ctx.h) == VARIANT_MULTI_EMPTY
+        assert_bits_equal(got["t"], ref["t"], "t")
+        assert_bits_equal(got["flags"], ref["flags"], "flags")
+        if mode == 0:
+            for k in ("normal", "slot", "material"):
+                assert_bits_equal(got[k], ref[k], k)
+        assert 100 < int((ref["flags"] & 1).sum()) < 20000
+    finally:
+        ctx.close()
+
+
+def test_scenes_outside_the_path_march_the_plain_kernel(oracle, small_scene):
+    from rkifield_b200 import _abi as abi
+    v = small_scene["vox"]
+    w, h = 96, 64
+    cam = _camera(4, w, h)
+    # a plane has no ball
+    objs = _scene_objects(small_scene) + [_analytic(5, (0.0, -17.0, 0.0), (0.0, 1.0, 0.0), (50.0, 0.1, 50.0), 3, 8)]
+    sc = oracle.Scene(objs, pool_words=v.words, brick_maps=v.map)
+    ctx = _context(small_scene, objs)
+    try:
+        p = _params(0)
+        ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+        got = ctx.march(cam, p, w, h, reference_planes=True)
+        assert ctx.lib.rkf_testing_last_variant(ctx.h) == VARIANT_MULTI
+        for k in PLANES:
+            assert_bits_equal(got[k], ref[k], f"with a plane: {k}")
+    finally:
+        ctx.close()
+    # the tiled strategy keeps its own kernel
+    objs = _scene_objects(small_scene)
+    sc = oracle.Scene(objs, pool_words=v.words, brick_maps=v.map)
+    ctx = _context(small_scene, objs)
+    try:
+        p = _params(abi.RKF_STRATEGY_TILED)
+        ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+        got = ctx.march(cam, p, w, h, reference_planes=True)
+        assert ctx.lib.rkf_testing_last_variant(ctx.h) == VARIANT_MULTI
+        for k in PLANES:
+            assert_bits_equal(got[k], ref[k], f"tiled: {k}")
+    finally:
+        ctx.close()
