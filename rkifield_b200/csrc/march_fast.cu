@@ -164,37 +164,81 @@ __device__ __forceinline__ float eval_bvh(const SceneDev& s, const ObjDev* objs,
 // EMPTY runs and settling chains stay outside every ball.
 enum : int { OBJ_MULTI = 0, OBJ_SINGLE = 1, OBJ_SINGLE_EMPTY = 2, OBJ_SINGLE_EMPTY_TILED = 3, OBJ_MULTI_EMPTY = 4 };
 
+// Interval helpers in directed rounding: each result interval contains the
+// exact result for every value of the operand intervals.
+__device__ __forceinline__ void iv_mul(float x, float lo, float hi, float& rlo, float& rhi) {  // x * [lo, hi]
+  if (x >= 0.0f) {
+    rlo = __fmul_rd(x, lo);
+    rhi = __fmul_ru(x, hi);
+  } else {
+    rlo = __fmul_rd(x, hi);
+    rhi = __fmul_ru(x, lo);
+  }
+}
+__device__ __forceinline__ void iv_sq(float lo, float hi, float& rlo, float& rhi) {  // [lo, hi]^2
+  const float mlo = lo > 0.0f ? lo : (hi < 0.0f ? -hi : 0.0f);
+  const float mhi = fmaxf(fabsf(lo), fabsf(hi));
+  rlo = __fmul_rd(mlo, mlo);
+  rhi = __fmul_ru(mhi, mhi);
+}
+
 // Largest t' >= t such that every position of the ray o + d*u, u in [t, t'],
 // lies outside every ball (kMaxFloat when no ball lies ahead); -1 when the
-// position at t may lie inside one.  In double precision: differences and
-// products of floats are exact there, and the rest rounds at 2^-53, whose
-// effect on the entry time (at most ~1e-8 |o - c| / |d| where the ray grazes
-// a ball) the 2^-20 |o - c| widening of each radius covers many times over.
-// A non-finite ray (or a zero direction) makes every ball near.
-__device__ __noinline__ float far_limit(const FarBall* __restrict__ far, uint32_t n, float ox, float oy, float oz,
-                                        float dx, float dy, float dz, float tmax, float t) {
-  const double Dx = dx, Dy = dy, Dz = dz;
-  const double dd = Dx * Dx + Dy * Dy + Dz * Dz;
-  const double P = sqrt(static_cast<double>(ox) * ox + static_cast<double>(oy) * oy + static_cast<double>(oz) * oz) +
-                   sqrt(dd) * fabs(static_cast<double>(tmax));
-  const double td = t;
-  double lim = 1e300;
+// position at t may lie inside one, with *recheck set to the earliest time
+// the ray may leave the balls that may hold it (else -1).  Per ball, with
+// w = o - c: the line's squared distance to the centre is |w|^2 - (d.w)^2/|d|^2,
+// its closest approach is at -(d.w)/|d|^2, and the chord within the ball
+// spans sqrt((rho^2 - h^2)/|d|^2) on each side.  Every quantity is an interval
+// evaluated in directed rounding, so the entry time used is a lower bound
+// and the exit time an upper bound of the exact ones.  A non-finite ray (or
+// a zero direction) makes every ball near.
+__device__ __forceinline__ float far_limit(const FarBall* __restrict__ far, uint32_t n, float ox, float oy,
+                                           float oz, float dx, float dy, float dz, float tmax, float t,
+                                           float& recheck) {
+  const float a_lo = __fadd_rd(__fadd_rd(__fmul_rd(dx, dx), __fmul_rd(dy, dy)), __fmul_rd(dz, dz));
+  const float a_hi = __fadd_ru(__fadd_ru(__fmul_ru(dx, dx), __fmul_ru(dy, dy)), __fmul_ru(dz, dz));
+  // P >= |o| + |d| |tmax| (an L1 norm bounds the L2 norm)
+  const float P = __fadd_ru(__fadd_ru(__fadd_ru(fabsf(ox), fabsf(oy)), fabsf(oz)),
+                            __fmul_ru(__fsqrt_ru(a_hi), fabsf(tmax)));
+  float lim = kMaxFloat;
+  bool inside = false;
+  recheck = kMaxFloat;
   for (uint32_t j = 0; j < n; ++j) {
     const FarBall& f = far[j];
-    const double wx = static_cast<double>(ox) - f.c[0], wy = static_cast<double>(oy) - f.c[1],
-                 wz = static_cast<double>(oz) - f.c[2];
-    const double rho = (static_cast<double>(f.a) + static_cast<double>(f.b) * P) * (1.0 + 0x1p-20) +
-                       0x1p-20 * sqrt(wx * wx + wy * wy + wz * wz);
-    const double tc = -(Dx * wx + Dy * wy + Dz * wz) / dd;  // closest approach
-    const double qx = wx + Dx * tc, qy = wy + Dy * tc, qz = wz + Dz * tc;
-    const double h2 = qx * qx + qy * qy + qz * qz;
-    if (h2 > rho * rho) continue;  // the line never comes within rho (NaN: not skipped)
-    const double half = sqrt((rho * rho - h2) / dd);
-    const double e = tc - half, x = tc + half;
-    if (td < e) lim = fmin(lim, e);
-    else if (!(td > x)) return -1.0f;  // inside the ball now (or NaN)
+    const float rho = __fadd_ru(f.a, __fmul_ru(f.b, P));
+    const float rho2 = __fmul_ru(rho, rho);
+    const float wxl = __fsub_rd(ox, f.c[0]), wxh = __fsub_ru(ox, f.c[0]);
+    const float wyl = __fsub_rd(oy, f.c[1]), wyh = __fsub_ru(oy, f.c[1]);
+    const float wzl = __fsub_rd(oz, f.c[2]), wzh = __fsub_ru(oz, f.c[2]);
+    float sxl, sxh, syl, syh, szl, szh;
+    iv_sq(wxl, wxh, sxl, sxh);
+    iv_sq(wyl, wyh, syl, syh);
+    iv_sq(wzl, wzh, szl, szh);
+    const float W_lo = __fadd_rd(__fadd_rd(sxl, syl), szl);
+    float pxl, pxh, pyl, pyh, pzl, pzh;  // d.w
+    iv_mul(dx, wxl, wxh, pxl, pxh);
+    iv_mul(dy, wyl, wyh, pyl, pyh);
+    iv_mul(dz, wzl, wzh, pzl, pzh);
+    const float b_lo = __fadd_rd(__fadd_rd(pxl, pyl), pzl), b_hi = __fadd_ru(__fadd_ru(pxh, pyh), pzh);
+    float b2l, b2h;
+    iv_sq(b_lo, b_hi, b2l, b2h);
+    const float h2_lo = __fsub_rd(W_lo, __fdiv_ru(b2h, a_lo));
+    if (h2_lo > rho2) continue;  // the line never comes within rho (NaN: not skipped)
+    const float half = __fsqrt_ru(__fdiv_ru(__fsub_ru(rho2, h2_lo), a_lo));
+    const float nb_lo = -b_hi, nb_hi = -b_lo;  // closest approach -(d.w)/|d|^2
+    const float tc_lo = __fdiv_rd(nb_lo, nb_lo < 0.0f ? a_lo : a_hi);
+    const float tc_hi = __fdiv_ru(nb_hi, nb_hi > 0.0f ? a_lo : a_hi);
+    const float e = __fsub_rd(tc_lo, half), x = __fadd_ru(tc_hi, half);
+    if (t < e) {
+      lim = fminf(lim, e);
+    } else if (!(t > x)) {  // may be inside now (or NaN)
+      inside = true;
+      recheck = fminf(recheck, x);
+    }
   }
-  return lim >= 3.4028234663852886e38 ? kMaxFloat : __double2float_rd(lim);
+  if (inside) return -1.0f;
+  recheck = -1.0f;
+  return lim;
 }
 
 // Grid coordinate (position + half grid size, object-local) of the ray at t,
@@ -484,6 +528,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
   float t = 0, prev_t = 0, prev_dist = kMaxFloat, tmax = 0;
   float box_t = -1.0f;  // empty-space path: positions up to here sample the EMPTY value
   float far_t = -1.0f;  // multi-object empty-space path: positions up to here lie outside every ball
+  float far_recheck = -1.0f;  // multi-object empty-space path: no ball check before this t
   uint32_t near = 0, step = 0;
   bool exhausted = false;
 
@@ -560,7 +605,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
               near = 0;
               step = 0;
               box_t = -1.0f;
-              if (MULTI_EMPTY) far_t = -1.0f;
+              if (MULTI_EMPTY) far_t = far_recheck = -1.0f;
               prev_dist = kMaxFloat;
               cs.hit = cs.bisected = cs.mat_ok = false;
               if (mode == RKF_TRACE_SHADOW) {
@@ -606,11 +651,16 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
         const float near_thr = sh ? -1.0f : p.near_surface_threshold;
         const float min_step = sh ? 0.005f : p.min_step;
         const bool clean = kp.empty_lo >= brk && kp.empty_lo >= near_thr && kp.empty_lo >= min_step;
-        if (t > box_t && prev_dist >= kp.probe_min) {
+        // a ray that may be inside a ball takes full steps until it may have left
+        if (t > box_t && prev_dist >= kp.probe_min && (!MULTI_EMPTY || t > far_recheck)) {
           box_t = probe_empty(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, t);
           const float cube_t = box_t;
-          if (MULTI_EMPTY) {  // only positions outside every ball sample the EMPTY value
-            if (t <= box_t) far_t = far_limit(kp.far, kp.n_far, ox, oy, oz, dx, dy, dz, tmax, t);
+          if (MULTI_EMPTY) {
+            // only positions outside every ball sample the EMPTY value.  far_t
+            // (the first entry into a ball ahead) stays valid until the ray
+            // passes it: balls ahead stay ahead, balls behind stay behind.
+            if (t <= box_t && t > far_t)
+              far_t = far_limit(kp.far, kp.n_far, ox, oy, oz, dx, dy, dz, tmax, t, far_recheck);
             box_t = fminf(box_t, far_t);
           }
           if (t <= box_t && clean && kp.settle_links && step < max_step && near < max_near) {
