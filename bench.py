@@ -396,7 +396,7 @@ def run_batching(ctx, spec, prims, p, args, stream):
             "secondary_ray_slots": wl["n_secondary_slots"],
             "tuning": {"tile": [tu.tile_w, tu.tile_h], "compact_interval": tu.compact_interval,
                        "step_budget": tu.step_budget, "refill_idle": tu.refill_idle,
-                       "probe_in_run": tu.probe_in_run,
+                       "probe_in_run": tu.probe_in_run, "no_empty_path": tu.no_empty_path,
                        "threads_per_block": tu.threads_per_block, "tune_s": tune_s},
             "batched": {"value": val(mb), "unit": "Mrays/s", "ms": float(np.mean(mb)), "launches": 1},
             "batched_graph": {"value": val(mg), "unit": "Mrays/s", "ms": float(np.mean(mg)), "launches": 1},

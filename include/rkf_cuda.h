@@ -505,6 +505,11 @@ typedef struct rkf_batch_tuning {
     uint32_t probe_in_run;       /* 1: a lane whose EMPTY cube ends probes   */
                                  /* the next one inside the run (0: at the   */
                                  /* run's end, with the warp's other lanes)  */
+    uint32_t no_empty_path;      /* 1: march every step through the full     */
+                                 /* sampler (0: EMPTY runs wherever the      */
+                                 /* scene allows them).  rkf_march,          */
+                                 /* rkf_march_batch and rkf_trace_rays only; */
+                                 /* the outputs are the same either way      */
 } rkf_batch_tuning;
 
 /* Run every view and ray batch in one persistent work-stealing launch.

@@ -144,7 +144,7 @@ class rkf_batch_tuning(C.Structure):
     _fields_ = [("tile_w", C.c_uint32), ("tile_h", C.c_uint32), ("step_budget", C.c_uint32),
                 ("compact_interval", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("threads_per_block", C.c_uint32), ("refill_idle", C.c_uint32),
-                ("probe_in_run", C.c_uint32)]
+                ("probe_in_run", C.c_uint32), ("no_empty_path", C.c_uint32)]
 
 
 class rkf_request(C.Structure):

@@ -1,15 +1,16 @@
 // autotune.cu — pick the persistent march's launch tuning for a workload.
 //
-// The batched march has six knobs that change speed but never results:
+// The batched march has seven knobs that change speed but never results:
 // the ray-tile shape that orders a view's work ids (the spatial coherence of
 // the rays a warp holds), the compaction interval (march iterations between
 // lane refills), the step budget (empty-space steps a lane runs before its
 // warp re-converges), the refill threshold (idle lanes that make a warp
 // refill), where a lane probes its next EMPTY cube (inside a run or between
-// runs) and the block size.  rkf_autotune times candidates on the caller's
+// runs), the block size and whether it runs EMPTY runs at all.  rkf_autotune times candidates on the caller's
 // sample of the work with CUDA events: every tile x interval x block size at
 // the default budget and threshold, then every budget, then every threshold,
-// then the other probe placement, each at the best so far.
+// then the other probe placement, then the march without EMPTY runs, each
+// at the best so far.
 // The fastest is kept in the context, where rkf_march and rkf_march_batch
 // use it.
 #include <cfloat>
@@ -66,7 +67,7 @@ extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t
   for (const auto& tl : tiles)
     for (uint32_t iv : intervals)
       for (uint32_t th : threads)
-        if (st == RKF_OK) trial(rkf_batch_tuning{tl[0], tl[1], 32, iv, 0, th, 32, 0});
+        if (st == RKF_OK) trial(rkf_batch_tuning{tl[0], tl[1], 32, iv, 0, th, 32, 0, 0});
   const rkf_batch_tuning base = best;
   for (uint32_t b : budgets) {
     if (st != RKF_OK) break;
@@ -84,6 +85,13 @@ extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t
   if (st == RKF_OK) {
     rkf_batch_tuning tu = best;
     tu.probe_in_run = 1;
+    trial(tu);
+  }
+  // where EMPTY runs do not pay (a camera outside a dense grid: short runs,
+  // probes that mostly fail), the full sampler alone is faster
+  if (st == RKF_OK) {
+    rkf_batch_tuning tu = best;
+    tu.no_empty_path = 1;
     trial(tu);
   }
   cudaEventDestroy(e0);

@@ -392,7 +392,7 @@ rkf_status rkf_create(const rkf_config* cfg, rkf_ctx** out) {
   }
   c->free_slots.resize(cap);
   for (size_t i = 0; i < cap; ++i) c->free_slots[i] = static_cast<uint32_t>(cap - 1 - i);
-  c->tuning = rkf_batch_tuning{4, 8, 32, 64, 0, 256, 32, 0};
+  c->tuning = rkf_batch_tuning{4, 8, 32, 64, 0, 256, 32, 0, 0};
   *out = reinterpret_cast<rkf_ctx*>(c.release());
   return RKF_OK;
 }

@@ -1247,7 +1247,11 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   std::vector<Segment> tiled_segs;
   TiledDev td;
   std::memset(&td, 0, sizeof(td));
-  const int objs = object_set(c);
+  int objs = object_set(c);
+  if (tu.no_empty_path) {  // the same outputs through the full sampler only
+    if (objs == detail::OBJ_SINGLE_EMPTY) objs = detail::OBJ_SINGLE;
+    if (objs == detail::OBJ_MULTI_EMPTY) objs = detail::OBJ_MULTI;
+  }
   if (tiled) {
     tiled_segs = segs_host;
     rkf_status s2 = prepare_tiled(c, tiled_segs, st, &td);

@@ -7,7 +7,10 @@ output stays bit-exact against the oracle: views, and ray casts in the three
 modes (closest, any hit, soft shadow), with analytic objects outside the
 grid, just beyond it and inside it, rotated and non-uniformly scaled, and the
 voxelized object not first in the list.  Scenes the path does not cover (a
-plane; the tiled strategy) march the plain multi-object kernel."""
+plane; the tiled strategy) march the plain multi-object kernel.  A tuning without the empty path marches the
+full sampler only, with the same outputs, and the autotuner may pick it."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -175,3 +178,36 @@ def test_scenes_outside_the_path_march_the_plain_kernel(oracle, small_scene):
             assert_bits_equal(got[k], ref[k], f"tiled: {k}")
     finally:
         ctx.close()
+
+
+def test_tuning_without_the_empty_path(oracle, small_scene):
+    from rkifield_b200 import _abi as abi, cudart
+    v = small_scene["vox"]
+    w, h = 160, 120
+    cam = _camera(5, w, h)
+    p = _params(0)
+    for objs, plain in (([small_scene["obj"]], 1), (_scene_objects(small_scene), VARIANT_MULTI)):
+        sc = oracle.Scene(objs, pool_words=v.words, brick_maps=v.map)
+        ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+        ctx = _context(small_scene, objs)
+        try:
+            g = cudart.device_gbuffer(w * h, reference_planes=True)
+            vw = (abi.rkf_view * 1)()
+            vw[0].camera = cam
+            vw[0].width, vw[0].height = w, h
+            for k, a in g.items():
+                setattr(vw[0].out, k, a.ptr)
+            vw[0].out.mem = abi.RKF_MEM_DEVICE
+            tu = abi.rkf_batch_tuning(4, 8, 32, 64, 0, 256, 32, 0, 1)
+            abi.check(ctx.lib.rkf_march_batch(ctx.h, vw, 1, None, 0, C.byref(p), C.byref(tu)), "rkf_march_batch")
+            assert ctx.lib.rkf_testing_last_variant(ctx.h) == plain
+            for k, a in g.items():
+                assert_bits_equal(a.download(), ref[k], f"{len(objs)} objects, no empty path: {k}")
+            out = abi.rkf_batch_tuning()
+            abi.check(ctx.lib.rkf_autotune(ctx.h, vw, 1, None, 0, C.byref(p), C.byref(out)), "rkf_autotune")
+            assert out.no_empty_path in (0, 1)
+            got = ctx.march(cam, p, w, h, reference_planes=True)  # with the tuning the context keeps
+            for k in PLANES:
+                assert_bits_equal(got[k], ref[k], f"{len(objs)} objects, autotuned: {k}")
+        finally:
+            ctx.close()
