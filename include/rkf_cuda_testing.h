@@ -43,6 +43,14 @@ RKF_API rkf_status rkf_testing_export_coarse(rkf_ctx* ctx, float origin[3], uint
  * several objects on the multi-object empty-space path; -1 before the first. */
 RKF_API int rkf_testing_last_variant(rkf_ctx* ctx);
 
+/* The multi-object empty-space path's ball of an analytic object, for EMPTY
+ * values up to empty_hi: out = {centre x, y, z, a, b}, radius a + b*P where P
+ * bounds |o| + |d| |tmax| of a ray.  Every value the object takes outside the
+ * ball exceeds empty_hi.  Host only (no device is touched).  1 when the
+ * object has a ball; 0 for a plane, a singular or ill-conditioned
+ * transform, a non-positive scale or non-finite parameters. */
+RKF_API int rkf_testing_far_ball(const rkf_gpu_object* obj, float empty_hi, float out[5]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -247,6 +247,7 @@ SIGNATURES = {
     "rkf_testing_set_host_bands": (None, [C.c_int]),
     "rkf_testing_export_coarse": (_I, [_P, _P, _P, _P, C.POINTER(C.c_uint64)]),
     "rkf_testing_last_variant": (C.c_int, [_P]),
+    "rkf_testing_far_ball": (C.c_int, [_P, C.c_float, _P]),
     "rkf_world_relative": (None, [C.POINTER(rkf_world_pos), C.POINTER(rkf_world_pos),
                                   C.POINTER(C.c_double), C.POINTER(C.c_float)]),
 }
