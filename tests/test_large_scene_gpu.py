@@ -106,3 +106,49 @@ def test_large_view_tiled_rows_bit_exact(oracle, large, large_oracle):
         ref = oracle.march(large_oracle, cam, p, W, H, rows=(r, r + 1), with_reference_planes=True)
         for k in PLANES:
             assert_bits_equal(got[k].reshape(H, -1)[r], ref[k].reshape(1, -1)[0], f"tiled row {r} {k}")
+
+
+def test_large_view_with_analytic_objects_rows_bit_exact(oracle, large):
+    """The multi-object empty-space path at full size: analytic objects in
+    front of the camera (spheres, a rotated and scaled box) and one far away,
+    beside the voxelized object; EMPTY runs and settling chains stop at each
+    object's ball.  Sampled rows bit-exact against the oracle reading the same
+    planes and index.  The scene is restored afterwards."""
+    from test_multi_empty_gpu import _rotation, _transformed
+    from test_tiled_gpu import _analytic
+    ctx, spec, cam, p = large
+    vox = ctx.object(0)
+    pos = np.array(cam.position[:3], np.float64)
+    fwd = np.array(cam.forward[:3], np.float64)
+    right = np.array(cam.right[:3], np.float64)
+    up = np.array(cam.up[:3], np.float64)
+    fwd, right, up = (v / np.linalg.norm(v) for v in (fwd, right, up))
+    props = []
+    for i, (dist, x, y, r) in enumerate([(12, -3, 1, 1.0), (25, 4, -2, 2.0), (40, 0, 0, 3.0), (60, -10, 5, 2.5),
+                                         (90, 12, -6, 4.0)]):
+        c = pos + fwd * dist + right * x + up * y
+        props.append(_analytic(0, tuple(float(v) for v in c), (r,), (r, r, r), 5, 10 + i))
+    c = pos + fwd * 30 + right * 8
+    props.append(_transformed(1, tuple(float(v) for v in c), (2.0, 1.0, 1.5), _rotation((1, 2, 3), 0.7),
+                              (1.5, 0.7, 1.2), 7, 20))
+    props.append(_analytic(0, (0.0, 0.0, 500.0), (1.0,), (1.0, 1.0, 1.0), 5, 21))
+    try:
+        ctx.update_objects([vox] + props, [0] + [-1] * len(props))
+        n = ctx.info()["pool_bricks_used"]
+        pl = ctx.export_planes(0, n)
+        idx = ctx.export_index()
+        objs = [ctx.object(i) for i in range(ctx.info()["num_objects"])]
+        sc = oracle.Scene(objs, top=idx["top"], leaves=idx["leaves"], obj_top_info=idx["obj_top_info"],
+                          dist_f16=pl["dist"], mat_plane=pl["mat"], blend_plane=pl["blend"])
+        got = ctx.march(cam, p, W, H, reference_planes=True)
+        assert ctx.lib.rkf_testing_last_variant(ctx.h) == 4
+        prop_hits = 0
+        for r in (0, 389, 480, 540, 541, 777, 1079):
+            ref = oracle.march(sc, cam, p, W, H, rows=(r, r + 1), with_reference_planes=True)
+            for k in PLANES:
+                assert_bits_equal(got[k].reshape(H, -1)[r], ref[k].reshape(1, -1)[0], f"with objects, row {r} {k}")
+            hit = (ref["flags"] & 1) != 0
+            prop_hits += int((((ref["packed_material"][hit] >> 24) & 0xFF) >= 10).sum())
+        assert prop_hits > 0, "the sampled rows should see the analytic objects"
+    finally:
+        ctx.update_objects([vox])
