@@ -107,7 +107,7 @@ rkf_status rkf_batch_graph_create(rkf_ctx* ctx, const rkf_view* views, uint32_t 
     e = cudaMemcpyAsync(dev_segs, g->pinned, sb, cudaMemcpyHostToDevice, cap);
     if (e == cudaSuccess)
       st = launch_persistent_scratch(c, g->segs.data(), static_cast<uint32_t>(g->segs.size()), first, p, tu, cap,
-                                     dev_segs, counter, true);
+                                     dev_segs, counter, true, true);
     const cudaError_t e2 = cudaStreamEndCapture(cap, &g->graph);
     if (e == cudaSuccess) e = e2;
   }

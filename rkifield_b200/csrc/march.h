@@ -50,10 +50,13 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs, uint64_t 
 // in caller-provided device memory (it allocates nothing).  segs_uploaded:
 // the caller has already queued the copy of the table into dev_segs on st
 // (from page-locked memory, so that enqueueing never waits on the stream).
+// multi_empty: a scene of one voxelized object beside analytic objects
+// marches the multi-object empty-space variant (else the plain multi-object
+// kernel).
 rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t nseg, uint64_t total,
                                      const rkf_march_params* p, const rkf_batch_tuning& tu,
                                      cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter,
-                                     bool segs_uploaded = false);
+                                     bool segs_uploaded = false, bool multi_empty = false);
 rkf_status launch_trace_plain(Ctx* c, const float* o, const float* d, const float* tmax, uint32_t n,
                               uint32_t mode, const rkf_march_params* p, const rkf_hits& out,
                               cudaStream_t st);

@@ -1357,7 +1357,7 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
 rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t nseg, uint64_t total,
                                      const rkf_march_params* p, const rkf_batch_tuning& tu,
                                      cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter,
-                                     bool segs_uploaded) {
+                                     bool segs_uploaded, bool multi_empty) {
   if (p->strategy != RKF_STRATEGY_BRUTE)
     return fail(RKF_UNSUPPORTED, "march: this launch path runs the brute strategy only");
   if (c->obj_count() > kMaxObjectsFast)
@@ -1379,25 +1379,29 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
   kp.counter = dev_counter;
   kp.p = *p;
   kp.p.scene.num_objects = c->obj_count();
-  // this launch path keeps the variants it had: several objects march the
-  // plain multi-object kernel
+  // without multi_empty, several objects march the plain multi-object kernel
   int obj = object_set(c);
-  if (obj == detail::OBJ_MULTI_EMPTY) obj = detail::OBJ_MULTI;
-  kp.probe_min = obj == detail::OBJ_SINGLE_EMPTY ? 0.99f * kp.objs[0].be * kp.objs[0].min_scale : kMaxFloat;
+  if (obj == detail::OBJ_MULTI_EMPTY && !multi_empty) obj = detail::OBJ_MULTI;
+  const bool memp = obj == detail::OBJ_MULTI_EMPTY;
+  if (memp) {
+    uint32_t vi = 0;
+    multi_empty_scene(c, &vi, kp.far, &kp.n_far);
+    kp.vox = c->objdev_host[vi];
+  }
+  const ObjDev& e0 = memp ? kp.vox : kp.objs[0];  // the object of the empty-space path
+  const bool empty = obj == detail::OBJ_SINGLE_EMPTY || memp;
+  kp.probe_min = empty ? 0.99f * e0.be * e0.min_scale : kMaxFloat;
   kp.budget = tu.step_budget ? tu.step_budget : 32;
   kp.refill_active = 32u - std::min<uint32_t>(tu.refill_idle ? tu.refill_idle : 32u, 32u);
   kp.run_probe = tu.probe_in_run ? 1u : 0u;
   // mix(c, c, t) three times stays within 12 roundings of c (relative 2^-24
   // each); 0.999 leaves a wide margin
-  kp.empty_lo = obj == detail::OBJ_SINGLE_EMPTY ? 0.999f * kp.objs[0].be * kp.objs[0].min_scale : 0.0f;
+  kp.empty_lo = empty ? 0.999f * e0.be * e0.min_scale : 0.0f;
   // twelve roundings of 2^-24 stay far inside 2^-16
-  kp.empty_lo_t = kp.objs[0].be * kp.objs[0].min_scale * (1.0f - 1.52587890625e-5f);
-  kp.empty_hi = kp.objs[0].be * kp.objs[0].min_scale * (1.0f + 1.52587890625e-5f);
-  kp.settle_links = obj == detail::OBJ_SINGLE_EMPTY ? 48u : 0u;
-  kp.plain_obj = (kp.objs[0].m[12] == 0.0f && kp.objs[0].m[13] == 0.0f && kp.objs[0].m[14] == 0.0f &&
-                  kp.objs[0].min_scale == 1.0f)
-                     ? 1u
-                     : 0u;
+  kp.empty_lo_t = e0.be * e0.min_scale * (1.0f - 1.52587890625e-5f);
+  kp.empty_hi = e0.be * e0.min_scale * (1.0f + 1.52587890625e-5f);
+  kp.settle_links = empty ? 48u : 0u;
+  kp.plain_obj = (e0.m[12] == 0.0f && e0.m[13] == 0.0f && e0.m[14] == 0.0f && e0.min_scale == 1.0f) ? 1u : 0u;
   const void* fn = nullptr;
   switch (c->cfg.precision) {
     case RKF_PRECISION_F32:

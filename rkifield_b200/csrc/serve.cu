@@ -375,7 +375,7 @@ bool ServeState::launch_tick(std::vector<uint64_t>& ids) {
       }
       lst = launch_persistent_scratch(c, segs.data(), static_cast<uint32_t>(segs.size()), first, &p, c->tuning,
                                       st, dev_segs, reinterpret_cast<unsigned long long*>(arena.at(off)),
-                                      uploaded);
+                                      uploaded, true);
     } else {
       lst = fail(RKF_OOM, "serve: no arena room for the segment table");
     }

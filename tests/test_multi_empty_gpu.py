@@ -211,3 +211,72 @@ def test_tuning_without_the_empty_path(oracle, small_scene):
                 assert_bits_equal(got[k], ref[k], f"{len(objs)} objects, autotuned: {k}")
         finally:
             ctx.close()
+
+
+def test_graph_marches_the_multi_object_path(oracle, small_scene):
+    """A batch graph captured over the multi-object scene: its launch writes
+    the oracle's planes."""
+    from rkifield_b200 import _abi as abi, cudart
+    v = small_scene["vox"]
+    objs = _scene_objects(small_scene)
+    sc = oracle.Scene(objs, pool_words=v.words, brick_maps=v.map)
+    ctx = _context(small_scene, objs)
+    graph = C.c_void_p()
+    try:
+        w, h = 160, 120
+        cam = _camera(8, w, h)
+        p = _params(0)
+        ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+        g = cudart.device_gbuffer(w * h, reference_planes=True)
+        vw = (abi.rkf_view * 1)()
+        vw[0].camera = cam
+        vw[0].width, vw[0].height = w, h
+        for k, a in g.items():
+            setattr(vw[0].out, k, a.ptr)
+        vw[0].out.mem = abi.RKF_MEM_DEVICE
+        abi.check(ctx.lib.rkf_batch_graph_create(ctx.h, vw, 1, None, 0, C.byref(p), None, C.byref(graph)),
+                  "rkf_batch_graph_create")
+        abi.check(ctx.lib.rkf_batch_graph_launch(graph, None), "rkf_batch_graph_launch")
+        cudart.synchronize()
+        assert int((ref["flags"] & 1).sum()) > 200
+        for k, a in g.items():
+            assert_bits_equal(a.download(), ref[k], f"graph: {k}")
+    finally:
+        if graph.value:
+            ctx.lib.rkf_batch_graph_destroy(graph)
+        ctx.close()
+
+
+def test_serving_marches_the_multi_object_path(oracle, small_scene):
+    """Renders and ray batches served by the resident loop over the
+    multi-object scene equal the oracle's."""
+    from rkifield_b200 import engine, scenes
+    from rkifield_b200.engine import Server
+    v = small_scene["vox"]
+    objs = _scene_objects(small_scene)
+    sc = oracle.Scene(objs, pool_words=v.words, brick_maps=v.map)
+    ctx = _context(small_scene, objs)
+    p = scenes.march_params(small_scene["spec"])
+    p.scene.max_distance = 200.0
+    srv = Server(ctx, p)
+    try:
+        w, h = 160, 120
+        cam = _camera(3, w, h)
+        o, d, tmax = _rays(5000, seed=77, box=24.0)
+        out_r = engine.render_out(w * h)
+        out_b = engine.rays_out(5000, 0)
+        tickets = [srv.submit_render(cam, w, h, out_r), srv.submit_rays(o, d, tmax, 0, out_b)]
+        for t in tickets:
+            res = srv.poll(t, 10_000_000)
+            assert res is not None and res["status"] == 0, res
+        ref = oracle.march(sc, cam, p, w, h)
+        for k in out_r:
+            if k in ref:
+                assert_bits_equal(out_r[k], ref[k], f"served render: {k}")
+        ref_b = oracle.trace(sc, o.ravel(), d.ravel(), tmax, 0, p)
+        for k in out_b:
+            assert_bits_equal(out_b[k], ref_b[k], f"served rays: {k}")
+        assert int((ref["flags"] & 1).sum()) > 200
+    finally:
+        srv.stop()
+        ctx.close()
