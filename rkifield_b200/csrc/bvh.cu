@@ -180,6 +180,8 @@ rkf_status rkf_bvh_import(rkf_ctx* ctx, const rkf_bvh_node* nodes, uint32_t n) {
     c->bvh_next.release();
     c->bvh_n = 0;
     c->bvh_one_leaf0 = false;
+    c->bvh_host.clear();
+    c->bvh_next_host.clear();
     return RKF_OK;
   }
   const std::vector<uint32_t> next = walk_links(nodes, n);
@@ -195,6 +197,8 @@ rkf_status rkf_bvh_import(rkf_ctx* ctx, const rkf_bvh_node* nodes, uint32_t n) {
   std::swap(c->bvh_next.bytes, nn.bytes);
   c->bvh_n = n;
   c->bvh_one_leaf0 = n == 1 && nodes[0].left == RKF_BVH_INVALID && nodes[0].right_or_object == 0;
+  c->bvh_host.assign(nodes, nodes + n);
+  c->bvh_next_host = next;
   return RKF_OK;
 }
 

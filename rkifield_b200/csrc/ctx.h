@@ -109,6 +109,8 @@ struct Ctx {
   DevBuf bvh, bvh_next;
   uint32_t bvh_n = 0;
   bool bvh_one_leaf0 = false;  // the tree is one leaf naming object 0
+  std::vector<rkf_bvh_node> bvh_host;  // the imported tree, root first
+  std::vector<uint32_t> bvh_next_host;  // its walk links (bvh_next)
 
   // objects
   std::vector<rkf_gpu_object> objects;

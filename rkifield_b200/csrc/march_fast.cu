@@ -760,7 +760,7 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                 }
               }
             }
-          } else if (!EMPTY_PATH && kp.use_bvh) {
+          } else if ((!EMPTY_PATH || MULTI_EMPTY) && kp.use_bvh) {
             best = eval_bvh<PREC>(s, sh_objs, kp.bvh, kp.bvh_next, nobj, wx, wy, wz, best_un, best_i, lc);
           } else {
             best = eval_min<PREC, SINGLE>(s, sh_objs, 0, nobj, wx, wy, wz, best_un, best_i, lc);
@@ -1226,6 +1226,44 @@ bool multi_empty_scene(const Ctx* c, uint32_t* vi_out, detail::FarBall* far, uin
   return true;
 }
 
+// The BVH walk (eval_bvh) evaluates object vi at every position inside its
+// grid (the clamp range every EMPTY cube lies in): some leaf naming vi has
+// every node on its path from the root containing that box, and every
+// internal node on it descends (the shader's stack had room for its
+// children: bit 31 of its walk link).  The walk skips a node only when its
+// box distance exceeds the best value so far; inside such nodes that
+// distance is 0, and along EMPTY runs outside every ball no value is
+// negative, so the leaf is reached and the walk's minimum is the brute one.
+bool bvh_reaches(const Ctx* c, uint32_t vi) {
+  const std::vector<rkf_bvh_node>& nd = c->bvh_host;
+  const std::vector<uint32_t>& link = c->bvh_next_host;
+  if (nd.empty() || link.size() != nd.size()) return false;
+  const ObjDev& o = c->objdev_host[vi];
+  float lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    const float base = -o.half_gs[a] - o.m[12 + a];
+    lo[a] = 0.5f * o.vs + base;
+    hi[a] = (static_cast<float>(o.tv[a] - 1) + 0.5f) * o.vs + base;
+  }
+  std::vector<uint32_t> stack{0u};
+  while (!stack.empty()) {
+    const uint32_t i = stack.back();
+    stack.pop_back();
+    if (i >= nd.size()) continue;
+    const rkf_bvh_node& b = nd[i];
+    bool holds = true;
+    for (int a = 0; a < 3; ++a) holds = holds && b.aabb_min[a] <= lo[a] && b.aabb_max[a] >= hi[a];
+    if (!holds) continue;
+    if (b.left == RKF_BVH_INVALID) {
+      if (b.right_or_object == vi) return true;
+    } else if (link[i] >> 31) {
+      stack.push_back(b.left);
+      stack.push_back(b.right_or_object);
+    }
+  }
+  return false;
+}
+
 // Which kernel variant a launch over this context's objects uses.
 int object_set(const Ctx* c) {
   if (c->obj_count() != 1)
@@ -1294,15 +1332,13 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
     obj = detail::OBJ_SINGLE_EMPTY_TILED;
     kp.s.empty_dist = c->tiled_empty_dist.as<uint8_t>();
   }
-  // the multi-object empty-space path marches the brute strategy only
-  if (objs == detail::OBJ_MULTI_EMPTY && (tiled || walk)) obj = detail::OBJ_MULTI;
-  if (obj == detail::OBJ_MULTI_EMPTY) {
-    uint32_t vi = 0;
-    multi_empty_scene(c, &vi, kp.far, &kp.n_far);
-    kp.vox = c->objdev_host[vi];
-  } else {
-    kp.vox = kp.objs[0];
-  }
+  // the multi-object empty-space path marches the brute strategy, and the
+  // BVH strategy on trees whose walk reaches the voxelized object everywhere
+  // in its grid
+  uint32_t vi = 0;
+  if (objs == detail::OBJ_MULTI_EMPTY) multi_empty_scene(c, &vi, kp.far, &kp.n_far);
+  if (objs == detail::OBJ_MULTI_EMPTY && (tiled || (walk && !bvh_reaches(c, vi)))) obj = detail::OBJ_MULTI;
+  kp.vox = obj == detail::OBJ_MULTI_EMPTY ? c->objdev_host[vi] : kp.objs[0];
   const bool empty = obj == detail::OBJ_SINGLE_EMPTY || obj == detail::OBJ_SINGLE_EMPTY_TILED ||
                      obj == detail::OBJ_MULTI_EMPTY;
   kp.td = td;

@@ -280,3 +280,44 @@ def test_serving_marches_the_multi_object_path(oracle, small_scene):
     finally:
         srv.stop()
         ctx.close()
+
+
+def test_bvh_strategy_marches_the_multi_object_path(oracle, small_scene):
+    """The BVH strategy over the runtime's tree (one leaf per object AABB):
+    its walk reaches the voxelized object everywhere in its grid, so the
+    multi-object empty-space variant marches it, bit-exact against the
+    oracle's walk; a tree whose leaf for the voxelized object does not hold
+    its grid marches the plain kernel, also bit-exact."""
+    from rkifield_b200 import _abi as abi, engine, scenes
+    v = small_scene["vox"]
+    objs = _scene_objects(small_scene)
+    nodes = engine.object_bvh(objs)
+    shrunk = (abi.rkf_bvh_node * len(nodes))(*nodes)
+    leaf = [i for i, n in enumerate(shrunk) if n.left == abi.BVH_INVALID and n.right_or_object == 1]
+    assert len(leaf) == 1
+    shrunk[leaf[0]].aabb_min[0] += 1.0
+    ctx = _context(small_scene, objs)
+    try:
+        w, h = 200, 136
+        p = _params(abi.RKF_STRATEGY_BVH)
+        for tree, variant in ((nodes, VARIANT_MULTI_EMPTY), (shrunk, VARIANT_MULTI)):
+            ctx.upload_bvh(tree)
+            sc = oracle.Scene(objs, pool_words=v.words, brick_maps=v.map, bvh=tree)
+            for seed in (3, 5):
+                cam = _camera(seed, w, h)
+                ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+                got = ctx.march(cam, p, w, h, reference_planes=True)
+                assert ctx.lib.rkf_testing_last_variant(ctx.h) == variant
+                assert int((ref["flags"] & 1).sum()) > 500
+                for k in PLANES:
+                    assert_bits_equal(got[k], ref[k], f"variant {variant} seed {seed}: {k}")
+            o, d, tmax = _rays(8000, seed=91, box=24.0)
+            pr = scenes.march_params(small_scene["spec"])
+            pr.strategy = abi.RKF_STRATEGY_BVH
+            ref = oracle.trace(sc, o.ravel(), d.ravel(), tmax, 0, pr)
+            got = ctx.trace(o, d, tmax, 0, pr)
+            assert ctx.lib.rkf_testing_last_variant(ctx.h) == variant
+            for k in ("t", "flags", "normal", "slot", "material"):
+                assert_bits_equal(got[k], ref[k], f"variant {variant} rays: {k}")
+    finally:
+        ctx.close()
