@@ -40,7 +40,8 @@ RKF_API rkf_status rkf_testing_export_coarse(rkf_ctx* ctx, float origin[3], uint
 /* Kernel variant of the context's last march launch through rkf_march,
  * rkf_march_rays or rkf_march_batch: 0 several objects, 1 one object, 2 one
  * object on the empty-space path, 3 the same under the tiled strategy, 4
- * several objects on the multi-object empty-space path; -1 before the first. */
+ * several objects on the multi-object empty-space path, 5 the same under the
+ * tiled strategy; -1 before the first. */
 RKF_API int rkf_testing_last_variant(rkf_ctx* ctx);
 
 /* The multi-object empty-space path's ball of an analytic object, for EMPTY

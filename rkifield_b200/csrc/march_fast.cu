@@ -47,7 +47,10 @@ struct ColdState {
   float lo, hi, mat_t, gpos, shadow;
   uint32_t tile_base, tile_count;  // tiled strategy: the ray's object list (kNoTiles: every object)
   bool hit, bisected, mat_ok;
-  uint32_t pad_;  // an odd number of words per lane: a warp's accesses hit 32 distinct banks
+  // multi-object tiled empty-space path: the ray's object list holds the
+  // voxelized object.  (Also makes an odd number of words per lane: a warp's
+  // accesses hit 32 distinct banks.)
+  uint32_t vox_listed;
 };
 static_assert(sizeof(ColdState) % 8 == 4, "ColdState must span an odd number of 32-bit words");
 
@@ -96,6 +99,7 @@ struct KParams {
   ObjDev vox;                     // multi-object empty-space path: the voxelized object
   FarBall far[kMaxObjectsFast];   // multi-object empty-space path: the analytic objects' balls
   uint32_t n_far;
+  uint32_t vox_i;                 // multi-object empty-space path: the voxelized object's index
 };
 
 // The candidate loop of ray_march_bvh (ray_march.wgsl:672-721): a stack walk
@@ -162,7 +166,17 @@ __device__ __forceinline__ float eval_bvh(const SceneDev& s, const ObjDev* objs,
 // OBJ_MULTI_EMPTY: one object that qualifies for the empty-space path plus
 // analytic objects that each fit a ball (FarBall) and objects of no type; its
 // EMPTY runs and settling chains stay outside every ball.
-enum : int { OBJ_MULTI = 0, OBJ_SINGLE = 1, OBJ_SINGLE_EMPTY = 2, OBJ_SINGLE_EMPTY_TILED = 3, OBJ_MULTI_EMPTY = 4 };
+// OBJ_MULTI_EMPTY_TILED: the same under the tiled strategy (EMPTY runs on
+// the tiled empty-space field, for rays whose object list holds the
+// voxelized object; tiled full steps elsewhere).
+enum : int {
+  OBJ_MULTI = 0,
+  OBJ_SINGLE = 1,
+  OBJ_SINGLE_EMPTY = 2,
+  OBJ_SINGLE_EMPTY_TILED = 3,
+  OBJ_MULTI_EMPTY = 4,
+  OBJ_MULTI_EMPTY_TILED = 5
+};
 
 // Interval helpers in directed rounding: each result interval contains the
 // exact result for every value of the operand intervals.
@@ -505,11 +519,12 @@ __device__ __forceinline__ uint32_t empty_run_x2(const ObjDev& o, const uint8_t*
 
 template <int PREC, int OBJ>
 __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_constant__ KParams kp) {
-  constexpr bool MULTI_EMPTY = OBJ == OBJ_MULTI_EMPTY;
+  constexpr bool MULTI_TILED = OBJ == OBJ_MULTI_EMPTY_TILED;
+  constexpr bool MULTI_EMPTY = OBJ == OBJ_MULTI_EMPTY || MULTI_TILED;
   constexpr bool SINGLE = OBJ != OBJ_MULTI && !MULTI_EMPTY;
   constexpr bool EMPTY_PATH = OBJ == OBJ_SINGLE_EMPTY || OBJ == OBJ_SINGLE_EMPTY_TILED || MULTI_EMPTY;
   // tile bookkeeping of tiled launches
-  constexpr bool TILES = OBJ != OBJ_SINGLE_EMPTY && !MULTI_EMPTY;
+  constexpr bool TILES = OBJ != OBJ_SINGLE_EMPTY && OBJ != OBJ_MULTI_EMPTY;
   const ObjDev* sh_objs = kp.objs;
   const SceneDev& s = kp.s;
   const rkf_march_params& p = kp.p;
@@ -586,10 +601,17 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                     cs.tile_base = tl * kTileObjects;
                     cs.tile_count = __ldg(kp.td.tile_cnt + tl);
                   }
+                  if (MULTI_TILED) {
+                    bool listed = cs.tile_count == kNoTiles;
+                    for (uint32_t j = 0; !listed && j < cs.tile_count; ++j)
+                      listed = __ldg(kp.td.tile_list + cs.tile_base + j) == kp.vox_i;
+                    cs.vox_listed = listed ? 1u : 0u;
+                  }
                 }
               }
             } else {
               if (TILES) cs.tile_count = kNoTiles;
+              if (MULTI_TILED) cs.vox_listed = 1u;
               cs.idx = static_cast<uint32_t>(local);
               const size_t i3 = 3 * static_cast<size_t>(cs.idx);
               ox = __ldg(sg.origins + i3);
@@ -638,7 +660,9 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
 #pragma unroll 1
     for (uint32_t k = 0; k < kp.interval; ++k) {
       bool full = true;  // take a full step (index lookups) this iteration
-      if (EMPTY_PATH && (state == ST_MARCH || state == ST_SHADOW)) {
+      // (a tiled step evaluates the ray's object list only: EMPTY runs need
+      // the voxelized object in it)
+      if (EMPTY_PATH && (state == ST_MARCH || state == ST_SHADOW) && (!MULTI_TILED || cs.vox_listed)) {
         // empty-space run: inside a cube of EMPTY blocks every sample is
         // empty_value(), so up to kp.budget steps run without the sampler
         const ObjDev& o0 = MULTI_EMPTY ? kp.vox : sh_objs[0];
@@ -1100,6 +1124,8 @@ __global__ void k_sdf_ao(SceneDev s, const float* __restrict__ pos, const float*
 template <int PREC>
 const void* persistent_fn(int obj) {
   if (obj == OBJ_MULTI_EMPTY) return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_MULTI_EMPTY>);
+  if (obj == OBJ_MULTI_EMPTY_TILED)
+    return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_MULTI_EMPTY_TILED>);
   if (obj == OBJ_SINGLE_EMPTY) return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_SINGLE_EMPTY>);
   if (obj == OBJ_SINGLE_EMPTY_TILED)
     return reinterpret_cast<const void*>(&k_march_persistent<PREC, OBJ_SINGLE_EMPTY_TILED>);
@@ -1290,11 +1316,15 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
     if (objs == detail::OBJ_SINGLE_EMPTY) objs = detail::OBJ_SINGLE;
     if (objs == detail::OBJ_MULTI_EMPTY) objs = detail::OBJ_MULTI;
   }
+  uint32_t vi = 0;  // the object of the empty-space path
+  if (objs == detail::OBJ_MULTI_EMPTY) multi_empty_scene(c, &vi, nullptr, nullptr);
   if (tiled) {
     tiled_segs = segs_host;
     rkf_status s2 = prepare_tiled(c, tiled_segs, st, &td);
     if (s2 != RKF_OK) return s2;
-    if (objs == detail::OBJ_SINGLE_EMPTY && (s2 = prepare_tiled_empty(c, st)) != RKF_OK) return s2;
+    if ((objs == detail::OBJ_SINGLE_EMPTY || objs == detail::OBJ_MULTI_EMPTY) &&
+        (s2 = prepare_tiled_empty(c, st, vi)) != RKF_OK)
+      return s2;
   }
   const std::vector<Segment>& segs_dev = tiled ? tiled_segs : segs_host;
   const size_t sb = segs_dev.size() * sizeof(Segment);
@@ -1332,15 +1362,19 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
     obj = detail::OBJ_SINGLE_EMPTY_TILED;
     kp.s.empty_dist = c->tiled_empty_dist.as<uint8_t>();
   }
-  // the multi-object empty-space path marches the brute strategy, and the
-  // BVH strategy on trees whose walk reaches the voxelized object everywhere
-  // in its grid
-  uint32_t vi = 0;
-  if (objs == detail::OBJ_MULTI_EMPTY) multi_empty_scene(c, &vi, kp.far, &kp.n_far);
-  if (objs == detail::OBJ_MULTI_EMPTY && (tiled || (walk && !bvh_reaches(c, vi)))) obj = detail::OBJ_MULTI;
-  kp.vox = obj == detail::OBJ_MULTI_EMPTY ? c->objdev_host[vi] : kp.objs[0];
-  const bool empty = obj == detail::OBJ_SINGLE_EMPTY || obj == detail::OBJ_SINGLE_EMPTY_TILED ||
-                     obj == detail::OBJ_MULTI_EMPTY;
+  // the multi-object empty-space path marches the brute and tiled
+  // strategies, and the BVH strategy on trees whose walk reaches the
+  // voxelized object everywhere in its grid
+  if (objs == detail::OBJ_MULTI_EMPTY) multi_empty_scene(c, nullptr, kp.far, &kp.n_far);
+  if (objs == detail::OBJ_MULTI_EMPTY && walk && !bvh_reaches(c, vi)) obj = detail::OBJ_MULTI;
+  if (obj == detail::OBJ_MULTI_EMPTY && tiled) {
+    obj = detail::OBJ_MULTI_EMPTY_TILED;
+    kp.s.empty_dist = c->tiled_empty_dist.as<uint8_t>();
+  }
+  const bool multi_empty = obj == detail::OBJ_MULTI_EMPTY || obj == detail::OBJ_MULTI_EMPTY_TILED;
+  kp.vox = multi_empty ? c->objdev_host[vi] : kp.objs[0];
+  kp.vox_i = vi;
+  const bool empty = obj == detail::OBJ_SINGLE_EMPTY || obj == detail::OBJ_SINGLE_EMPTY_TILED || multi_empty;
   kp.td = td;
   kp.tiled = tiled ? 1u : 0u;
   kp.bvh = walk ? c->bvh.as<rkf_bvh_node>() : nullptr;

@@ -288,11 +288,11 @@ __global__ void k_tiled_mask(const __grid_constant__ SafeArgs a) {
 
 }  // namespace detail
 
-rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st) {
+rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st, uint32_t vi) {
   if (c->tiled_epoch == c->epoch && c->tiled_empty_dist.p) return RKF_OK;
   if (c->coarse_epoch != c->epoch || !c->coarse_tex.p)
     return fail(RKF_CUDA_ERROR, "tiled march: coarse field missing for the empty-space field");
-  const ObjDev& o = c->objdev_host[0];
+  const ObjDev& o = c->objdev_host[vi];
   const uint32_t cd[3] = {c->coarse_dims[0], c->coarse_dims[1], c->coarse_dims[2]};
   const uint32_t nt = cd[0] * cd[1] * cd[2];
   DevBuf pre, masked, field;

@@ -38,7 +38,7 @@ rkf_status prepare_tiled(Ctx* c, std::vector<Segment>& segs, cudaStream_t st, Ti
 // c->tiled_empty_dist when the scene epoch changed; needs the coarse field of
 // the same epoch.  Enqueued on st and synchronised.
 constexpr float kCoarseSafe = 0.49f;  // below COARSE_NEAR_THRESHOLD with room for mix() rounding
-rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st);
+rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st, uint32_t vi = 0);
 
 // sample_coarse_field (ray_march.wgsl:228-235) at a camera-relative position:
 // 0 outside the field, else a linear, clamp-to-edge read of the texture, with

@@ -150,5 +150,15 @@ def test_large_view_with_analytic_objects_rows_bit_exact(oracle, large):
             hit = (ref["flags"] & 1) != 0
             prop_hits += int((((ref["packed_material"][hit] >> 24) & 0xFF) >= 10).sum())
         assert prop_hits > 0, "the sampled rows should see the analytic objects"
+        # the same under the tiled strategy (EMPTY runs on the tiled empty-space field)
+        from rkifield_b200 import _abi as abi, scenes
+        pt = scenes.march_params(spec)
+        pt.strategy = abi.RKF_STRATEGY_TILED
+        got = ctx.march(cam, pt, W, H, reference_planes=True)
+        assert ctx.lib.rkf_testing_last_variant(ctx.h) == 5
+        for r in (0, 480, 541, 1079):
+            ref = oracle.march(sc, cam, pt, W, H, rows=(r, r + 1), with_reference_planes=True)
+            for k in PLANES:
+                assert_bits_equal(got[k].reshape(H, -1)[r], ref[k].reshape(1, -1)[0], f"tiled, row {r} {k}")
     finally:
         ctx.update_objects([vox])

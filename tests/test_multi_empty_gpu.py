@@ -6,8 +6,9 @@ minimum over the scene there is the voxelized object's EMPTY value, and every
 output stays bit-exact against the oracle: views, and ray casts in the three
 modes (closest, any hit, soft shadow), with analytic objects outside the
 grid, just beyond it and inside it, rotated and non-uniformly scaled, and the
-voxelized object not first in the list.  Scenes the path does not cover (a
-plane; the tiled strategy) march the plain multi-object kernel.  A tuning without the empty path marches the
+voxelized object not first in the list, under the brute, tiled and BVH
+strategies.  Scenes the path does not cover (a plane) march the plain
+multi-object kernel.  A tuning without the empty path marches the
 full sampler only, with the same outputs, and the autotuner may pick it."""
 import ctypes as C
 
@@ -21,7 +22,7 @@ from test_trace_gpu import _rays
 pytestmark = pytest.mark.gpu
 
 
-VARIANT_MULTI, VARIANT_MULTI_EMPTY = 0, 4
+VARIANT_MULTI, VARIANT_MULTI_EMPTY, VARIANT_MULTI_EMPTY_TILED = 0, 4, 5
 
 
 def _rotation(axis, angle):
@@ -165,9 +166,7 @@ def test_scenes_outside_the_path_march_the_plain_kernel(oracle, small_scene):
             assert_bits_equal(got[k], ref[k], f"with a plane: {k}")
     finally:
         ctx.close()
-    # the tiled strategy keeps its own kernel
-    objs = _scene_objects(small_scene)
-    sc = oracle.Scene(objs, pool_words=v.words, brick_maps=v.map)
+    # the tiled strategy over a scene with a plane: the plain kernel's tiled steps
     ctx = _context(small_scene, objs)
     try:
         p = _params(abi.RKF_STRATEGY_TILED)
@@ -175,7 +174,34 @@ def test_scenes_outside_the_path_march_the_plain_kernel(oracle, small_scene):
         got = ctx.march(cam, p, w, h, reference_planes=True)
         assert ctx.lib.rkf_testing_last_variant(ctx.h) == VARIANT_MULTI
         for k in PLANES:
-            assert_bits_equal(got[k], ref[k], f"tiled: {k}")
+            assert_bits_equal(got[k], ref[k], f"tiled with a plane: {k}")
+    finally:
+        ctx.close()
+
+
+def test_tiled_strategy_marches_the_multi_object_path(oracle, small_scene):
+    """The tiled strategy (coarse skips, per-tile object lists): EMPTY runs
+    on the tiled empty-space field for rays whose tile lists the voxelized
+    object, tiled steps elsewhere; bit-exact against the oracle's tiled march
+    from afar (coarse skips active) and close to the objects."""
+    from rkifield_b200 import _abi as abi, scenes
+    v = small_scene["vox"]
+    objs = _scene_objects(small_scene)
+    sc = oracle.Scene(objs, pool_words=v.words, brick_maps=v.map)
+    ctx = _context(small_scene, objs)
+    try:
+        p = _params(abi.RKF_STRATEGY_TILED)
+        views = [(_camera(seed, 200, 136), 200, 136) for seed in (3, 5, 8)]
+        views += [(scenes.camera_uniforms(eye, target, 160, 120), 160, 120)
+                  for eye, target in (((0.0, 32.0, 18.0), (0.0, 19.5, 0.0)), ((-22.0, 6.0, 24.0), (-10.0, 2.0, 8.0)),
+                                      ((5.0, 3.0, 4.0), (20.0, -2.0, -9.0)))]
+        for i, (cam, w, h) in enumerate(views):
+            ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+            got = ctx.march(cam, p, w, h, reference_planes=True)
+            assert ctx.lib.rkf_testing_last_variant(ctx.h) == VARIANT_MULTI_EMPTY_TILED
+            assert int((ref["flags"] & 1).sum()) > 300
+            for k in PLANES:
+                assert_bits_equal(got[k], ref[k], f"tiled view {i}: {k}")
     finally:
         ctx.close()
 
