@@ -205,8 +205,10 @@ __device__ __forceinline__ void iv_sq(float lo, float hi, float& rlo, float& rhi
 // spans sqrt((rho^2 - h^2)/|d|^2) on each side.  Every quantity is an interval
 // evaluated in directed rounding, so the entry time used is a lower bound
 // and the exit time an upper bound of the exact ones.  A non-finite ray (or
-// a zero direction) makes every ball near.
-__device__ __forceinline__ float far_limit(const FarBall* __restrict__ far, uint32_t n, float ox, float oy,
+// a zero direction) makes every ball near.  Out of line: the march loop
+// calls it about once per ray, and its code would otherwise sit among the
+// loop's hot paths (measured 3% faster out of line).
+__device__ __noinline__ float far_limit(const FarBall* __restrict__ far, uint32_t n, float ox, float oy,
                                            float oz, float dx, float dy, float dz, float tmax, float t,
                                            float& recheck) {
   const float a_lo = __fadd_rd(__fadd_rd(__fmul_rd(dx, dx), __fmul_rd(dy, dy)), __fmul_rd(dz, dz));
