@@ -540,19 +540,22 @@ RKF_API rkf_status rkf_trace_rays_plain_async(rkf_ctx* ctx, const float* origins
  * the device) and callers whose framework owns every device allocation.  No
  * counterpart in the reference (its march allocates nothing per dispatch).
  *
- * Same inputs, outputs and results as rkf_march_batch (device pointers
- * only), but it allocates nothing: the launch scratch (segment table and
- * work counter) is one fixed static device array of
- * RKF_NOALLOC_MAX_SEGMENTS segments (about 15 KB, held on every device that
+ * Same inputs, outputs and results as rkf_march_batch for the brute
+ * strategy (device pointers only; the tiled and BVH strategies return
+ * RKF_UNSUPPORTED), but it allocates nothing: the launch scratch (segment
+ * table and work counter) is one fixed static device array of
+ * RKF_NOALLOC_MAX_SEGMENTS segments (about 17 KB, held on every device that
  * loads the library until the process exits).  More views plus ray batches
  * than that in one call returns RKF_INVALID_ARG.  The first call on a device
  * resolves the array's device address; make that first call before any
- * stream capture.  The work is enqueued on `stream` (a cudaStream_t, NULL =
- * the context stream) and the call returns without waiting.  Every call
- * shares the one array and the counter is cleared at the start of each
- * call, so calls that overlap on the GPU (other streams, other contexts on
- * the same device) race: order them on one stream or synchronise between
- * them. */
+ * stream capture.  The segment table travels as the parameter of a small
+ * staging kernel, so the call enqueues two kernels on `stream` (a
+ * cudaStream_t, NULL = the context stream) and returns without waiting on
+ * it.  Refusals (sizes, strategy, tuning) come before anything is enqueued.
+ * Every call shares the one array and the counter is cleared at the start
+ * of each call, so calls that overlap on the GPU (other streams, other
+ * contexts on the same device) race: order them on one stream or
+ * synchronise between them. */
 #define RKF_NOALLOC_MAX_SEGMENTS 64u
 RKF_API rkf_status rkf_march_batch_noalloc(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views,
                                            const rkf_ray_batch* batches, uint32_t n_batches,

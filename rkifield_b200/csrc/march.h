@@ -53,6 +53,9 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs, uint64_t 
 // multi_empty: a scene of one voxelized object beside analytic objects
 // marches the multi-object empty-space variant (else the plain multi-object
 // kernel).
+// The refusals of launch_persistent_scratch (strategy, object count, block
+// size), without enqueueing anything.
+rkf_status check_persistent_scratch(const Ctx* c, const rkf_march_params* p, const rkf_batch_tuning& tu);
 rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t nseg, uint64_t total,
                                      const rkf_march_params* p, const rkf_batch_tuning& tu,
                                      cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter,

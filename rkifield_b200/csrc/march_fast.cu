@@ -1426,15 +1426,25 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   return RKF_OK;
 }
 
-rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t nseg, uint64_t total,
-                                     const rkf_march_params* p, const rkf_batch_tuning& tu,
-                                     cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter,
-                                     bool segs_uploaded, bool multi_empty) {
+rkf_status check_persistent_scratch(const Ctx* c, const rkf_march_params* p, const rkf_batch_tuning& tu) {
   if (p->strategy != RKF_STRATEGY_BRUTE)
     return fail(RKF_UNSUPPORTED, "march: this launch path runs the brute strategy only");
   if (c->obj_count() > kMaxObjectsFast)
     return fail(RKF_UNSUPPORTED, "march: more objects than the persistent kernel holds");
   if (c->obj_count() == 0) return fail(RKF_INVALID_ARG, "march: the scene has no objects");
+  const uint32_t threads = tu.threads_per_block ? tu.threads_per_block : 256;
+  if (threads > 256 || threads % 32)
+    return fail(RKF_INVALID_ARG, "march: threads_per_block must be a multiple of 32 <= 256");
+  return RKF_OK;
+}
+
+rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t nseg, uint64_t total,
+                                     const rkf_march_params* p, const rkf_batch_tuning& tu,
+                                     cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter,
+                                     bool segs_uploaded, bool multi_empty) {
+  // every refusal comes before anything is enqueued on the stream
+  const rkf_status chk = check_persistent_scratch(c, p, tu);
+  if (chk != RKF_OK) return chk;
   if (!segs_uploaded)
     RKF_CUDA_TRY(cudaMemcpyAsync(dev_segs, segs_host, sizeof(Segment) * nseg, cudaMemcpyHostToDevice, st));
   RKF_CUDA_TRY(cudaMemsetAsync(dev_counter, 0, sizeof(unsigned long long), st));
@@ -1485,9 +1495,8 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
     default:
       fn = detail::persistent_fn<RKF_PRECISION_F16>(obj);
   }
-  const uint32_t threads = tu.threads_per_block ? tu.threads_per_block : 256;
-  if (threads > 256 || threads % 32)
-    return fail(RKF_INVALID_ARG, "march: threads_per_block must be a multiple of 32 <= 256");
+  c->last_variant = obj;
+  const uint32_t threads = tu.threads_per_block ? tu.threads_per_block : 256;  // checked above
   uint32_t bps = tu.blocks_per_sm;
   if (bps == 0) {
     int occ = 0;

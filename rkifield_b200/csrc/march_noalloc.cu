@@ -8,7 +8,12 @@
 // every device allocation through its own allocator, cannot call an entry
 // point that might allocate.  rkf_march_batch_noalloc does the same work
 // with that scratch in one fixed file-scope device array instead.
-#include <array>
+//
+// The segment table reaches the array through a small staging kernel that
+// takes the whole table as a kernel parameter (at most 64 segments, under
+// 17 KB): enqueueing a launch never waits on the stream, where a copy from
+// pageable host memory can, and the table's bytes travel with the launch, so
+// no host buffer has to outlive the call.
 #include <cstring>
 #include <mutex>
 
@@ -20,7 +25,7 @@ namespace {
 
 // Scratch of the allocation-free launch: the work counter, then the segment
 // table.  It occupies RKF_NOALLOC_MAX_SEGMENTS * sizeof(Segment) + 256 bytes
-// (about 15 KB) on every device that loads the library, until the process
+// (about 17 KB) on every device that loads the library, until the process
 // exits.  Every call shares it.
 struct NoAllocScratch {
   unsigned long long counter;
@@ -28,6 +33,25 @@ struct NoAllocScratch {
   Segment segs[RKF_NOALLOC_MAX_SEGMENTS];
 };
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+// The segment table of one call, passed by value to the staging kernel.
+struct NoAllocTable {
+  uint32_t nseg;
+  uint32_t pad;
+  Segment segs[RKF_NOALLOC_MAX_SEGMENTS];
+};
+static_assert(sizeof(NoAllocTable) <= 32000, "the table must fit the kernel parameter space");
+static_assert(sizeof(Segment) % 8 == 0, "segments are copied as 8-byte words");
+
+// Writes the call's segments into the scratch array and clears the work
+// counter.  One block; each thread copies 8-byte words.
+__global__ void k_noalloc_stage(const __grid_constant__ NoAllocTable tbl, NoAllocScratch* dst) {
+  const uint32_t words = tbl.nseg * static_cast<uint32_t>(sizeof(Segment) / 8);
+  const auto* src = reinterpret_cast<const unsigned long long*>(tbl.segs);
+  auto* out = reinterpret_cast<unsigned long long*>(dst->segs);
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) out[i] = src[i];
+  if (threadIdx.x == 0) dst->counter = 0ull;
+}
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
@@ -74,7 +98,12 @@ extern "C" rkf_status rkf_march_batch_noalloc(rkf_ctx* ctx, const rkf_view* view
   const rkf_batch_tuning tu = tuning ? *tuning : c->tuning;
   if (tu.tile_w == 0 || tu.tile_h == 0 || tu.tile_w * tu.tile_h > 4096)
     return fail(RKF_INVALID_ARG, "rkf_march_batch_noalloc: bad tile shape");
-  std::array<Segment, RKF_NOALLOC_MAX_SEGMENTS> segs;
+  // every refusal of the launch itself, before anything touches the shared
+  // scratch (a refused call must not overwrite a table another call uses)
+  st = check_persistent_scratch(c, p, tu);
+  if (st != RKF_OK) return st;
+  NoAllocTable tbl;
+  std::memset(&tbl, 0, sizeof(tbl));
   uint32_t nseg = 0;
   uint64_t first = 0;
   for (uint32_t i = 0; i < n_views; ++i) {
@@ -85,7 +114,7 @@ extern "C" rkf_status rkf_march_batch_noalloc(rkf_ctx* ctx, const rkf_view* view
     Segment sg = view_segment(&v.camera, v.width, v.height, tu.tile_w, tu.tile_h, v.out);
     sg.first = first;
     first += sg.n_ids;
-    segs[nseg++] = sg;
+    tbl.segs[nseg++] = sg;
   }
   for (uint32_t i = 0; i < n_batches; ++i) {
     const rkf_ray_batch& r = batches[i];
@@ -95,12 +124,14 @@ extern "C" rkf_status rkf_march_batch_noalloc(rkf_ctx* ctx, const rkf_view* view
     Segment sg = ray_segment(r.origins, r.dirs, r.tmax, r.n, r.mode, r.out);
     sg.first = first;
     first += sg.n_ids;
-    segs[nseg++] = sg;
+    tbl.segs[nseg++] = sg;
   }
   if (nseg == 0) return RKF_OK;
-  // the counter must start at zero on every call (launch_persistent_scratch
-  // clears it on the stream before the launch)
-  return launch_persistent_scratch(c, segs.data(), nseg, first, p, tu,
-                                   stream ? static_cast<cudaStream_t>(stream) : c->stream,
-                                   scratch->segs, &scratch->counter);
+  tbl.nseg = nseg;
+  const cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  // the table and a cleared counter go in by value; the march then reads them
+  k_noalloc_stage<<<1, 256, 0, s>>>(tbl, scratch);
+  RKF_CUDA_TRY(cudaGetLastError());
+  return launch_persistent_scratch(c, tbl.segs, nseg, first, p, tu, s, scratch->segs, &scratch->counter,
+                                   /*segs_uploaded=*/true, /*multi_empty=*/true);
 }
