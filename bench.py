@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import argparse
 import contextlib
+import dataclasses
 import json
 import os
 import subprocess
@@ -61,9 +62,11 @@ def parse():
     ap.add_argument("--cb-views", type=int, default=64, help="views in the batching workload (0 = skip)")
     ap.add_argument("--cb-steps", type=int, default=3)
     ap.add_argument("--cs-requests", type=int, default=600, help="requests in the serving run (0 = skip)")
-    ap.add_argument("--cs-rate", type=float, default=2000.0)
+    ap.add_argument("--cs-rate", type=float, default=2000.0, help="the serving workload's offered rate")
+    ap.add_argument("--cs-rates", default="5000,10000,20000",
+                    help="further offered rates of the same requests (comma list; empty = none)")
     ap.add_argument("--cs-sat-rate", type=float, default=50000.0,
-                    help="arrival rate of a second serving run that saturates the loop (0 = skip)")
+                    help="arrival rate of a last serving run that saturates the loop (0 = skip)")
     ap.add_argument("--cs-budget", type=int, default=32768, help="serving memory budget, MiB")
     ap.add_argument("--pool-bricks", type=int, default=0, help="brick slots to reserve (0 = default)")
     ap.add_argument("--no-reference-pool", action="store_true",
@@ -461,17 +464,47 @@ def warm_serving(local):
         ctx.close()
 
 
-def run_serving(args, spec, prims, p, local, rate=None, with_plain=True):
-    """Poisson request stream through the serving loop vs plain per-request
-    launches of the same requests."""
-    import ctypes as C
-
-    from rkifield_b200 import cudart, engine, workloads
-    from rkifield_b200.engine import Context, RkfError, Server
-    rate = rate or args.cs_rate
-    reqs = workloads.make_request_stream(spec, prims, args.cs_requests, seed=500, rate_hz=rate)
+def run_serving(args, spec, prims, p, local, rates, with_plain=True):
+    """Poisson request stream through the serving loop at each offered rate
+    (the same requests, arrivals scaled), vs plain per-request launches of
+    the same requests (one at a time in arrival order; their service times
+    are measured once, and each rate's latencies follow from its arrivals)."""
+    from rkifield_b200 import workloads
+    base = workloads.make_request_stream(spec, prims, args.cs_requests, seed=500, rate_hz=args.cs_rate)
     keep = []
-    # page-locked inputs and outputs for every request
+    bufs = _serving_buffers(base, keep)
+    plain = _serving_plain(args, spec, prims, p, local, base, bufs) if with_plain else None
+    out = {"requests": len(base), "rays": sum(r.n for r in base if r.kind in (0, 1)),
+           "points": sum(r.n for r in base if r.kind == 2), "edits": sum(1 for r in base if r.kind == 3),
+           "by_rate": []}
+    for rate in rates:
+        scale = args.cs_rate / rate
+        reqs = [dataclasses.replace(r, arrival_s=r.arrival_s * scale) for r in base]
+        served = _serving_served(args, spec, prims, p, local, reqs, bufs)
+        row = {"rate_hz": rate, "served": served}
+        if plain is not None:
+            lat_p = _fifo_latency(reqs, plain["service_s"])
+            row["plain_latency_ms"] = {"p50": float(np.percentile(lat_p, 50)), "p99": float(np.percentile(lat_p, 99))}
+            row["vs_plain"] = served["value"] / plain["value"]
+        out["by_rate"].append(row)
+    if plain is not None:
+        out["plain_per_request"] = {k: v for k, v in plain.items() if k != "service_s"}
+    return out
+
+
+def _fifo_latency(reqs, service):
+    """Latencies (ms) of a single FIFO server with the given service times."""
+    done, lat = 0.0, []
+    for r, s in zip(reqs, service):
+        start = max(done, r.arrival_s)
+        done = start + s
+        lat.append((done - r.arrival_s) * 1e3)
+    return lat
+
+
+def _serving_buffers(reqs, keep):
+    """Page-locked inputs and outputs for every request."""
+    from rkifield_b200 import engine
     bufs = []
     for r in reqs:
         if r.kind == 0:
@@ -491,11 +524,14 @@ def run_serving(args, spec, prims, p, local, rate=None, with_plain=True):
             bufs.append((ins, dict(zip(names, _pinned_copy([o[k] for k in names], keep)))))
         else:
             bufs.append((None, None))
-    rays_of = lambda r: r.n if r.kind in (0, 1) else 0  # noqa: E731
-    total_rays = sum(rays_of(r) for r in reqs)
-    total_pts = sum(r.n for r in reqs if r.kind == 2)
+    return bufs
 
-    # ---- served ----------------------------------------------------------------
+
+def _serving_served(args, spec, prims, p, local, reqs, bufs):
+    """One serving session over the requests at their arrival times."""
+    from rkifield_b200.engine import Context, RkfError, Server
+    total_rays = sum(r.n for r in reqs if r.kind in (0, 1))
+    total_pts = sum(r.n for r in reqs if r.kind == 2)
     ctx = Context(device=local, pool_capacity=LARGE_POOL, mem_budget_bytes=args.cs_budget << 20,
                   max_inflight=1024)
     ctx.voxelize(prims, scenes.voxelize_params(spec, prims))
@@ -541,11 +577,19 @@ def run_serving(args, spec, prims, p, local, rate=None, with_plain=True):
     # latency = admission delay (arrival -> accepted) + loop latency (accepted -> done)
     lat = np.array([(submit_wall[k] - reqs[k].arrival_s) * 1e3 + (res[k]["done_us"] - res[k]["submit_us"]) / 1e3
                     for k in range(len(reqs))])
-    served = {"value": total_rays / wall / 1e6, "unit": "Mrays/s", "points_per_s": total_pts / wall,
-              "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
-              "busy_retries": busy, "wall_s": wall}
-    if not with_plain:
-        return {"requests": len(reqs), "rate_hz": rate, "served": served}
+    return {"value": total_rays / wall / 1e6, "unit": "Mrays/s", "points_per_s": total_pts / wall,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "busy_retries": busy, "wall_s": wall, "offered_s": reqs[-1].arrival_s}
+
+
+def _serving_plain(args, spec, prims, p, local, reqs, bufs):
+    """Each request through its own launches, one at a time in arrival order."""
+    import ctypes as C
+
+    from rkifield_b200 import cudart, engine
+    from rkifield_b200.engine import Context
+    total_rays = sum(r.n for r in reqs if r.kind in (0, 1))
+    total_pts = sum(r.n for r in reqs if r.kind == 2)
 
     # ---- plain: one launch per request, in arrival order, one at a time --------
     # device buffers are allocated once (the largest request); each request
@@ -584,18 +628,12 @@ def run_serving(args, spec, prims, p, local, rate=None, with_plain=True):
             ctx.edit(r.edit)
         service.append(time.perf_counter() - a)
     ctx.close()
-    # FIFO single server fed by the same arrivals
-    done, lat_p = 0.0, []
-    for r, s in zip(reqs, service):
-        start = max(done, r.arrival_s)
-        done = start + s
-        lat_p.append((done - r.arrival_s) * 1e3)
     plain_wall = sum(service)
-    plain = {"value": total_rays / plain_wall / 1e6, "unit": "Mrays/s", "points_per_s": total_pts / plain_wall,
-             "latency_ms": {"p50": float(np.percentile(lat_p, 50)), "p99": float(np.percentile(lat_p, 99))}}
-    return {"requests": len(reqs), "rate_hz": rate, "rays": total_rays, "points": total_pts,
-            "edits": sum(1 for r in reqs if r.kind == 3), "served": served, "plain_per_request": plain,
-            "vs_plain": served["value"] / plain["value"]}
+    lat_p = _fifo_latency(reqs, service)
+    return {"value": total_rays / plain_wall / 1e6, "unit": "Mrays/s", "points_per_s": total_pts / plain_wall,
+            "latency_ms_at_base_rate": {"p50": float(np.percentile(lat_p, 50)),
+                                        "p99": float(np.percentile(lat_p, 99))},
+            "service_s": service}
 
 
 def run_precision_report(args):
@@ -630,8 +668,9 @@ def run_precision_report(args):
     report = {"scene": spec.name, "view": f"{w}x{h}", "rays": w * h, "fp64_hit_fraction": float(hit64.mean()),
               "fp64_oracle_s": oracle_s, "precisions": {}}
     ao_ref = None
-    for prec in ("f32", "f16", "u8"):
-        ctx = Context(pool_capacity=v.n_bricks + 1024, precision=prec, keep_reference_pool=False)
+    # u8: codes rounded toward zero (never overstating |d|) and to nearest
+    for name, prec, rnd in (("f32", "f32", 0), ("f16", "f16", 0), ("u8", "u8", 0), ("u8_nearest", "u8", 1)):
+        ctx = Context(pool_capacity=v.n_bricks + 1024, precision=prec, keep_reference_pool=False, u8_round=rnd)
         ctx.voxelize(prims, vp)
         g = ctx.march(cam, p, w, h)
         hit = (g["flags"] & 1) != 0
@@ -680,9 +719,135 @@ def run_precision_report(args):
         entry["ao_rays"] = int(ao_t.size)
         entry["ao_occlusion_agreement"] = float(ag.mean())
         entry["ao_occlusion_agreement_non_grazing"] = float(ag[ao_ref["margin"] >= 1e-3 * vs].mean())
-        report["precisions"][prec] = entry
+        report["precisions"][name] = entry
         ctx.close()
     print(json.dumps({"report": "precision", **report}), flush=True)
+
+
+def _view_dirs(cam, w, h):
+    """Unit primary-ray directions of a view (float64, ray_march.wgsl:1046-1053)."""
+    px, py = np.meshgrid(np.arange(w, dtype=np.float64), np.arange(h, dtype=np.float64))
+    u, v = (px.ravel() + 0.5) / w, (py.ravel() + 0.5) / h
+    fwd, right, up = (np.array(x[:3], np.float64) for x in (cam.forward, cam.right, cam.up))
+    d = fwd[None] + (2 * u - 1)[:, None] * right[None] + (1 - 2 * v)[:, None] * up[None]
+    return d / np.linalg.norm(d, axis=1, keepdims=True)
+
+
+def _error_entry(g, ref, dirs, vs):
+    """Per-view error of a device march against the FP64 march, with the
+    grazing rays of the parity rule set aside: an FP64 decision within 1e-3
+    voxel of its threshold, a hit at under 0.05 of normal incidence, or a
+    hit/miss the device (FP32) and FP64 marches disagree on."""
+    hit = (g["flags"] & 1) != 0
+    hit64 = (ref["flags"] & 1) != 0
+    n64 = ref["normal64"].reshape(-1, 3)
+    cosi = np.abs(np.sum(dirs * n64, axis=1))
+    graze = (ref["margin"] < 1e-3 * vs) | (hit64 & (cosi < 0.05)) | (hit != hit64)
+    both = hit & hit64 & ~graze
+    dt = np.abs(g["t"][both].astype(np.float64) - ref["t64"][both]) / vs
+    ng = g["normal"].reshape(-1, 3)[both].astype(np.float64)
+    cosang = np.clip(np.sum(ng * n64[both], axis=1) / np.maximum(
+        np.linalg.norm(ng, axis=1) * np.linalg.norm(n64[both], axis=1), 1e-300), -1.0, 1.0)
+    ang = np.arccos(cosang)
+    q = lambda a, f: float(f(a)) if a.size else None  # noqa: E731
+    return {"rays": int(hit.size), "fp64_hits": int(hit64.sum()), "grazing_fraction": float(graze.mean()),
+            "hit_agreement": float((hit == hit64).mean()),
+            "hit_agreement_non_grazing": float((hit == hit64)[~graze].mean()),
+            "material_agreement": float((g["material"][both] == ref["material"][both]).mean()) if both.any() else None,
+            "dt_voxels": {"max": q(dt, np.max), "p99": q(dt, lambda a: np.percentile(a, 99)), "mean": q(dt, np.mean)},
+            "within_0.01_voxel": q(dt, lambda a: (a <= 0.01).mean()),
+            "normal_rad": {"max": q(ang, np.max), "p99": q(ang, lambda a: np.percentile(a, 99)),
+                           "mean": q(ang, np.mean)}}
+
+
+def run_precision_report_large(args):
+    """FP64 error of the large scene's f16 march: the headline view at
+    1920x1080 and 960x540, three views of the batching workload (smallest,
+    median, largest) and 20,000 of their soft-shadow and AO rays, against the
+    FP64 march over FP64 voxel values at the same voxel centres."""
+    import ctypes as C
+
+    from oracle import binding as oracle
+    from rkifield_b200 import cudart, workloads
+    from rkifield_b200.engine import Context
+    spec = scenes.SCENE_LARGE
+    prims = scenes.make_prims(spec)
+    vp = scenes.voxelize_params(spec, prims)
+    p = scenes.march_params(spec)
+    vs = spec.voxel_size
+    threads = os.cpu_count() or 1
+    ctx = Context(pool_capacity=LARGE_POOL, keep_reference_pool=False)
+    ctx.voxelize(prims, vp)
+    idx = ctx.export_index()
+    t0 = time.perf_counter()
+    bxyz, slots = oracle.index_bricks(idx["top"], idx["leaves"], idx["obj_top_info"])
+    n_slots = int(slots.max()) + 1
+    pl = ctx.export_planes(0, n_slots)
+    f64 = oracle.voxel_values_f64_bricks(prims, vp, bxyz, slots, n_slots, threads)
+    values_s = time.perf_counter() - t0
+    obj = ctx.object(0)
+    sc64 = oracle.Scene([obj], top=idx["top"], leaves=idx["leaves"], obj_top_info=idx["obj_top_info"],
+                        mat_plane=pl["mat"], blend_plane=pl["blend"], precision=oracle.PRECISION_F64, dist_f64=f64)
+    report = {"scene": spec.name, "bricks": int(slots.size), "fp64_values_s": values_s, "views": {}}
+    views = [("headline 1920x1080", camera_for(spec, 1920, 1080, 0), 1920, 1080),
+             ("headline 960x540", camera_for(spec, 960, 540, 0), 960, 540)]
+    cb = workloads.make_views(spec, prims, 64, seed=300)
+    order = np.argsort([v.width * v.height for v in cb], kind="stable")
+    for name, i in (("batch smallest", order[0]), ("batch median", order[len(order) // 2]),
+                    ("batch largest", order[-1])):
+        v = cb[i]
+        views.append((f"{name} {v.width}x{v.height}", v.cam, v.width, v.height))
+    cb_gbufs = []
+    for name, cam, w, h in views:
+        t1 = time.perf_counter()
+        g = ctx.march(cam, p, w, h)
+        ref = oracle.march(sc64, cam, p, w, h, fp64=True, threads=threads, with_margin=True)
+        e = _error_entry(g, ref, _view_dirs(cam, w, h), vs)
+        e["fp64_march_s"] = time.perf_counter() - t1
+        report["views"][name] = e
+        if name.startswith("batch"):
+            cb_gbufs.append((cam, w, h, g))
+        print(json.dumps({name: e}), file=sys.stderr, flush=True)
+    # secondary rays of the three batch views, through the device march and FP64
+    rng = np.random.default_rng(17)
+    sec = {"shadow": [], "ao": []}
+    for i, (cam, w, h, g) in enumerate(cb_gbufs):
+        npx = w * h
+        dev = cudart.device_gbuffer(npx)
+        for k in ("t", "normal", "flags"):
+            dev[k].upload(g[k])
+        target = np.array(cam.position[:3], np.float64) + 8.0 * np.array(cam.forward[:3], np.float64)
+        lights = (target[None] + rng.uniform(-10, 10, (4, 3)) + np.array([0.0, 8.0, 0.0])).astype(np.float32)
+        arrs = [cudart.DeviceArray(3 * 4 * npx, np.float32), cudart.DeviceArray(3 * 4 * npx, np.float32),
+                cudart.DeviceArray(4 * npx, np.float32), cudart.DeviceArray(3 * 8 * npx, np.float32),
+                cudart.DeviceArray(3 * 8 * npx, np.float32), cudart.DeviceArray(8 * npx, np.float32)]
+        gb = abi.rkf_gbuffer()
+        gb.t, gb.normal, gb.flags, gb.mem = dev["t"].ptr, dev["normal"].ptr, dev["flags"].ptr, abi.RKF_MEM_DEVICE
+        nh = C.c_uint32()
+        abi.check(ctx.lib.rkf_secondary_rays(ctx.h, C.byref(cam), w, h, C.byref(gb), lights.ctypes.data, 4, 8, 1.0,
+                                             300 * 1000 + i, *[a.ptr for a in arrs], C.byref(nh), None), "secondary")
+        for key, (o, d, t) in (("shadow", arrs[0:3]), ("ao", arrs[3:6])):
+            tm = t.download()
+            live = np.nonzero(tm > 0)[0]
+            sel = live if live.size <= 3400 else np.sort(rng.choice(live, 3400, replace=False))
+            sec[key].append((o.download().reshape(-1, 3)[sel], d.download().reshape(-1, 3)[sel], tm[sel]))
+    for key, mode in (("shadow", abi.RKF_TRACE_SHADOW), ("ao", abi.RKF_TRACE_ANY)):
+        o = np.concatenate([a[0] for a in sec[key]])
+        d = np.concatenate([a[1] for a in sec[key]])
+        tm = np.concatenate([a[2] for a in sec[key]])
+        got = ctx.trace(o, d, tm, mode, p)
+        ref = oracle.trace(sc64, o.ravel(), d.ravel(), tm, mode, p, fp64=True, threads=threads, with_margin=True)
+        ok = ref["margin"] >= 1e-3 * vs
+        ent = {"rays": int(tm.size), "grazing_fraction": float((~ok).mean()),
+               "occlusion_agreement": float(((got["flags"] & 1) == (ref["flags"] & 1)).mean()),
+               "occlusion_agreement_non_grazing": float(((got["flags"] & 1) == (ref["flags"] & 1))[ok].mean())}
+        if mode == abi.RKF_TRACE_SHADOW:
+            ds = np.abs(got["t"].astype(np.float64) - ref["t64"])[ok]
+            ent["shadow_factor_abs_err"] = {"max": float(ds.max()), "p99": float(np.percentile(ds, 99)),
+                                            "mean": float(ds.mean())}
+        report["secondary_" + key] = ent
+    ctx.close()
+    print(json.dumps({"report": "precision_large", **report}), flush=True)
 
 
 def time_view(ctx, cam, p, w, h, stream, steps, plain=False):
@@ -739,6 +904,27 @@ def run_extras(args, spec, prims, p, ctx, stream):
             c2.close()
     out["precision_views"] = prec
     out["note"] = "CUDA-event means without the L2 flush of the headline steps"
+    return out
+
+
+def _headline_summary(batching, serving):
+    """The metric's comparison in one place: the batched launch and the
+    serving loop (at each offered rate) against plain per-request launches
+    of the same work, with the loop's p50/p99 latency."""
+    if batching is None and serving is None:
+        return None
+    out = {}
+    if batching is not None:
+        out["batched"] = {"value": batching["batched"]["value"], "unit": "Mrays/s",
+                          "vs_plain": batching["vs_plain"],
+                          "vs_b200_per_request": batching["batched"]["value"] / batching["b200_per_request"]["value"],
+                          "plain_per_request": batching["plain_per_request"]["value"]}
+    if serving is not None:
+        out["served"] = [{"rate_hz": r["rate_hz"], "value": r["served"]["value"], "unit": "Mrays/s",
+                          "p50_ms": r["served"]["latency_ms"]["p50"], "p99_ms": r["served"]["latency_ms"]["p99"],
+                          "vs_plain": r.get("vs_plain")} for r in serving["by_rate"]]
+        if "plain_per_request" in serving:
+            out["served_plain_per_request"] = serving["plain_per_request"]["value"]
     return out
 
 
@@ -843,13 +1029,12 @@ def run_b200(args, world, rank, local, dist):
     serving = None
     if args.cs_requests > 0 and rank == 0:
         warm_serving(local)
-        serving = run_serving(args, spec, prims, p, local)
+        # the offered rate, faster ones, and one that saturates the loop
+        # (throughput at capacity instead of the offered load)
+        rates = [args.cs_rate] + [float(x) for x in args.cs_rates.split(",") if x.strip()]
         if args.cs_sat_rate > 0:
-            # the same requests arriving faster than they can be served:
-            # throughput at capacity instead of at the offered load
-            sat = run_serving(args, spec, prims, p, local, rate=args.cs_sat_rate, with_plain=False)
-            sat["vs_plain"] = sat["served"]["value"] / serving["plain_per_request"]["value"]
-            serving["saturated"] = sat
+            rates.append(args.cs_sat_rate)
+        serving = run_serving(args, spec, prims, p, local, rates)
 
     out = None
     if rank == 0:
@@ -909,6 +1094,7 @@ def run_b200(args, world, rank, local, dist):
             "extras": extras,
             "batching": batching,
             "serving": serving,
+            "served_batched": _headline_summary(batching, serving),
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": args.steps,
@@ -924,7 +1110,10 @@ def main():
     try:
         if args.report == "precision":
             if rank == 0:
-                run_precision_report(args)
+                if args.scene == "large" and "--scene" in sys.argv:
+                    run_precision_report_large(args)
+                else:
+                    run_precision_report(args)
         elif args.impl == "reference":
             run_reference(args, world, rank, dist)
         else:

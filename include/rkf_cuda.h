@@ -167,7 +167,14 @@ typedef struct rkf_config {
                                     /* (needed by rkf_march_plain)           */
     uint64_t mem_budget_bytes;      /* serving admission budget, 0 = auto    */
     uint32_t max_inflight;          /* serving slots, 0 = default (64)       */
-    uint32_t reserved[7];
+    float u8_band;                  /* u8 precision: half-width (metres) of  */
+                                    /* the distance band the codes cover;    */
+                                    /* 0 = 3 voxels for voxelized objects,   */
+                                    /* each brick's largest |d| for imports  */
+    uint32_t u8_round;              /* u8 precision: 0 = codes round toward  */
+                                    /* zero (a decoded |d| never exceeds the */
+                                    /* true one), 1 = to nearest (unbiased)  */
+    uint32_t reserved[5];
 } rkf_config;
 
 RKF_API void rkf_config_default(rkf_config* cfg);
@@ -510,6 +517,10 @@ typedef struct rkf_batch_tuning {
                                  /* scene allows them).  rkf_march,          */
                                  /* rkf_march_batch and rkf_trace_rays only; */
                                  /* the outputs are the same either way      */
+    uint32_t order_tiles;        /* 1: hand out each view's ray tiles        */
+                                 /* heaviest first, by an estimate of their  */
+                                 /* empty-space steps (0: row order); the    */
+                                 /* outputs are the same either way          */
 } rkf_batch_tuning;
 
 /* Run every view and ray batch in one persistent work-stealing launch.
@@ -562,11 +573,17 @@ RKF_API rkf_status rkf_march_batch_noalloc(rkf_ctx* ctx, const rkf_view* views, 
                                            const rkf_march_params* p,
                                            const rkf_batch_tuning* tuning, void* stream);
 
-/* Search tile shape x step budget x compaction interval on a sample of the
- * given work and store the winner in the context.  Writes it to *out. */
+/* Search tile shape x step budget x compaction interval (and the other
+ * knobs of rkf_batch_tuning) on a sample of the given work and store the
+ * winner in the context.  Writes it to *out. */
 RKF_API rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t n_views,
                         const rkf_ray_batch* batches, uint32_t n_batches,
                         const rkf_march_params* p, rkf_batch_tuning* out);
+/* The tuning the context's marches use when none is given (rkf_march,
+ * rkf_march_async, rkf_trace_rays, the serving loop): set one found earlier
+ * (a tuning never changes results), or read the current one. */
+RKF_API rkf_status rkf_tuning_set(rkf_ctx* ctx, const rkf_batch_tuning* tuning);
+RKF_API rkf_status rkf_tuning_get(rkf_ctx* ctx, rkf_batch_tuning* out);
 
 /* ------------------------------------------------------------------------ */
 /* A batched march captured as a CUDA graph (no counterpart in the          */
@@ -653,6 +670,31 @@ typedef struct rkf_world_pos {
 /* out = (float)(pos - origin) computed in FP64 (relative_to_f64). */
 RKF_API void rkf_world_relative(const rkf_world_pos* pos, const rkf_world_pos* origin,
                         double out_f64[3], float out_f32[3]);
+
+/* The WorldPosition that the scene's f32 world-space coordinates (object
+ * transforms and grids) are relative to; chunk (0,0,0) and local (0,0,0)
+ * until set.  A world far from the origin (chunks beyond what f32 metres
+ * resolve) is uploaded relative to a nearby origin, and cameras and ray
+ * origins given as WorldPositions are rebased against it in FP64 on the host
+ * (WorldPosition::relative_to_f64, world_position.rs:107-120; the render
+ * path's camera-relative positions, transform_flatten.rs:8-12) and rounded
+ * to f32 once, before the f32 march.  Not while serving. */
+RKF_API rkf_status rkf_scene_origin_set(rkf_ctx* ctx, const rkf_world_pos* origin);
+RKF_API rkf_status rkf_scene_origin_get(rkf_ctx* ctx, rkf_world_pos* out);
+
+/* rkf_march with the camera at a WorldPosition: the march uses cam with
+ * its position replaced by the f32 rounding of relative_to_f64(cam_pos,
+ * scene origin). */
+RKF_API rkf_status rkf_march_world(rkf_ctx* ctx, const rkf_world_pos* cam_pos, const rkf_camera* cam,
+                                   const rkf_march_params* p, uint32_t width, uint32_t height,
+                                   rkf_gbuffer* out);
+
+/* rkf_trace_rays with ray origins as WorldPositions (host arrays: origins[n],
+ * dirs[3n], tmax[n]), each rebased against the scene origin in FP64 and
+ * rounded to f32 once. */
+RKF_API rkf_status rkf_trace_rays_world(rkf_ctx* ctx, const rkf_world_pos* origins, const float* dirs,
+                                        const float* tmax, uint32_t n, uint32_t mode,
+                                        const rkf_march_params* p, rkf_hits* out);
 
 #ifdef __cplusplus
 }

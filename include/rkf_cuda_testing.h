@@ -52,6 +52,12 @@ RKF_API int rkf_testing_last_variant(rkf_ctx* ctx);
  * transform, a non-positive scale or non-finite parameters. */
 RKF_API int rkf_testing_far_ball(const rkf_gpu_object* obj, float empty_hi, float out[5]);
 
+/* Brick-pool and index-leaf bookkeeping: out = {pool capacity, live bricks
+ * (pool_bricks_used), free slots, leaf blocks allocated, free leaf blocks}.
+ * Slots neither live nor free are held for work of older epochs.  Read it
+ * while no edit runs (a serving session between requests, or no session). */
+RKF_API rkf_status rkf_testing_pool_state(rkf_ctx* ctx, uint32_t out[5]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -84,6 +84,7 @@ def lib() -> C.CDLL:
         L.orc_sample_brick_trilinear.argtypes = [P, P, C.c_float]
         L.orc_march_params_default.argtypes = [P]
         L.orc_voxel_values_f64.argtypes = [P, U32, P, P, U32, P, I]
+        L.orc_voxel_values_f64_bricks.argtypes = [P, U32, P, P, P, C.c_uint64, P, I]
         _lib = L
     return _lib
 
@@ -256,3 +257,32 @@ def voxel_values_f64(prims, vp, brick_map, n_slots: int, threads: int | None = N
     lib().orc_voxel_values_f64(ptr(prims), len(prims), C.byref(vp), ptr(brick_map), n_slots, ptr(out),
                                threads or nthreads())
     return out
+
+
+def voxel_values_f64_bricks(prims, vp, bxyz, slots, n_slots: int, threads: int | None = None):
+    """FP64 scene SDF at the voxel centres of the listed bricks (coordinates
+    bxyz (n,3), pool slots (n,)), into an array of n_slots bricks."""
+    bxyz = np.ascontiguousarray(bxyz, np.uint32)
+    slots = np.ascontiguousarray(slots, np.uint32)
+    out = np.zeros(int(n_slots) * 512, np.float64)
+    lib().orc_voxel_values_f64_bricks(ptr(prims), len(prims), C.byref(vp), ptr(bxyz), ptr(slots), slots.size,
+                                      ptr(out), threads or nthreads())
+    return out
+
+
+def index_bricks(top, leaves, obj_top_info, obj: int = 0):
+    """Brick coordinates and pool slots of every allocated brick of one object
+    in a two-level index (top grid of 8^3-brick blocks, 512-entry leaves)."""
+    off, tx, ty, tz = (int(x) for x in obj_top_info[4 * obj:4 * obj + 4])
+    cells = np.asarray(top[off:off + tx * ty * tz], np.uint32)
+    blk = np.nonzero(cells < abi.INTERIOR_SLOT)[0]
+    leaf = cells[blk].astype(np.int64)
+    kx, ky, kz = blk % tx, (blk // tx) % ty, blk // (tx * ty)
+    j = np.arange(512)
+    sl = np.asarray(leaves, np.uint32).reshape(-1, 512)[leaf]  # (nblk, 512)
+    m = sl < abi.INTERIOR_SLOT
+    bi, ji = np.nonzero(m)
+    bx = kx[bi] * 8 + (j[ji] & 7)
+    by = ky[bi] * 8 + ((j[ji] >> 3) & 7)
+    bz = kz[bi] * 8 + (j[ji] >> 6)
+    return np.stack([bx, by, bz], axis=1).astype(np.uint32), sl[bi, ji].astype(np.uint32)

@@ -1268,6 +1268,147 @@ orc_voxelized* orc_voxelize(const rkf_prim* prims, uint32_t n_prims,
   return v;
 }
 
+// The same voxelization into a two-level index (top grid of 8^3-brick
+// blocks, 512-entry leaves) and SoA planes, for grids whose flat brick map
+// would not fit host memory.  A brick no primitive's candidate test reaches
+// has no candidates, so classify_brick finds it EMPTY; only the bricks near
+// some primitive are classified, in ascending flat order, which keeps the slot
+// order and every word of orc_voxelize.
+struct orc_sparse {
+  Grid g;
+  uint32_t tdim[3] = {0, 0, 0};
+  std::vector<uint32_t> top, leaves;
+  std::vector<uint16_t> dist_f16, mat;
+  std::vector<uint8_t> blend;
+  std::vector<uint32_t> bxyz;  // coordinates of each allocated brick, by slot
+  uint32_t n_bricks = 0, n_interior = 0, n_leaves = 0;
+};
+
+orc_sparse* orc_voxelize_sparse(const rkf_prim* prims, uint32_t n_prims, const rkf_voxelize_params* vp,
+                                int threads) {
+  auto* v = new orc_sparse;
+  v->g = make_grid(vp);
+  const Grid& g = v->g;
+  const uint64_t dx = g.dims[0], dy = g.dims[1], dz = g.dims[2];
+  // 1. bricks some primitive's candidate test reaches (brick_candidates)
+  std::vector<std::vector<uint64_t>> per(n_prims);
+  parallel_for(n_prims, threads, [&](uint64_t i, int) {
+    const rkf_prim& pr = prims[i];
+    const double reach = static_cast<double>(pr.bound_radius) + vp->cut_distance + 0.05 * g.bws + 1e-3;
+    int64_t lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = static_cast<int64_t>(std::floor((pr.centre[a] - reach - g.origin[a]) / g.bws)) - 1;
+      hi[a] = static_cast<int64_t>(std::ceil((pr.centre[a] + reach - g.origin[a]) / g.bws)) + 1;
+      lo[a] = std::max<int64_t>(lo[a], 0);
+      hi[a] = std::min<int64_t>(hi[a], static_cast<int64_t>(g.dims[a]) - 1);
+    }
+    for (int64_t z = lo[2]; z <= hi[2]; ++z)
+      for (int64_t y = lo[1]; y <= hi[1]; ++y)
+        for (int64_t x = lo[0]; x <= hi[0]; ++x) {
+          float bmin[3];
+          brick_min_of(g, static_cast<uint32_t>(x), static_cast<uint32_t>(y), static_cast<uint32_t>(z), bmin);
+          double d2 = 0.0;
+          for (int a = 0; a < 3; ++a) {
+            const double l = bmin[a], h = static_cast<double>(bmin[a]) + g.bws;
+            const double c = pr.centre[a];
+            const double e = c < l ? l - c : (c > h ? c - h : 0.0);
+            d2 += e * e;
+          }
+          if (d2 < reach * reach) per[i].push_back(static_cast<uint64_t>(x) + y * dx + z * dx * dy);
+        }
+  });
+  std::vector<uint64_t> cand;
+  for (auto& p : per) {
+    cand.insert(cand.end(), p.begin(), p.end());
+    std::vector<uint64_t>().swap(p);
+  }
+  std::sort(cand.begin(), cand.end());
+  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+  // 2. classify the candidates
+  std::vector<uint8_t> cls(cand.size(), 1);
+  std::vector<std::vector<uint32_t>> cands(std::max(threads, 1));
+  parallel_for(cand.size(), threads, [&](uint64_t k, int th) {
+    const uint64_t f = cand[k];
+    BrickResult r;
+    classify_brick(prims, n_prims, vp, g, static_cast<uint32_t>(f % dx), static_cast<uint32_t>((f / dx) % dy),
+                   static_cast<uint32_t>(f / (dx * dy)), cands[th], r);
+    cls[k] = static_cast<uint8_t>(r.cls);
+  });
+  // 3. slots in ascending flat order; index blocks
+  for (int a = 0; a < 3; ++a) v->tdim[a] = (g.dims[a] + 7) / 8;
+  const uint64_t tx = v->tdim[0], ty = v->tdim[1], tz = v->tdim[2];
+  v->top.assign(tx * ty * tz, RKF_EMPTY_SLOT);
+  std::vector<uint64_t> alloc;
+  std::vector<uint32_t> slot_of(cand.size(), RKF_EMPTY_SLOT);
+  for (uint64_t k = 0; k < cand.size(); ++k) {
+    if (cls[k] == 1) continue;
+    const uint64_t f = cand[k];
+    const uint64_t blk = (f % dx) / 8 + ((f / dx) % dy) / 8 * tx + (f / (dx * dy)) / 8 * tx * ty;
+    if (v->top[blk] == RKF_EMPTY_SLOT) v->top[blk] = v->n_leaves++;
+    if (cls[k] == 0) {
+      slot_of[k] = v->n_bricks++;
+      alloc.push_back(k);
+    } else {
+      slot_of[k] = RKF_INTERIOR_SLOT;
+      v->n_interior++;
+    }
+  }
+  v->leaves.assign(static_cast<uint64_t>(v->n_leaves) * 512, RKF_EMPTY_SLOT);
+  for (uint64_t k = 0; k < cand.size(); ++k) {
+    if (cls[k] == 1) continue;
+    const uint64_t f = cand[k];
+    const uint64_t x = f % dx, y = (f / dx) % dy, z = f / (dx * dy);
+    const uint64_t blk = x / 8 + y / 8 * tx + z / 8 * tx * ty;
+    v->leaves[static_cast<uint64_t>(v->top[blk]) * 512 + (x & 7) + (y & 7) * 8 + (z & 7) * 64] = slot_of[k];
+  }
+  // 4. the allocated bricks' planes
+  const uint64_t nb = v->n_bricks;
+  v->dist_f16.resize(nb * 512);
+  v->mat.resize(nb * 512);
+  v->blend.resize(nb * 512);
+  v->bxyz.resize(nb * 3);
+  parallel_for(nb, threads, [&](uint64_t s, int th) {
+    const uint64_t f = cand[alloc[s]];
+    const uint32_t x = static_cast<uint32_t>(f % dx), y = static_cast<uint32_t>((f / dx) % dy),
+                   z = static_cast<uint32_t>(f / (dx * dy));
+    BrickResult r;
+    classify_brick(prims, n_prims, vp, g, x, y, z, cands[th], r);
+    for (uint32_t i = 0; i < 512; ++i) {
+      const uint32_t w0 = r.words[2 * i];
+      v->dist_f16[s * 512 + i] = static_cast<uint16_t>(w0 & 0xFFFFu);
+      v->mat[s * 512 + i] = static_cast<uint16_t>(((w0 >> 16) & 0x3Fu) | (((w0 >> 22) & 0x3Fu) << 6));
+      v->blend[s * 512 + i] = static_cast<uint8_t>(r.words[2 * i + 1] >> 24);
+    }
+    v->bxyz[3 * s] = x;
+    v->bxyz[3 * s + 1] = y;
+    v->bxyz[3 * s + 2] = z;
+  });
+  return v;
+}
+
+void orc_sparse_info(const orc_sparse* v, uint32_t dims[3], uint32_t tdim[3], uint32_t* n_bricks,
+                     uint32_t* n_interior, uint32_t* n_leaves) {
+  for (int a = 0; a < 3; ++a) {
+    dims[a] = v->g.dims[a];
+    tdim[a] = v->tdim[a];
+  }
+  *n_bricks = v->n_bricks;
+  *n_interior = v->n_interior;
+  *n_leaves = v->n_leaves;
+}
+
+void orc_sparse_copy(const orc_sparse* v, uint32_t* top, uint32_t* leaves, uint16_t* dist_f16, uint16_t* mat,
+                     uint8_t* blend, uint32_t* bxyz) {
+  std::memcpy(top, v->top.data(), v->top.size() * 4);
+  std::memcpy(leaves, v->leaves.data(), v->leaves.size() * 4);
+  std::memcpy(dist_f16, v->dist_f16.data(), v->dist_f16.size() * 2);
+  std::memcpy(mat, v->mat.data(), v->mat.size() * 2);
+  std::memcpy(blend, v->blend.data(), v->blend.size());
+  std::memcpy(bxyz, v->bxyz.data(), v->bxyz.size() * 4);
+}
+
+void orc_sparse_free(orc_sparse* v) { delete v; }
+
 void orc_voxelized_info(const orc_voxelized* v, uint32_t dims[3], uint32_t* n_bricks,
                         uint32_t* n_interior) {
   for (int a = 0; a < 3; ++a) dims[a] = v->g.dims[a];
@@ -1304,6 +1445,29 @@ void orc_voxel_values_f64(const rkf_prim* prims, uint32_t n_prims, const rkf_vox
       const double py = bmin[1] + (static_cast<float>((v >> 3) & 7) * g.vs + hv);
       const double pz = bmin[2] + (static_cast<float>(v >> 6) * g.vs + hv);
       dist[static_cast<uint64_t>(slot) * 512 + v] =
+          scene_eval<double>(prims, cands[th].data(), static_cast<uint32_t>(cands[th].size()), vp->smooth_k,
+                             vp->cut_distance, px, py, pz, nullptr, nullptr, nullptr);
+    }
+  });
+}
+
+void orc_voxel_values_f64_bricks(const rkf_prim* prims, uint32_t n_prims, const rkf_voxelize_params* vp,
+                                 const uint32_t* bxyz, const uint32_t* slots, uint64_t n, double* dist,
+                                 int threads) {
+  // the same values as orc_voxel_values_f64, for bricks listed with their
+  // slots (a two-level index has no flat map to walk)
+  const Grid g = make_grid(vp);
+  std::vector<std::vector<uint32_t>> cands(std::max(threads, 1));
+  parallel_for(n, threads, [&](uint64_t i, int th) {
+    float bmin[3];
+    brick_min_of(g, bxyz[3 * i], bxyz[3 * i + 1], bxyz[3 * i + 2], bmin);
+    brick_candidates(prims, n_prims, bmin, g.bws, vp->cut_distance, cands[th]);
+    const float hv = g.vs * 0.5f;
+    for (uint32_t v = 0; v < 512; ++v) {
+      const double px = bmin[0] + (static_cast<float>(v & 7) * g.vs + hv);
+      const double py = bmin[1] + (static_cast<float>((v >> 3) & 7) * g.vs + hv);
+      const double pz = bmin[2] + (static_cast<float>(v >> 6) * g.vs + hv);
+      dist[static_cast<uint64_t>(slots[i]) * 512 + v] =
           scene_eval<double>(prims, cands[th].data(), static_cast<uint32_t>(cands[th].size()), vp->smooth_k,
                              vp->cut_distance, px, py, pz, nullptr, nullptr, nullptr);
     }

@@ -62,6 +62,17 @@ typedef struct orc_voxelized orc_voxelized;
 /* Voxelize into a fresh pool (slots 0..n-1) + a flat brick map. */
 orc_voxelized* orc_voxelize(const rkf_prim* prims, uint32_t n_prims,
                             const rkf_voxelize_params* vp, int threads);
+// Voxelization into a two-level index and SoA planes (no flat map): the
+// same slots and words as orc_voxelize, for grids too large for a flat map.
+struct orc_sparse;
+orc_sparse* orc_voxelize_sparse(const rkf_prim* prims, uint32_t n_prims, const rkf_voxelize_params* vp,
+                                int threads);
+void orc_sparse_info(const orc_sparse* v, uint32_t dims[3], uint32_t tdim[3], uint32_t* n_bricks,
+                     uint32_t* n_interior, uint32_t* n_leaves);
+void orc_sparse_copy(const orc_sparse* v, uint32_t* top, uint32_t* leaves, uint16_t* dist_f16, uint16_t* mat,
+                     uint8_t* blend, uint32_t* bxyz);
+void orc_sparse_free(orc_sparse* v);
+
 void orc_voxelized_info(const orc_voxelized* v, uint32_t dims[3], uint32_t* n_bricks,
                         uint32_t* n_interior);
 /* words: 1024 u32 per brick (VoxelSample AoS). map: dims.x*dims.y*dims.z. */
@@ -109,6 +120,11 @@ typedef struct orc_scene {
  * values a perfect storage format would hold. */
 void orc_voxel_values_f64(const rkf_prim* prims, uint32_t n_prims, const rkf_voxelize_params* vp,
                           const uint32_t* map, uint32_t n_slots, double* dist, int threads);
+// orc_voxel_values_f64 for n bricks given by their coordinates (bxyz, 3 per
+// brick) and pool slots.
+void orc_voxel_values_f64_bricks(const rkf_prim* prims, uint32_t n_prims, const rkf_voxelize_params* vp,
+                                 const uint32_t* bxyz, const uint32_t* slots, uint64_t n, double* dist,
+                                 int threads);
 
 typedef struct orc_stats {
     uint64_t sectors;        /* distinct 32-B sectors, summed over rays     */

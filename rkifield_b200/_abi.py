@@ -72,7 +72,7 @@ class rkf_config(C.Structure):
     _fields_ = [("device", C.c_int), ("pool_capacity_bricks", C.c_uint32),
                 ("precision", C.c_uint32), ("keep_reference_pool", C.c_uint32),
                 ("mem_budget_bytes", C.c_uint64), ("max_inflight", C.c_uint32),
-                ("reserved", C.c_uint32 * 7)]
+                ("u8_band", C.c_float), ("u8_round", C.c_uint32), ("reserved", C.c_uint32 * 5)]
 
 
 class rkf_bvh_node(C.Structure):
@@ -144,7 +144,8 @@ class rkf_batch_tuning(C.Structure):
     _fields_ = [("tile_w", C.c_uint32), ("tile_h", C.c_uint32), ("step_budget", C.c_uint32),
                 ("compact_interval", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("threads_per_block", C.c_uint32), ("refill_idle", C.c_uint32),
-                ("probe_in_run", C.c_uint32), ("no_empty_path", C.c_uint32)]
+                ("probe_in_run", C.c_uint32), ("no_empty_path", C.c_uint32),
+                ("order_tiles", C.c_uint32)]
 
 
 class rkf_request(C.Structure):
@@ -235,6 +236,8 @@ SIGNATURES = {
                                      C.POINTER(rkf_march_params), C.POINTER(rkf_batch_tuning), _P]),
     "rkf_autotune": (_I, [_P, C.POINTER(rkf_view), _U32, C.POINTER(rkf_ray_batch), _U32,
                           C.POINTER(rkf_march_params), C.POINTER(rkf_batch_tuning)]),
+    "rkf_tuning_set": (_I, [_P, C.POINTER(rkf_batch_tuning)]),
+    "rkf_tuning_get": (_I, [_P, C.POINTER(rkf_batch_tuning)]),
     "rkf_serve_start": (_I, [_P, C.POINTER(rkf_march_params)]),
     "rkf_serve_stop": (_I, [_P]),
     "rkf_submit": (_I, [_P, C.POINTER(rkf_request), C.POINTER(_U64)]),
@@ -248,8 +251,15 @@ SIGNATURES = {
     "rkf_testing_export_coarse": (_I, [_P, _P, _P, _P, C.POINTER(C.c_uint64)]),
     "rkf_testing_last_variant": (C.c_int, [_P]),
     "rkf_testing_far_ball": (C.c_int, [_P, C.c_float, _P]),
+    "rkf_testing_pool_state": (_I, [_P, _P]),
     "rkf_world_relative": (None, [C.POINTER(rkf_world_pos), C.POINTER(rkf_world_pos),
                                   C.POINTER(C.c_double), C.POINTER(C.c_float)]),
+    "rkf_scene_origin_set": (_I, [_P, C.POINTER(rkf_world_pos)]),
+    "rkf_scene_origin_get": (_I, [_P, C.POINTER(rkf_world_pos)]),
+    "rkf_march_world": (_I, [_P, C.POINTER(rkf_world_pos), C.POINTER(rkf_camera), C.POINTER(rkf_march_params),
+                             _U32, _U32, C.POINTER(rkf_gbuffer)]),
+    "rkf_trace_rays_world": (_I, [_P, _P, _P, _P, _U32, _U32, C.POINTER(rkf_march_params),
+                                  C.POINTER(rkf_hits)]),
 }
 
 _lib = None

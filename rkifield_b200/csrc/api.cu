@@ -5,6 +5,7 @@
 // A large view with host outputs is marched in bands of tile rows, each
 // band's rows copied back on a second stream while the next band marches.
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <cstring>
 #include <vector>
@@ -12,6 +13,7 @@
 #include "../../include/rkf_cuda_testing.h"
 #include "ctx.h"
 #include "march.h"
+#include "tile_order.h"
 
 using namespace rkf;
 
@@ -111,15 +113,35 @@ rkf_status march_host_banded(Ctx* c, const rkf_camera* cam, const rkf_march_para
   const rkf_batch_tuning& tu = c->tuning;
   std::vector<Segment> segs{view_segment(cam, w, h, tu.tile_w, tu.tile_h, dev)};
   segs[0].first = 0;
-  const size_t sb = sizeof(Segment);
-  if (c->seg_buf.bytes < sb && (st = c->seg_buf.alloc(sb)) != RKF_OK) return st;
-  RKF_CUDA_TRY(cudaMemcpyAsync(c->seg_buf.p, segs.data(), sb, cudaMemcpyHostToDevice, c->stream));
-  RKF_CUDA_TRY(cudaEventRecord(c->segs_ev, c->stream));
-  RKF_CUDA_TRY(cudaStreamWaitEvent(c->band_stream, c->segs_ev, 0));
   const uint32_t tile_w = tu.tile_w ? tu.tile_w : 8, tile_h = tu.tile_h ? tu.tile_h : 4;
   const uint64_t row_ids = static_cast<uint64_t>(segs[0].tiles_x) * tile_w * tile_h;
   const uint32_t rows = (h + tile_h - 1) / tile_h;
   const uint32_t weight = 2u * static_cast<uint32_t>(bands) - 1u;
+  // tile rows of each band: band b marches rows [band_rows[b], band_rows[b+1])
+  std::vector<uint32_t> band_rows{0};
+  for (int b = 0; b < bands && band_rows.back() < rows; ++b) {
+    const uint32_t r1 = b == bands - 1 ? rows
+                                       : std::min(rows, static_cast<uint32_t>(
+                                                            (static_cast<uint64_t>(rows) * 2u * (b + 1)) / weight));
+    if (r1 > band_rows.back()) band_rows.push_back(r1);
+  }
+  // heaviest-first order within each band, planned once for all bands
+  ObjDev order_obj;
+  OrderTable order_tbl;
+  bool ordered = false;
+  if (tu.order_tiles && p->strategy != RKF_STRATEGY_TILED && empty_order_source(c, p, tu, &order_obj) &&
+      (st = tile_order_prepare(c, segs, tile_w, tile_h, band_rows.data(),
+                               static_cast<uint32_t>(band_rows.size() - 1), &order_tbl, &ordered)) != RKF_OK)
+    return st;
+  const size_t sb = sizeof(Segment);
+  if (c->seg_buf.bytes < sb && (st = c->seg_buf.alloc(sb)) != RKF_OK) return st;
+  RKF_CUDA_TRY(cudaMemcpyAsync(c->seg_buf.p, segs.data(), sb, cudaMemcpyHostToDevice, c->stream));
+  if (ordered &&
+      (st = tile_order_enqueue(c, order_tbl, c->seg_buf.as<Segment>(), order_obj, c->empty_dist.as<uint8_t>(),
+                               order_reach(order_obj, p), order_obj.be * order_obj.min_scale, c->stream)) != RKF_OK)
+    return st;
+  RKF_CUDA_TRY(cudaEventRecord(c->segs_ev, c->stream));
+  RKF_CUDA_TRY(cudaStreamWaitEvent(c->band_stream, c->segs_ev, 0));
   // on an error, work already queued must finish before the caller's
   // buffers are handed back
   struct Drain {
@@ -132,12 +154,8 @@ rkf_status march_host_banded(Ctx* c, const rkf_camera* cam, const rkf_march_para
   } drain{c};
   // one counter per band, 64 bytes apart, past the counters other launches use
   unsigned long long* counters = reinterpret_cast<unsigned long long*>(c->counters.as<char>() + 1024);
-  uint32_t r0 = 0;
-  for (int b = 0; b < bands && r0 < rows; ++b) {
-    const uint32_t r1 = b == bands - 1 ? rows
-                                       : std::min(rows, static_cast<uint32_t>(
-                                                            (static_cast<uint64_t>(rows) * 2u * (b + 1)) / weight));
-    if (r1 <= r0) continue;
+  for (size_t b = 0; b + 1 < band_rows.size(); ++b) {
+    const uint32_t r0 = band_rows[b], r1 = band_rows[b + 1];
     cudaStream_t bs = (b & 1) ? c->band_stream : c->stream;
     st = launch_persistent(c, segs, (r1 - r0) * row_ids, p, tu, bs, &c->seg_buf, counters + 8 * b,
                            r0 * row_ids, true);
@@ -159,7 +177,6 @@ rkf_status march_host_banded(Ctx* c, const rkf_camera* cam, const rkf_march_para
     RKF_CUDA_TRY(cp(host.position, dev.position, 16));
     RKF_CUDA_TRY(cp(host.packed_material, dev.packed_material, 4));
     RKF_CUDA_TRY(cp(host.motion, dev.motion, 16));
-    r0 = r1;
   }
   RKF_CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
   RKF_CUDA_TRY(cudaStreamSynchronize(c->band_stream));
@@ -462,5 +479,42 @@ rkf_status rkf_march_batch_async(rkf_ctx* ctx, const rkf_view* views, uint32_t n
 }
 
 void rkf_testing_set_host_bands(int bands) { detail::g_host_bands.store(bands < 0 ? -1 : bands); }
+
+rkf_status rkf_scene_origin_set(rkf_ctx* ctx, const rkf_world_pos* origin) {
+  if (!ctx || !origin) return fail(RKF_INVALID_ARG, "rkf_scene_origin_set: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (c->serve) return fail(RKF_BUSY, "rkf_scene_origin_set: the context is serving");
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(origin->local[a])) return fail(RKF_INVALID_ARG, "rkf_scene_origin_set: non-finite offset");
+  c->origin = *origin;
+  return RKF_OK;
+}
+
+rkf_status rkf_scene_origin_get(rkf_ctx* ctx, rkf_world_pos* out) {
+  if (!ctx || !out) return fail(RKF_INVALID_ARG, "rkf_scene_origin_get: null argument");
+  *out = reinterpret_cast<Ctx*>(ctx)->origin;
+  return RKF_OK;
+}
+
+rkf_status rkf_march_world(rkf_ctx* ctx, const rkf_world_pos* cam_pos, const rkf_camera* cam,
+                           const rkf_march_params* p, uint32_t width, uint32_t height, rkf_gbuffer* out) {
+  if (!ctx || !cam_pos || !cam) return fail(RKF_INVALID_ARG, "rkf_march_world: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  rkf_camera rel = *cam;
+  float pos[3];
+  rkf_world_relative(cam_pos, &c->origin, nullptr, pos);
+  for (int a = 0; a < 3; ++a) rel.position[a] = pos[a];
+  return rkf_march(ctx, &rel, p, width, height, out);
+}
+
+rkf_status rkf_trace_rays_world(rkf_ctx* ctx, const rkf_world_pos* origins, const float* dirs,
+                                const float* tmax, uint32_t n, uint32_t mode, const rkf_march_params* p,
+                                rkf_hits* out) {
+  if (!ctx || (n && (!origins || !dirs || !tmax))) return fail(RKF_INVALID_ARG, "rkf_trace_rays_world: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  std::vector<float> rel(3ull * n);
+  for (uint32_t i = 0; i < n; ++i) rkf_world_relative(origins + i, &c->origin, nullptr, rel.data() + 3ull * i);
+  return rkf_trace_rays(ctx, rel.data(), dirs, tmax, n, mode, p, RKF_MEM_HOST, out);
+}
 
 }  // extern "C"

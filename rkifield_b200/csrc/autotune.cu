@@ -1,16 +1,17 @@
 // autotune.cu — pick the persistent march's launch tuning for a workload.
 //
-// The batched march has seven knobs that change speed but never results:
+// The batched march has eight knobs that change speed but never results:
 // the ray-tile shape that orders a view's work ids (the spatial coherence of
 // the rays a warp holds), the compaction interval (march iterations between
 // lane refills), the step budget (empty-space steps a lane runs before its
 // warp re-converges), the refill threshold (idle lanes that make a warp
 // refill), where a lane probes its next EMPTY cube (inside a run or between
-// runs), the block size and whether it runs EMPTY runs at all.  rkf_autotune times candidates on the caller's
+// runs), the block size, whether it runs EMPTY runs at all and whether views
+// hand out their heaviest ray tiles first.  rkf_autotune times candidates on the caller's
 // sample of the work with CUDA events: every tile x interval x block size at
 // the default budget and threshold, then every budget, then every threshold,
-// then the other probe placement, then the march without EMPTY runs, each
-// at the best so far.
+// then the other probe placement, then the heaviest-first tile order, then
+// the march without EMPTY runs, each at the best so far.
 // The fastest is kept in the context, where rkf_march and rkf_march_batch
 // use it.
 #include <cfloat>
@@ -87,6 +88,12 @@ extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t
     tu.probe_in_run = 1;
     trial(tu);
   }
+  // heaviest tiles first (views on the empty-space path)
+  if (st == RKF_OK && n_views) {
+    rkf_batch_tuning tu = best;
+    tu.order_tiles = 1;
+    trial(tu);
+  }
   // where EMPTY runs do not pay (a camera outside a dense grid: short runs,
   // probes that mostly fail), the full sampler alone is faster
   if (st == RKF_OK) {
@@ -100,5 +107,25 @@ extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t
   c->tuning = best;
   c->tuned = true;
   if (out) *out = best;
+  return RKF_OK;
+}
+
+extern "C" rkf_status rkf_tuning_set(rkf_ctx* ctx, const rkf_batch_tuning* tuning) {
+  if (!ctx || !tuning) return fail(RKF_INVALID_ARG, "rkf_tuning_set: null argument");
+  const rkf_batch_tuning& tu = *tuning;
+  const uint32_t threads = tu.threads_per_block ? tu.threads_per_block : 256;
+  if ((tu.tile_w == 0) != (tu.tile_h == 0) || tu.tile_w * tu.tile_h > 4096 || threads > 256 || threads % 32 ||
+      tu.refill_idle > 32 || tu.probe_in_run > 1 || tu.no_empty_path > 1 || tu.order_tiles > 1)
+    return fail(RKF_INVALID_ARG, "rkf_tuning_set: bad tuning");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (c->serve) return fail(RKF_BUSY, "rkf_tuning_set: the context is serving");
+  c->tuning = tu;
+  c->tuned = true;
+  return RKF_OK;
+}
+
+extern "C" rkf_status rkf_tuning_get(rkf_ctx* ctx, rkf_batch_tuning* out) {
+  if (!ctx || !out) return fail(RKF_INVALID_ARG, "rkf_tuning_get: null argument");
+  *out = reinterpret_cast<Ctx*>(ctx)->tuning;
   return RKF_OK;
 }

@@ -279,12 +279,19 @@ rkf_status lookup_bricks(Ctx* c, uint32_t obj, const uint32_t* d_bxyz, uint32_t 
   return RKF_OK;
 }
 
-// Band-normalised signed u8 code of one brick: step = range/127 with range the
-// largest finite |d| in the brick; |code| = min(floor(|d|/step), 127), less one
-// when the decoded product code*step would round above |d|, so a decoded |d|
-// never exceeds the stored one (sphere tracing never overshoots).
+// Band-normalised signed u8 code of one brick.  The brick's band is
+// B = min(band, largest finite |d| in the brick) -- band is the narrow band's
+// half-width (3 voxels for a voxelized object), so B / band is the brick's
+// scale s_b <= 1 -- and step = B/127.  |code| = min(floor(|d|/step), 127),
+// rounding toward zero and clamping |d| to B, less one when the decoded
+// product code*step would round above |d|: a decoded |d| never exceeds the
+// true one (sphere tracing never overshoots).  band = +inf: B is the brick's
+// largest |d|.  nearest: |code| = min(rint(|d|/step), 127) instead -- each
+// code within half a step of |d| (clamped to B), errors of either sign, so
+// they do not add up along a ray's steps the way a one-sided bias does.
 __global__ void k_encode_u8(const float* __restrict__ src_f32, const uint16_t* __restrict__ src_f16,
-                            uint32_t first_slot, uint32_t n_bricks, int8_t* code, float* step) {
+                            uint32_t first_slot, uint32_t n_bricks, int8_t* code, float* step, float band,
+                            bool nearest) {
   const uint32_t b = blockIdx.x;
   if (b >= n_bricks) return;
   const uint64_t base = (static_cast<uint64_t>(first_slot) + b) * 512;
@@ -301,17 +308,18 @@ __global__ void k_encode_u8(const float* __restrict__ src_f32, const uint16_t* _
     if (threadIdx.x < s) red[threadIdx.x] = fmaxf(red[threadIdx.x], red[threadIdx.x + s]);
     __syncthreads();
   }
-  const float range = fmaxf(red[0], 1e-6f);
+  const float range = fmaxf(fminf(red[0], band), 1e-6f);
   const float st = __fdiv_rn(range, 127.0f);
   if (threadIdx.x == 0) step[first_slot + b] = st;
   for (int i = threadIdx.x; i < 512; i += blockDim.x) {
     const float d = src_f32 ? src_f32[base + i] : __half2float(__ushort_as_half(src_f16[base + i]));
     const float a = fabsf(d);
-    const float q = floorf(__fdiv_rn(a, st));
+    const float qa = __fdiv_rn(a, st);
+    const float q = nearest ? rintf(qa) : floorf(qa);
     int c = q >= 127.0f ? 127 : static_cast<int>(q);
-    // the decoder's product RN(c*step) must not exceed |d| (the quotient
-    // may round up to the next integer)
-    if (c > 0 && __fmul_rn(static_cast<float>(c), st) > a) --c;
+    // toward zero: the decoder's product RN(c*step) must not exceed |d| (the
+    // quotient may round up to the next integer)
+    if (!nearest && c > 0 && __fmul_rn(static_cast<float>(c), st) > a) --c;
     code[base + i] = static_cast<int8_t>(d < 0.0f ? -c : c);
   }
 }
@@ -353,6 +361,7 @@ void rkf_config_default(rkf_config* cfg) {
 rkf_status rkf_create(const rkf_config* cfg, rkf_ctx** out) {
   if (!cfg || !out) return fail(RKF_INVALID_ARG, "rkf_create: null argument");
   if (cfg->precision > RKF_PRECISION_U8) return fail(RKF_INVALID_ARG, "rkf_create: bad precision");
+  if (!(cfg->u8_band >= 0.0f) || cfg->u8_round > 1) return fail(RKF_INVALID_ARG, "rkf_create: bad u8 encoding");
   if (cfg->pool_capacity_bricks == 0 || cfg->pool_capacity_bricks > (RKF_INTERIOR_SLOT - 1))
     return fail(RKF_INVALID_ARG, "rkf_create: pool_capacity_bricks out of range");
   int ndev = 0;
@@ -423,8 +432,12 @@ namespace {
 // encoding when the context stores codes, then the slots leave the free list.
 rkf_status finish_pool_import(Ctx* c, uint32_t first_slot, uint32_t n_bricks) {
   if (c->cfg.precision == RKF_PRECISION_U8) {
+    // the pool does not know the voxel size of its bricks: the configured
+    // band, else each brick's own largest |d|
+    const float band = c->cfg.u8_band > 0.0f ? c->cfg.u8_band : INFINITY;
     k_encode_u8<<<n_bricks, 256, 0, c->stream>>>(nullptr, c->dist_f16.as<uint16_t>(), first_slot, n_bricks,
-                                                 c->dist_u8.as<int8_t>(), c->brick_step.as<float>());
+                                                 c->dist_u8.as<int8_t>(), c->brick_step.as<float>(), band,
+                                                 c->cfg.u8_round == 1);
     RKF_CUDA_TRY(cudaGetLastError());
   }
   RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -601,6 +614,7 @@ rkf_status rkf_objects_import(rkf_ctx* ctx, const rkf_gpu_object* objects, uint3
   std::swap(c->leaves.bytes, nleaves.bytes);
   c->leaf_cap = cap;
   c->n_leaves = nl;
+  c->free_leaves.clear();
   std::swap(c->top.p, ntop.p);
   std::swap(c->top.bytes, ntop.bytes);
   std::swap(c->empty_dist.p, nfield.p);

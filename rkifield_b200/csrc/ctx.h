@@ -91,6 +91,7 @@ struct Ctx {
   DevBuf empty_dist;  // u8 per top cell: empty-space distance field (empty_dist.h)
   DevBuf leaves;
   uint32_t n_leaves = 0, leaf_cap = 0;
+  std::vector<uint32_t> free_leaves;  // leaf numbers below n_leaves that no epoch references
   bool leaves_frozen = false;  // set while serving: the leaf buffer must not move
 
   // tiled strategy (tiled.h): coarse field (rebuilt when epoch changes) and tile lists
@@ -118,6 +119,7 @@ struct Ctx {
   DevBuf objdev;
 
   uint64_t epoch = 0;
+  rkf_world_pos origin{};  // WorldPosition the scene's f32 world space is relative to
 
   // scratch reused by march calls (host-pointer outputs staged here)
   DevBuf stage;
@@ -129,6 +131,7 @@ struct Ctx {
   cudaStream_t band_stream = nullptr;  // the second band stream; the first is `stream`
   cudaEvent_t band_ev[kMaxBands] = {};
   cudaEvent_t segs_ev = nullptr;
+  DevBuf order_buf;  // heaviest-first tile order of views (tile_order.h)
   DevBuf counters;   // work counters of the persistent kernels
   DevBuf seg_buf;    // segment table of the persistent kernel
   DevBuf l2_flush;

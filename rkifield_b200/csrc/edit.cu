@@ -14,8 +14,8 @@
 // Copy-on-write: every touched brick is written to a fresh pool slot and a
 // new epoch of the two-level index (a copy of the top grid plus new leaves
 // for the touched blocks) points at the new slots.  Work launched on the old
-// epoch keeps reading the old slots, which return to the free list once no
-// work holds that epoch.
+// epoch keeps reading the old slots and leaves, which return to their free
+// lists once no work holds that epoch.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -211,6 +211,7 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   out->new_epoch = false;
   out->new_top.release();
   out->retired.clear();
+  out->retired_leaves.clear();
   if (op.object_index >= c->obj_count()) return fail(RKF_INVALID_ARG, "rkf_edit_csg: object index out of range");
   if (op.edit_type > 4 || op.shape_type > 2 || op.falloff > 2)
     return fail(RKF_INVALID_ARG, "rkf_edit_csg: unsupported edit, shape or falloff type");
@@ -294,12 +295,15 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   // slots nothing references).
   const size_t free_kept = c->free_slots.size();
   const uint32_t used0 = c->used_slots, leaves0 = c->n_leaves;
+  const std::vector<uint32_t> free_leaves0 = c->free_leaves;
   Rollback undo([&] {
     c->free_slots.resize(free_kept);
     for (size_t i = dst.size(); i-- > 0;) c->free_slots.push_back(dst[i]);
     c->used_slots = used0;
     c->n_leaves = leaves0;
+    c->free_leaves = free_leaves0;
     out->retired.clear();
+    out->retired_leaves.clear();
     out->changed_bricks = 0;
     out->new_top.release();
     out->new_empty_dist.release();
@@ -365,7 +369,19 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
     if (it == blocks.end()) blocks.push_back(blk);
   }
   const uint32_t nb = static_cast<uint32_t>(blocks.size());
-  if ((s2 = c->ensure_leaf_capacity(c->n_leaves + nb)) != RKF_OK) return s2;
+  // leaf numbers of the new epoch's touched blocks: freed leaves first (the
+  // last freed on top), then new ones after n_leaves
+  std::vector<uint32_t> newtop(nb);
+  uint32_t appended = 0;
+  for (uint32_t i = 0; i < nb; ++i) {
+    if (!c->free_leaves.empty()) {
+      newtop[i] = c->free_leaves.back();
+      c->free_leaves.pop_back();
+    } else {
+      newtop[i] = c->n_leaves + appended++;
+    }
+  }
+  if ((s2 = c->ensure_leaf_capacity(c->n_leaves + appended)) != RKF_OK) return s2;
   Temp g;
   if ((s2 = g.get(scratch, static_cast<size_t>(nb) * (4 + 4 + 2048) + 256)) != RKF_OK) return s2;
   uint32_t* d_blocks = g.as<uint32_t>();
@@ -375,18 +391,27 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   detail::k_gather_blocks<<<nb, 128, 0, st>>>(c->top.as<uint32_t>(), c->leaves.as<uint32_t>(), d_blocks, nb,
                                               d_topv, d_leafs);
   RKF_CUDA_TRY(cudaGetLastError());
-  std::vector<uint32_t> leafv(static_cast<size_t>(nb) * 512);
+  std::vector<uint32_t> leafv(static_cast<size_t>(nb) * 512), oldtop(nb);
   RKF_CUDA_TRY(cudaMemcpyAsync(leafv.data(), d_leafs, leafv.size() * 4, cudaMemcpyDeviceToHost, st));
+  RKF_CUDA_TRY(cudaMemcpyAsync(oldtop.data(), d_topv, nb * 4ull, cudaMemcpyDeviceToHost, st));
   RKF_CUDA_TRY(cudaStreamSynchronize(st));
+  // the leaves these blocks pointed at belong to the old epoch only
+  for (uint32_t i = 0; i < nb; ++i)
+    if (oldtop[i] < RKF_INTERIOR_SLOT) out->retired_leaves.push_back(oldtop[i]);
   for (size_t i = 0; i < ch_brick.size(); ++i) {
     const uint32_t* b = &bxyz[3 * ch_brick[i]];
     leafv[static_cast<size_t>(local_of[i]) * 512 + (b[0] & 7) + (b[1] & 7) * 8 + (b[2] & 7) * 64] = ch_slot[i];
   }
-  // new leaves appended; a new top grid points the touched blocks at them
-  std::vector<uint32_t> newtop(nb);
-  for (uint32_t i = 0; i < nb; ++i) newtop[i] = c->n_leaves + i;
-  RKF_CUDA_TRY(cudaMemcpyAsync(c->leaves.as<uint32_t>() + static_cast<size_t>(c->n_leaves) * 512, leafv.data(),
-                               leafv.size() * 4, cudaMemcpyHostToDevice, st));
+  // the new leaves (runs of consecutive numbers in one copy each); a new top
+  // grid points the touched blocks at them
+  for (uint32_t i = 0; i < nb;) {
+    uint32_t j = i + 1;
+    while (j < nb && newtop[j] == newtop[j - 1] + 1) ++j;
+    RKF_CUDA_TRY(cudaMemcpyAsync(c->leaves.as<uint32_t>() + static_cast<size_t>(newtop[i]) * 512,
+                                 leafv.data() + static_cast<size_t>(i) * 512, static_cast<size_t>(j - i) * 2048,
+                                 cudaMemcpyHostToDevice, st));
+    i = j;
+  }
   const bool into = out->top_dst && out->field_dst;
   if (!into && (s2 = out->new_top.alloc(std::max<uint64_t>(c->top_len, 1) * 4)) != RKF_OK) return s2;
   uint32_t* ntop = into ? out->top_dst : out->new_top.as<uint32_t>();
@@ -399,7 +424,7 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   uint8_t* nfield = into ? out->field_dst : out->new_empty_dist.as<uint8_t>();
   RKF_CUDA_TRY(cudaMemcpyAsync(nfield, c->empty_dist.p, c->top_len, cudaMemcpyDeviceToDevice, st));
   if ((s2 = lower_empty_dist(od, nfield, d_blocks, blocks, st)) != RKF_OK) return s2;
-  c->n_leaves += nb;
+  c->n_leaves += appended;
   // the reference flat map (read only by the plain march) is updated in place
   if (od.has_flat && !c->flat_host.empty()) {
     for (size_t i = 0; i < ch_brick.size(); ++i) {
@@ -437,6 +462,7 @@ extern "C" rkf_status rkf_edit_csg(rkf_ctx* ctx, const rkf_edit_op* op, uint64_t
     std::swap(c->empty_dist.bytes, r.new_empty_dist.bytes);
     c->epoch++;
     for (uint32_t s : r.retired) c->free_slots.push_back(s);
+    for (uint32_t l : r.retired_leaves) c->free_leaves.push_back(l);
   }
   if (new_epoch) *new_epoch = c->epoch;
   return RKF_OK;

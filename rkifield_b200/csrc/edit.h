@@ -14,6 +14,7 @@ struct EditOutcome {
   DevBuf new_top;                 // top grid of the new epoch (unless written to top_dst)
   DevBuf new_empty_dist;          // its empty-space distance field (unless field_dst)
   std::vector<uint32_t> retired;  // slots the new epoch no longer references
+  std::vector<uint32_t> retired_leaves;  // index leaves the new epoch no longer references
   // optional caller memory for the new epoch (top_len u32 / top_len bytes);
   // when both are set nothing is allocated for it
   uint32_t* top_dst = nullptr;
@@ -25,8 +26,9 @@ struct EditOutcome {
 using EditScratch = std::function<void*(size_t bytes)>;
 
 // Applies one edit; on success with changed bricks, out->new_top holds the
-// new epoch's top grid (the caller publishes it) and out->retired the slots
-// to free once no work reads the previous epoch.  Synchronises `st`.  With
+// new epoch's top grid (the caller publishes it), out->retired the slots and
+// out->retired_leaves the leaves to free once no work reads the previous
+// epoch.  New leaves reuse freed leaf numbers (Ctx::free_leaves) first.  Synchronises `st`.  With
 // scratch, the temporaries come from it instead of device allocations (whose
 // release would wait for every stream of the device).
 rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcome* out,

@@ -19,6 +19,7 @@ struct Segment {
   float pos[3], fwd[3], right[3], up[3], jitter[2];
   float coarse_ocr[3];                // coarse field origin relative to the camera (tiled strategy)
   uint32_t _pad;
+  const uint32_t* tile_perm;          // view: the tile handed out at each position (null: row order)
   float prev_vp[16];
   const float* origins;
   const float* dirs;
@@ -60,6 +61,12 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
                                      const rkf_march_params* p, const rkf_batch_tuning& tu,
                                      cudaStream_t st, Segment* dev_segs, unsigned long long* dev_counter,
                                      bool segs_uploaded = false, bool multi_empty = false);
+// Whether a launch over this context's objects with these parameters marches
+// the empty-space path (the condition for ordering its views' tiles), and
+// the object whose empty-space field it reads.
+bool empty_order_source(const Ctx* c, const rkf_march_params* p, const rkf_batch_tuning& tu, ObjDev* o);
+// Distance the tile-order estimate walks along a ray.
+float order_reach(const ObjDev& o, const rkf_march_params* p);
 rkf_status launch_trace_plain(Ctx* c, const float* o, const float* d, const float* tmax, uint32_t n,
                               uint32_t mode, const rkf_march_params* p, const rkf_hits& out,
                               cudaStream_t st);

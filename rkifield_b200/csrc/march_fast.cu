@@ -31,6 +31,7 @@
 #include "f32x2.cuh"
 #include "sampler.cuh"
 #include "tiled.h"
+#include "tile_order.h"
 
 namespace rkf {
 
@@ -570,7 +571,8 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
             bool valid = true;
             if (sg.kind == 0) {  // view: tile-ordered pixel ids
               const uint32_t per = kp.tile_w * kp.tile_h;
-              const uint32_t tile = static_cast<uint32_t>(local / per);
+              uint32_t tile = static_cast<uint32_t>(local / per);
+              if (sg.tile_perm) tile = __ldg(sg.tile_perm + tile);  // heaviest-first order
               const uint32_t r = static_cast<uint32_t>(local % per);
               const uint32_t px = (tile % sg.tiles_x) * kp.tile_w + r % kp.tile_w;
               const uint32_t py = (tile / sg.tiles_x) * kp.tile_h + r / kp.tile_w;
@@ -1300,6 +1302,31 @@ int object_set(const Ctx* c) {
 }
 }  // namespace
 
+bool empty_order_source(const Ctx* c, const rkf_march_params* p, const rkf_batch_tuning& tu, ObjDev* o) {
+  if (tu.no_empty_path || p->strategy == RKF_STRATEGY_TILED || c->obj_count() == 0 ||
+      c->obj_count() > kMaxObjectsFast)
+    return false;
+  const bool use_bvh = p->strategy == RKF_STRATEGY_BVH;
+  const int objs = object_set(c);
+  if (objs == detail::OBJ_SINGLE_EMPTY) {
+    if (use_bvh && !c->bvh_one_leaf0) return false;
+    *o = c->objdev_host[0];
+    return true;
+  }
+  if (objs == detail::OBJ_MULTI_EMPTY) {
+    uint32_t vi = 0;
+    multi_empty_scene(c, &vi, nullptr, nullptr);
+    if (use_bvh && !bvh_reaches(c, vi)) return false;
+    *o = c->objdev_host[vi];
+    return true;
+  }
+  return false;
+}
+
+float order_reach(const ObjDev& o, const rkf_march_params* p) {
+  return std::min(p->scene.max_distance, static_cast<float>(p->hard_max_steps) * o.be * o.min_scale);
+}
+
 rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint64_t total,
                              const rkf_march_params* p, const rkf_batch_tuning& tu,
                              cudaStream_t st, DevBuf* seg_buf, unsigned long long* counter, uint64_t id0,
@@ -1328,7 +1355,18 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
         (s2 = prepare_tiled_empty(c, st, vi)) != RKF_OK)
       return s2;
   }
-  const std::vector<Segment>& segs_dev = tiled ? tiled_segs : segs_host;
+  // heaviest-first order of the views' tiles (a whole launch only: a band of
+  // a view is ordered by its caller, which plans all bands at once)
+  ObjDev order_obj;
+  OrderTable order_tbl;
+  bool ordered = false;
+  std::vector<Segment> ordered_segs;
+  if (tu.order_tiles && id0 == 0 && !segs_resident && !tiled && empty_order_source(c, p, tu, &order_obj)) {
+    ordered_segs = segs_host;
+    rkf_status s2 = tile_order_prepare(c, ordered_segs, tu.tile_w, tu.tile_h, nullptr, 0, &order_tbl, &ordered);
+    if (s2 != RKF_OK) return s2;
+  }
+  const std::vector<Segment>& segs_dev = tiled ? tiled_segs : (ordered ? ordered_segs : segs_host);
   const size_t sb = segs_dev.size() * sizeof(Segment);
   if (!segs_resident || seg_buf->bytes < sb) {
     if (seg_buf->bytes < sb) {
@@ -1337,6 +1375,11 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
     }
     // a pageable source: the call returns once the stream has taken the data
     RKF_CUDA_TRY(cudaMemcpyAsync(seg_buf->p, segs_dev.data(), sb, cudaMemcpyHostToDevice, st));
+  }
+  if (ordered) {
+    rkf_status s2 = tile_order_enqueue(c, order_tbl, seg_buf->as<Segment>(), order_obj, c->empty_dist.as<uint8_t>(),
+                                       order_reach(order_obj, p), order_obj.be * order_obj.min_scale, st);
+    if (s2 != RKF_OK) return s2;
   }
   RKF_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
   detail::KParams kp;

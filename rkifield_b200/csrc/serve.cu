@@ -14,15 +14,21 @@
 // Edits run in admission order: requests admitted before an edit are launched
 // before it and read the old epoch of the brick index; requests admitted
 // after it read the new one.  Edits are copy-on-write (edit.cu), so in-flight
-// ticks are never disturbed.  During a session retired brick slots are not
-// reused (they return to the pool at rkf_serve_stop), which keeps slot numbers
-// -- and so every output -- a function of the request and its epoch alone.
+// ticks are never disturbed.  The brick slots and index leaves an edit
+// retires (the ones only older epochs reference) go back to their free lists
+// two edits later: when the edit that creates epoch E + 2 starts, the slots
+// and leaves retired at the creation of epoch E are reused, once every tick of
+// an epoch before E has completed.  That point is fixed by the order of the
+// edits alone, so slot numbers -- and so every output -- stay a function of
+// the request and its epoch, and a session with an edit every few requests
+// keeps its pool and leaf use bounded (brick_pool.rs:54,136 deallocate).
 #include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <map>
 #include <unordered_map>
 
+#include "../../include/rkf_cuda_testing.h"
 #include "ctx.h"
 #include "edit.h"
 #include "march.h"
@@ -181,7 +187,13 @@ struct ServeState {
   std::vector<std::pair<DevBuf*, DevBuf*>> spares;
   std::vector<std::pair<uint64_t, std::pair<DevBuf*, DevBuf*>>> retiring;
   void recycle();
-  std::vector<uint32_t> retired;
+  // slots and leaves retired at the creation of `epoch`, not yet reusable
+  struct Retired {
+    uint64_t epoch;
+    std::vector<uint32_t> slots, leaves;
+  };
+  std::deque<Retired> retired_q;
+  void reclaim();
   rkf_status error = RKF_OK;
   std::string error_msg;
 
@@ -191,6 +203,21 @@ struct ServeState {
   void poll_ticks();
 };
 
+// Returns to the free lists the slots and leaves retired at the creation of
+// epochs up to c->epoch - 1, i.e. two or more edits before the one about to
+// run (which would create c->epoch + 1), after waiting for the ticks of the
+// epochs that read them.
+void ServeState::reclaim() {
+  while (!retired_q.empty() && retired_q.front().epoch + 1 <= c->epoch) {
+    const Retired& r = retired_q.front();
+    for (const Tick& t : ticks)
+      if (t.epoch < r.epoch) cudaEventSynchronize(t.ev1);
+    for (uint32_t slot : r.slots) c->free_slots.push_back(slot);
+    for (uint32_t leaf : r.leaves) c->free_leaves.push_back(leaf);
+    retired_q.pop_front();
+  }
+}
+
 void ServeState::do_edit(uint64_t id) {
   rkf_edit_op op;
   {
@@ -199,6 +226,7 @@ void ServeState::do_edit(uint64_t id) {
     tickets[id].res.start_us = now_us(t0);
     tickets[id].state = 1;
   }
+  reclaim();
   EditOutcome out;
   std::pair<DevBuf*, DevBuf*> spare{nullptr, nullptr};
   if (!spares.empty()) {
@@ -227,8 +255,8 @@ void ServeState::do_edit(uint64_t id) {
     std::swap(c->empty_dist.bytes, spare.second->bytes);
     retiring.push_back({c->epoch, spare});
     spare = {nullptr, nullptr};
-    retired.insert(retired.end(), out.retired.begin(), out.retired.end());
     c->epoch++;
+    retired_q.push_back({c->epoch, out.retired, out.retired_leaves});
   } else if (st == RKF_OK && out.new_epoch) {
     DevBuf* old = new DevBuf();
     std::swap(old->p, c->top.p);
@@ -242,8 +270,8 @@ void ServeState::do_edit(uint64_t id) {
     std::swap(c->empty_dist.p, out.new_empty_dist.p);
     std::swap(c->empty_dist.bytes, out.new_empty_dist.bytes);
     old_tops.push_back(old_field);
-    retired.insert(retired.end(), out.retired.begin(), out.retired.end());
     c->epoch++;
+    retired_q.push_back({c->epoch, out.retired, out.retired_leaves});
   }
   if (spare.first) spares.push_back(spare);  // unused: no new epoch
   std::lock_guard<std::mutex> lk(mu);
@@ -584,8 +612,12 @@ rkf_status rkf_serve_stop(rkf_ctx* ctx) {
     delete r.second.first;
     delete r.second.second;
   }
-  for (uint32_t slot : s->retired) c->free_slots.push_back(slot);
-  c->used_slots -= static_cast<uint32_t>(s->retired.size());
+  // every stream is idle: what is still held is free now (apply_edit already
+  // took retired slots out of used_slots)
+  for (const ServeState::Retired& r : s->retired_q) {
+    for (uint32_t slot : r.slots) c->free_slots.push_back(slot);
+    for (uint32_t leaf : r.leaves) c->free_leaves.push_back(leaf);
+  }
   c->leaves_frozen = false;
   c->serve = nullptr;
   delete s;
@@ -680,3 +712,14 @@ rkf_status rkf_cancel(rkf_ctx* ctx, rkf_ticket ticket) {
 }
 
 }  // extern "C"
+
+extern "C" rkf_status rkf_testing_pool_state(rkf_ctx* ctx, uint32_t out[5]) {
+  if (!ctx || !out) return fail(RKF_INVALID_ARG, "rkf_testing_pool_state: null argument");
+  const Ctx* c = reinterpret_cast<const Ctx*>(ctx);
+  out[0] = c->capacity;
+  out[1] = c->used_slots;
+  out[2] = static_cast<uint32_t>(c->free_slots.size());
+  out[3] = c->n_leaves;
+  out[4] = static_cast<uint32_t>(c->free_leaves.size());
+  return RKF_OK;
+}

@@ -239,7 +239,8 @@ __global__ void k_scatter(const float* __restrict__ dist, const uint16_t* __rest
 
 // u8 encoder (ctx.cu)
 __global__ void k_encode_u8(const float* __restrict__ src_f32, const uint16_t* __restrict__ src_f16,
-                            uint32_t first_slot, uint32_t n_bricks, int8_t* code, float* step);
+                            uint32_t first_slot, uint32_t n_bricks, int8_t* code, float* step, float band,
+                            bool nearest);
 
 }  // namespace rkf
 
@@ -465,12 +466,15 @@ extern "C" rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, ui
                                                 d_cidx.as<uint32_t>(), d_slots.as<uint32_t>(), n_alloc, nullptr,
                                                 tmp.as<float>(), c->mat.as<uint16_t>(), c->blend.as<uint8_t>(), nullptr);
       RKF_CUDA_TRY(cudaGetLastError());
+      // the codes cover the narrow band: +-3 voxels unless configured
+      const float band = c->cfg.u8_band > 0.0f ? c->cfg.u8_band : 3.0f * g.vs;
       // slots of one voxelization are not necessarily contiguous: encode per slot
       for (uint32_t i = 0; i < n_alloc;) {
         uint32_t j = i + 1;
         while (j < n_alloc && slots[j] == slots[j - 1] + 1) ++j;
         k_encode_u8<<<j - i, 256, 0, c->stream>>>(tmp.as<float>(), nullptr, slots[i], j - i,
-                                                  c->dist_u8.as<int8_t>(), c->brick_step.as<float>());
+                                                  c->dist_u8.as<int8_t>(), c->brick_step.as<float>(), band,
+                                                  c->cfg.u8_round == 1);
         RKF_CUDA_TRY(cudaGetLastError());
         i = j;
       }

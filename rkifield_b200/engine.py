@@ -74,7 +74,7 @@ class Context:
 
     def __init__(self, device: int = 0, pool_capacity: int = 1 << 16, precision: str = "f16",
                  keep_reference_pool: bool = True, max_inflight: int = 64,
-                 mem_budget_bytes: int = 0):
+                 mem_budget_bytes: int = 0, u8_round: int = 0, u8_band: float = 0.0):
         self.lib = abi.load_library()
         cfg = abi.rkf_config()
         self.lib.rkf_config_default(C.byref(cfg))
@@ -84,6 +84,8 @@ class Context:
         cfg.keep_reference_pool = int(keep_reference_pool)
         cfg.max_inflight = max_inflight
         cfg.mem_budget_bytes = mem_budget_bytes
+        cfg.u8_round = u8_round
+        cfg.u8_band = u8_band
         h = C.c_void_p()
         check(self.lib.rkf_create(C.byref(cfg), C.byref(h)), "rkf_create")
         self.h = h
@@ -196,6 +198,15 @@ class Context:
         check(fn(self.h, C.byref(cam), C.byref(params), width, height, C.byref(g), stream_ptr),
               "rkf_march_async")
 
+    def set_tuning(self, tuning: abi.rkf_batch_tuning):
+        """The launch tuning of the context's marches (rkf_tuning_set)."""
+        check(self.lib.rkf_tuning_set(self.h, C.byref(tuning)), "rkf_tuning_set")
+
+    def tuning(self) -> abi.rkf_batch_tuning:
+        tu = abi.rkf_batch_tuning()
+        check(self.lib.rkf_tuning_get(self.h, C.byref(tu)), "rkf_tuning_get")
+        return tu
+
     def brick_lookup(self, obj: int, bxyz: np.ndarray) -> np.ndarray:
         bxyz = np.ascontiguousarray(bxyz, np.uint32)
         n = bxyz.size // 3
@@ -217,6 +228,49 @@ class Context:
         g = _gb_struct(dev_ptrs, abi.RKF_MEM_DEVICE)
         fn = self.lib.rkf_march_plain if plain else self.lib.rkf_march
         check(fn(self.h, C.byref(cam), C.byref(params), width, height, C.byref(g)), "march")
+
+    # -- WorldPosition cameras and rays (FP64 rebasing, world_position.rs) --
+    def set_scene_origin(self, chunk, local=(0.0, 0.0, 0.0)):
+        """The WorldPosition the scene's f32 world space is relative to."""
+        o = abi.rkf_world_pos()
+        o.chunk[:] = [int(x) for x in chunk]
+        o.local[:] = [float(x) for x in local]
+        check(self.lib.rkf_scene_origin_set(self.h, C.byref(o)), "rkf_scene_origin_set")
+
+    def march_world(self, cam_chunk, cam_local, cam, params, width: int, height: int,
+                    reference_planes: bool = False) -> dict:
+        """rkf_march with the camera at WorldPosition (cam_chunk, cam_local)."""
+        wp = abi.rkf_world_pos()
+        wp.chunk[:] = [int(x) for x in cam_chunk]
+        wp.local[:] = [float(x) for x in cam_local]
+        out = gbuffer_host(width * height, reference_planes)
+        g = _gb_struct(out)
+        check(self.lib.rkf_march_world(self.h, C.byref(wp), C.byref(cam), C.byref(params), width, height,
+                                       C.byref(g)), "rkf_march_world")
+        return out
+
+    def trace_world(self, chunks, locals_, dirs, tmax, mode: int, params) -> dict:
+        """rkf_trace_rays with origins given as WorldPositions (chunks int32
+        (n,3), local offsets float32 (n,3))."""
+        chunks = np.ascontiguousarray(chunks, np.int32).reshape(-1, 3)
+        locals_ = np.ascontiguousarray(locals_, np.float32).reshape(-1, 3)
+        n = chunks.shape[0]
+        wp = (abi.rkf_world_pos * max(1, n))()
+        buf = np.frombuffer(wp, dtype=np.dtype([("c", np.int32, 3), ("l", np.float32, 3)]), count=n)
+        buf["c"], buf["l"] = chunks, locals_
+        dirs = np.ascontiguousarray(dirs, np.float32).ravel()
+        tmax = np.ascontiguousarray(tmax, np.float32).ravel()
+        out = {"t": np.zeros(n, np.float32), "flags": np.zeros(n, np.uint16)}
+        if mode == abi.RKF_TRACE_CLOSEST:
+            out.update(normal=np.zeros(3 * n, np.float32), slot=np.zeros(n, np.uint32),
+                       material=np.zeros(n, np.uint16))
+        h = abi.rkf_hits()
+        h.t, h.flags = _p(out["t"]), _p(out["flags"])
+        h.normal, h.slot, h.material = _p(out.get("normal")), _p(out.get("slot")), _p(out.get("material"))
+        h.mem = abi.RKF_MEM_HOST
+        check(self.lib.rkf_trace_rays_world(self.h, wp, _p(dirs), _p(tmax), n, mode, C.byref(params), C.byref(h)),
+              "rkf_trace_rays_world")
+        return out
 
     # -- generic ray casts -------------------------------------------------
     def trace(self, origins, dirs, tmax, mode: int, params, closest_planes: bool = True) -> dict:

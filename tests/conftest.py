@@ -45,6 +45,44 @@ def small_ctx(small_scene):
     ctx.close()
 
 
+@pytest.fixture(scope="session")
+def large():
+    """The full-size workload: 512 seeded primitives in a 256 m cube voxelized
+    at 2 cm on the device (about 1.1 M bricks, two-level index), the headline
+    camera inside the grid and the march parameters of that scene."""
+    from rkifield_b200 import scenes
+    from rkifield_b200.engine import Context
+    spec = scenes.SCENE_LARGE
+    prims = scenes.make_prims(spec)
+    ctx = Context(pool_capacity=3_000_000, keep_reference_pool=False)
+    ctx.voxelize(prims, scenes.voxelize_params(spec, prims))
+    cam = scenes.seeded_camera(spec, 1920, 1080, seed=100, inside=True, distance=spec.cube * 0.18)
+    p = scenes.march_params(spec)
+    yield ctx, spec, cam, p
+    ctx.close()
+
+
+def oracle_scene_of(oracle, ctx, objects=None):
+    """An oracle scene reading the context's own pool planes and index (the
+    inputs the device march reads), with its objects."""
+    idx = ctx.export_index()
+    leaves = idx["leaves"]
+    live = leaves[leaves < 0xFFFFFFFE]
+    n = int(live.max()) + 1 if live.size else 1
+    pl = ctx.export_planes(0, n)
+    if objects is None:
+        objects = [ctx.object(i) for i in range(ctx.info()["num_objects"])]
+    return oracle.Scene(objects, top=idx["top"], leaves=leaves, obj_top_info=idx["obj_top_info"],
+                        dist_f16=pl["dist"], mat_plane=pl["mat"], blend_plane=pl["blend"])
+
+
+@pytest.fixture(scope="session")
+def large_oracle(oracle, large):
+    ctx = large[0]
+    assert ctx.info()["pool_bricks_used"] > 1_000_000
+    return oracle_scene_of(oracle, ctx, [ctx.object(0)])
+
+
 def assert_bits_equal(a: np.ndarray, b: np.ndarray, what: str):
     a = np.ascontiguousarray(a)
     b = np.ascontiguousarray(b)

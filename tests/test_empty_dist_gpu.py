@@ -145,3 +145,45 @@ def test_shadow_and_any_rays_bit_exact(oracle, small_scene, small_ctx):
         got = small_ctx.trace(o.ravel(), d.ravel(), tmax, mode, p)
         for k in ("t", "flags"):
             assert_bits_equal(got[k], ref[k], f"mode {mode} {k}")
+
+
+@pytest.mark.parametrize("bands", [0, 3])
+def test_inside_views_heaviest_tiles_first_bit_exact(oracle, small_scene, bands):
+    """The same inside views with the views' tiles handed out heaviest first
+    (rkf_batch_tuning.order_tiles): identical to the oracle through device
+    outputs and through host outputs marched in bands (each band ordered
+    among its own rows)."""
+    from rkifield_b200 import _abi as abi
+    from rkifield_b200 import cudart, scenes
+    from rkifield_b200.engine import Context
+    spec = small_scene["spec"]
+    v = small_scene["vox"]
+    sc = oracle.Scene([small_scene["obj"]], pool_words=v.words, brick_maps=v.map)
+    ctx = Context(pool_capacity=max(v.n_bricks + 4096, 1 << 15))
+    try:
+        ctx.set_brick_pool(v.words)
+        ctx.upload_brick_maps(v.map)
+        ctx.upload_objects([small_scene["obj"]])
+        tu = abi.rkf_batch_tuning()
+        tu.tile_w, tu.tile_h, tu.compact_interval, tu.order_tiles = 8, 4, 128, 1
+        ctx.set_tuning(tu)
+        assert ctx.tuning().order_tiles == 1
+        p = scenes.march_params(spec)
+        if bands:
+            ctx.lib.rkf_testing_set_host_bands(bands)
+        for seed in (21, 24):
+            w, h = 240, 136
+            cam = scenes.seeded_camera(spec, w, h, seed=seed, inside=True)
+            ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+            got = ctx.march(cam, p, w, h, reference_planes=True)
+            assert ctx.lib.rkf_testing_last_variant(ctx.h) == 2
+            for k in PLANES:
+                assert_bits_equal(got[k], ref[k], f"seed {seed} bands {bands} {k}")
+            if not bands:
+                g = cudart.device_gbuffer(w * h, reference_planes=True)
+                ctx.march_device(cam, p, w, h, cudart.gbuffer_ptrs(g))
+                for k in PLANES:
+                    assert_bits_equal(g[k].download(), ref[k], f"device outputs seed {seed} {k}")
+    finally:
+        ctx.lib.rkf_testing_set_host_bands(-1)
+        ctx.close()

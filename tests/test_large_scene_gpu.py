@@ -1,11 +1,10 @@
 """The full-size workload: 512 seeded primitives in a 256 m cube voxelized at
-2 cm on the device (about 1.1 M bricks), one 1920x1080 view from inside the
-grid.  Sampled rows are compared bit for bit with the FP32 oracle reading
-the same pool planes and index, and the whole frame is checked for
-properties that need no oracle: a repeat of the march is identical.  Ray
-batches whose tmax falls around the distance a ray covers in its step budget
-exercise both ways a miss can end (out of steps, or past tmax) where the march
-settles rays without stepping them."""
+2 cm on the device (about 1.1 M bricks), one view from inside the grid at
+1920x1080 and 960x540.  Whole frames are compared bit for bit with the FP32
+oracle reading the same pool planes and index, and a repeat of the march is
+identical.  Ray batches whose tmax falls around the distance a ray covers in
+its step budget exercise both ways a miss can end (out of steps, or past tmax)
+where the march settles rays without stepping them."""
 import numpy as np
 import pytest
 
@@ -17,45 +16,35 @@ PLANES = ("t", "normal", "slot", "material", "flags", "position", "packed_materi
 W, H = 1920, 1080
 
 
-@pytest.fixture(scope="module")
-def large():
+@pytest.mark.parametrize("w,h", [(1920, 1080), (960, 540)], ids=["1080p", "540p"])
+def test_large_view_full_frame_bit_exact(oracle, large, large_oracle, w, h):
+    """The headline view at both sizes, every pixel, every output plane,
+    against the FP32 oracle (all host threads) on the same planes and index."""
     from rkifield_b200 import scenes
-    from rkifield_b200.engine import Context
-    spec = scenes.SCENE_LARGE
-    prims = scenes.make_prims(spec)
-    ctx = Context(pool_capacity=3_000_000, keep_reference_pool=False)
-    ctx.voxelize(prims, scenes.voxelize_params(spec, prims))
-    cam = scenes.seeded_camera(spec, W, H, seed=100, inside=True, distance=spec.cube * 0.18)
-    p = scenes.march_params(spec)
-    yield ctx, spec, cam, p
-    ctx.close()
-
-
-@pytest.fixture(scope="module")
-def large_oracle(oracle, large):
-    ctx = large[0]
-    n = ctx.info()["pool_bricks_used"]
-    assert n > 1_000_000
-    pl = ctx.export_planes(0, n)
-    idx = ctx.export_index()
-    return oracle.Scene([ctx.object(0)], top=idx["top"], leaves=idx["leaves"], obj_top_info=idx["obj_top_info"],
-                        dist_f16=pl["dist"], mat_plane=pl["mat"], blend_plane=pl["blend"])
-
-
-def test_large_view_sampled_rows_bit_exact(oracle, large, large_oracle):
-    ctx, spec, cam, p = large
-    got = ctx.march(cam, p, W, H, reference_planes=True)
-    sc = large_oracle
-    rows = [0, 137, 389, 540, 541, 777, 1023, 1079]
-    hits = 0
-    for r in rows:
-        ref = oracle.march(sc, cam, p, W, H, rows=(r, r + 1), with_reference_planes=True)
-        hits += int((ref["flags"] & 1).sum())
-        for k in PLANES:
-            per = ref[k].size // W
-            assert_bits_equal(got[k].reshape(H, -1)[r], ref[k].reshape(1, -1)[0], f"row {r} {k}")
-            assert per >= 1
-    assert hits > 0
+    ctx, spec, _, p = large
+    cam = scenes.seeded_camera(spec, w, h, seed=100, inside=True, distance=spec.cube * 0.18)
+    got = ctx.march(cam, p, w, h, reference_planes=True)
+    ref = oracle.march(large_oracle, cam, p, w, h, with_reference_planes=True)
+    for k in PLANES:
+        assert_bits_equal(got[k], ref[k], f"{w}x{h} {k}")
+    flags = ref["flags"]
+    assert (flags & 1).sum() > 0.01 * w * h, "the view should hit geometry"
+    assert (flags & 4).sum() > 0.5 * w * h, "most rays should run out of steps in empty space"
+    # heaviest tiles first, one launch and in three bands of host outputs
+    from rkifield_b200 import _abi as abi
+    tu0 = ctx.tuning()
+    tu = abi.rkf_batch_tuning.from_buffer_copy(tu0)
+    tu.order_tiles = 1
+    try:
+        ctx.set_tuning(tu)
+        for bands in (1, 3):
+            ctx.lib.rkf_testing_set_host_bands(bands)
+            got = ctx.march(cam, p, w, h, reference_planes=True)
+            for k in PLANES:
+                assert_bits_equal(got[k], ref[k], f"{w}x{h} heaviest tiles first, {bands} bands, {k}")
+    finally:
+        ctx.lib.rkf_testing_set_host_bands(-1)
+        ctx.set_tuning(tu0)
 
 
 def test_large_view_repeat_identical(large):
@@ -112,8 +101,9 @@ def test_large_view_with_analytic_objects_rows_bit_exact(oracle, large):
     """The multi-object empty-space path at full size: analytic objects in
     front of the camera (spheres, a rotated and scaled box) and one far away,
     beside the voxelized object; EMPTY runs and settling chains stop at each
-    object's ball.  Sampled rows bit-exact against the oracle reading the same
-    planes and index.  The scene is restored afterwards."""
+    object's ball.  The whole frame (brute strategy) and sampled rows (tiled
+    strategy) bit-exact against the oracle reading the same planes and index.
+    The scene is restored afterwards."""
     from test_multi_empty_gpu import _rotation, _transformed
     from test_tiled_gpu import _analytic
     ctx, spec, cam, p = large
@@ -142,14 +132,12 @@ def test_large_view_with_analytic_objects_rows_bit_exact(oracle, large):
                           dist_f16=pl["dist"], mat_plane=pl["mat"], blend_plane=pl["blend"])
         got = ctx.march(cam, p, W, H, reference_planes=True)
         assert ctx.lib.rkf_testing_last_variant(ctx.h) == 4
-        prop_hits = 0
-        for r in (0, 389, 480, 540, 541, 777, 1079):
-            ref = oracle.march(sc, cam, p, W, H, rows=(r, r + 1), with_reference_planes=True)
-            for k in PLANES:
-                assert_bits_equal(got[k].reshape(H, -1)[r], ref[k].reshape(1, -1)[0], f"with objects, row {r} {k}")
-            hit = (ref["flags"] & 1) != 0
-            prop_hits += int((((ref["packed_material"][hit] >> 24) & 0xFF) >= 10).sum())
-        assert prop_hits > 0, "the sampled rows should see the analytic objects"
+        ref = oracle.march(sc, cam, p, W, H, with_reference_planes=True)
+        for k in PLANES:
+            assert_bits_equal(got[k], ref[k], f"with objects, full frame {k}")
+        hit = (ref["flags"] & 1) != 0
+        prop_hits = int((((ref["packed_material"][hit] >> 24) & 0xFF) >= 10).sum())
+        assert prop_hits > 0, "the view should see the analytic objects"
         # the same under the tiled strategy (EMPTY runs on the tiled empty-space field)
         from rkifield_b200 import _abi as abi, scenes
         pt = scenes.march_params(spec)
