@@ -69,6 +69,11 @@ def lib() -> C.CDLL:
         L.orc_voxelized_copy.argtypes = [P, P, P]
         L.orc_voxelized_copy_f32.argtypes = [P, P]
         L.orc_voxelized_free.argtypes = [P]
+        L.orc_voxelize_sparse.restype = P
+        L.orc_voxelize_sparse.argtypes = [P, U32, P, I]
+        L.orc_sparse_info.argtypes = [P, P, P, P, P, P]
+        L.orc_sparse_copy.argtypes = [P, P, P, P, P, P, P]
+        L.orc_sparse_free.argtypes = [P]
         L.orc_voxelize_bricks.argtypes = [P, U32, P, P, U32, P, P, I]
         L.orc_march.argtypes = [P, P, P, U32, U32, I, I, U32, U32] + [P] * 12 + [I, P]
         L.orc_trace_rays.argtypes = [P, P, P, P, U32, U32, P, I, I] + [P] * 7
@@ -150,6 +155,68 @@ class Voxelized:
                 o.geometry_aabb_min[a] = float(gmin[a])
                 o.geometry_aabb_max[a] = float(gmax[a])
         return o
+
+
+def _object_of(dims, voxel_size, alloc_bxyz, object_id):
+    """GpuObject of a voxelized grid (identity transform, unit scale) with the
+    tight AABB of its allocated bricks (brick_ops.rs:225-262)."""
+    o = abi.rkf_gpu_object()
+    for i in range(4):
+        o.inverse_world[i * 4 + i] = 1.0
+    vs = np.float32(voxel_size)
+    be = vs * np.float32(8.0)
+    gs = np.asarray(dims).astype(np.float32) * be
+    for a in range(3):
+        o.aabb_min[a] = float(-gs[a] * np.float32(0.5))
+        o.aabb_max[a] = float(gs[a] * np.float32(0.5))
+        o.brick_map_dims[a] = int(dims[a])
+    o.brick_map_offset = 0
+    o.voxel_size = float(vs)
+    o.sdf_type = abi.RKF_SDF_VOXELIZED
+    o.accumulated_scale[0] = o.accumulated_scale[1] = o.accumulated_scale[2] = 1.0
+    o.object_id = object_id
+    if len(alloc_bxyz):
+        lo = alloc_bxyz.min(axis=0).astype(np.float32)
+        hi = (alloc_bxyz.max(axis=0) + 1).astype(np.float32)
+        gmin = lo * be - gs * np.float32(0.5)
+        gmax = hi * be - gs * np.float32(0.5)
+        for a in range(3):
+            o.geometry_aabb_min[a] = float(gmin[a])
+            o.geometry_aabb_max[a] = float(gmax[a])
+    return o
+
+
+class SparseVoxelized:
+    """Oracle voxelization into a two-level index and SoA planes (no flat
+    map): the same slots and words as Voxelized, for grids whose flat map
+    would not fit host memory."""
+
+    def __init__(self, prims: np.ndarray, vp: abi.rkf_voxelize_params, threads: int | None = None):
+        L = lib()
+        h = L.orc_voxelize_sparse(ptr(prims), len(prims), C.byref(vp), threads or nthreads())
+        self.dims = np.zeros(3, np.uint32)
+        self.tdim = np.zeros(3, np.uint32)
+        nb, ni, nl = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        L.orc_sparse_info(h, ptr(self.dims), ptr(self.tdim), C.byref(nb), C.byref(ni), C.byref(nl))
+        self.n_bricks, self.n_interior, self.n_leaves = nb.value, ni.value, nl.value
+        self.top = np.zeros(int(self.tdim.astype(np.int64).prod()), np.uint32)
+        self.leaves = np.zeros(max(1, self.n_leaves) * 512, np.uint32)
+        self.dist_f16 = np.zeros(self.n_bricks * 512, np.uint16)
+        self.mat = np.zeros(self.n_bricks * 512, np.uint16)
+        self.blend = np.zeros(self.n_bricks * 512, np.uint8)
+        self.bxyz = np.zeros((self.n_bricks, 3), np.uint32)
+        L.orc_sparse_copy(h, ptr(self.top), ptr(self.leaves), ptr(self.dist_f16), ptr(self.mat), ptr(self.blend),
+                          ptr(self.bxyz))
+        L.orc_sparse_free(h)
+        self.voxel_size = vp.voxel_size
+        self.obj_top_info = np.array([0, *self.tdim], np.uint32)
+
+    def gpu_object(self, object_id: int = 1) -> abi.rkf_gpu_object:
+        return _object_of(self.dims, self.voxel_size, self.bxyz, object_id)
+
+    def scene(self, object_id: int = 1) -> "Scene":
+        return Scene([self.gpu_object(object_id)], top=self.top, leaves=self.leaves, obj_top_info=self.obj_top_info,
+                     dist_f16=self.dist_f16, mat_plane=self.mat, blend_plane=self.blend)
 
 
 class Scene:

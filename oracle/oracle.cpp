@@ -1289,7 +1289,7 @@ orc_sparse* orc_voxelize_sparse(const rkf_prim* prims, uint32_t n_prims, const r
   auto* v = new orc_sparse;
   v->g = make_grid(vp);
   const Grid& g = v->g;
-  const uint64_t dx = g.dims[0], dy = g.dims[1], dz = g.dims[2];
+  const uint64_t dx = g.dims[0], dy = g.dims[1];
   // 1. bricks some primitive's candidate test reaches (brick_candidates)
   std::vector<std::vector<uint64_t>> per(n_prims);
   parallel_for(n_prims, threads, [&](uint64_t i, int) {

@@ -473,9 +473,34 @@ __device__ __forceinline__ uint32_t empty_run(const ObjDev& o, const uint8_t* __
   return c;
 }
 
-// empty_run<PLAIN=true, CLEAN=true> with the x and y chains of a step packed
-// into two-wide FP32 instructions (z stays scalar): the same operations on
-// the same values, so the same bits.
+// The EMPTY value of a plain object (zero translation, unit scale) at the
+// ray's position at t: empty_run<PLAIN=true>'s step with the x and y chains
+// packed into two-wide FP32 instructions (z stays scalar) -- the same
+// operations on the same values, so the same bits.
+__device__ __forceinline__ float empty_value_x2(f2 o01, f2 d01, f2 h01, f2 r2, f2 nvs2, f2 half2, float oz, float dz,
+                                                float hz, float vs, float rcp, float be, float t) {
+  const f2 g01 = f2_add(f2_add(o01, f2_mul(d01, f2_pack(t, t))), h01);
+  const f2 q0 = f2_mul(g01, r2);
+  const f2 v01 = f2_sub(f2_fma(f2_fma(q0, nvs2, g01), r2, q0), half2);
+  const float vz = __fsub_rn(exact_div_vs(__fadd_rn(__fadd_rn(oz, __fmul_rn(dz, t)), hz), vs, rcp), 0.5f);
+  float vx, vy;
+  f2_unpack(v01, vx, vy);
+  float tx, ty;
+  f2_unpack(f2_sub(v01, f2_pack(floorf(vx), floorf(vy))), tx, ty);
+  return mix3_const(be, tx, ty, __fsub_rn(vz, floorf(vz)));
+}
+
+// empty_run<PLAIN=true, CLEAN=true> four steps at a time.  Each step is
+// t' = t + E(t), a chain in which every step waits for the last.  E(t)
+// equals the brick extent c (the EMPTY constant) exactly for most positions
+// (mix(c, c, f) rounds back to c for about 93% of fractions f per level of
+// three), so the positions of the next steps are taken to be t + c, t + 2c,
+// t + 3c (sequential roundings, as the steps would make them) and their
+// four E values are computed independently.  Step j is accepted when every
+// earlier value was exactly c -- then its position is the one the serial
+// march reaches, bit for bit -- and when it passes the serial loop's checks
+// (budget, cube end, tmax); the first value other than c is still a valid
+// step, taken with that value, and the speculation restarts from there.
 template <bool INRUN, bool FAR>
 __device__ __forceinline__ uint32_t empty_run_x2(const ObjDev& o, const uint8_t* __restrict__ field, float ox,
                                                  float oy, float oz, float dx, float dy, float dz, float tmax,
@@ -487,8 +512,7 @@ __device__ __forceinline__ uint32_t empty_run_x2(const ObjDev& o, const uint8_t*
   const f2 o01 = f2_pack(ox, oy), d01 = f2_pack(dx, dy), h01 = f2_pack(o.half_gs[0], o.half_gs[1]);
   const f2 r2 = f2_pack(o.rcp_vs, o.rcp_vs), nvs2 = f2_pack(-o.vs, -o.vs), half2 = f2_pack(0.5f, 0.5f);
   const float hz = o.half_gs[2], vs = o.vs, rcp = o.rcp_vs, be = o.be;
-#pragma unroll 2
-  for (; c < n; ++c) {
+  while (c < n) {
     if (t > lim) {
       if (!INRUN || t > tmax) {
         stop_full = t > tmax;
@@ -502,20 +526,34 @@ __device__ __forceinline__ uint32_t empty_run_x2(const ObjDev& o, const uint8_t*
         break;
       }
     }
-    // grid coordinate (o + d*t) + half; exact quotient by vs (q0 + (g - q0*vs)*rcp,
-    // with -vs so that the FMA adds); minus 0.5
-    const f2 g01 = f2_add(f2_add(o01, f2_mul(d01, f2_pack(t, t))), h01);
-    const f2 q0 = f2_mul(g01, r2);
-    const f2 v01 = f2_sub(f2_fma(f2_fma(q0, nvs2, g01), r2, q0), half2);
-    const float vz = __fsub_rn(exact_div_vs(__fadd_rn(__fadd_rn(oz, __fmul_rn(dz, t)), hz), vs, rcp), 0.5f);
-    float vx, vy;
-    f2_unpack(v01, vx, vy);
-    float tx, ty;
-    f2_unpack(f2_sub(v01, f2_pack(floorf(vx), floorf(vy))), tx, ty);
-    const float d = mix3_const(be, tx, ty, __fsub_rn(vz, floorf(vz)));
-    prev_t = t;
-    prev_dist = d;
-    t = __fadd_rn(t, d);
+    // the positions of the next three steps if every value is c
+    const float t1 = __fadd_rn(t, be), t2 = __fadd_rn(t1, be), t3 = __fadd_rn(t2, be);
+    const float e0 = empty_value_x2(o01, d01, h01, r2, nvs2, half2, oz, dz, hz, vs, rcp, be, t);
+    const float e1 = empty_value_x2(o01, d01, h01, r2, nvs2, half2, oz, dz, hz, vs, rcp, be, t1);
+    const float e2 = empty_value_x2(o01, d01, h01, r2, nvs2, half2, oz, dz, hz, vs, rcp, be, t2);
+    const float e3 = empty_value_x2(o01, d01, h01, r2, nvs2, half2, oz, dz, hz, vs, rcp, be, t3);
+    // step 0 passed the checks above; step j > 0 needs the values before it
+    // to be c (so that t_j is the serial position) and the serial checks
+    float pt = t, pd = e0;
+    ++c;
+    if (e0 == be && c < n && t1 <= lim) {
+      pt = t1;
+      pd = e1;
+      ++c;
+      if (e1 == be && c < n && t2 <= lim) {
+        pt = t2;
+        pd = e2;
+        ++c;
+        if (e2 == be && c < n && t3 <= lim) {
+          pt = t3;
+          pd = e3;
+          ++c;
+        }
+      }
+    }
+    prev_t = pt;
+    prev_dist = pd;
+    t = __fadd_rn(pt, pd);
   }
   return c;
 }
