@@ -1616,71 +1616,134 @@ float orc_evaluate_falloff(uint32_t curve, float distance, float radius) {  // c
   return f * f * f;
 }
 
+// One voxel of apply_edit_cpu (cpu_apply.rs:28-200): the brush's value at
+// the voxel centre vp blended into the existing distance and material.
+// Returns false where the falloff is zero (the voxel keeps its values).
+static bool edit_voxel(const rkf_edit_op* op, float max_extent, const float iq[4], V3<float> vp,
+                       float existing, uint32_t smat, float* nd_out, uint32_t* mat_out) {
+  const V3<float> pos = v3<float>(op->position[0], op->position[1], op->position[2]);
+  const V3<float> el = quat_rotate(iq, sub(vp, pos));
+  const float ela[3] = {el.x, el.y, el.z};
+  const float shape_d = orc_evaluate_shape(op->shape_type, op->dimensions, ela);
+  const float dc = length(sub(vp, pos));
+  const float fw = orc_evaluate_falloff(op->falloff, dc, max_extent + op->blend_k);
+  if (fw <= 0.0f) return false;
+  const float strength = op->strength * fw;
+  float nd = existing;
+  uint32_t mat = smat;
+  switch (op->edit_type) {
+    case 0: {  // CsgUnion
+      const float e = shape_d + (1.0f - strength) * max_extent;
+      nd = fmin_(existing, e);
+      mat = e < existing ? op->material_id : ((nd < 0.0f && smat == 0) ? op->material_id : smat);
+      break;
+    }
+    case 1: {  // CsgSubtract
+      const float e = shape_d + (1.0f - strength) * max_extent;
+      nd = fmax_(existing, -e);
+      break;
+    }
+    case 2: {  // CsgIntersect
+      const float e = shape_d - (1.0f - strength) * max_extent;
+      nd = fmax_(existing, e);
+      break;
+    }
+    case 3: {  // SmoothUnion
+      const float k = fmax_(op->blend_k, 0.001f);
+      const float e = shape_d + (1.0f - strength) * max_extent;
+      nd = smin<float>(existing, e, k);
+      mat = e < existing ? op->material_id : ((nd < 0.0f && smat == 0) ? op->material_id : smat);
+      break;
+    }
+    case 4: {  // SmoothSubtract
+      const float k = fmax_(op->blend_k, 0.001f);
+      const float e = shape_d + (1.0f - strength) * max_extent;
+      nd = -smin<float>(-existing, e, k);
+      break;
+    }
+    default:
+      break;
+  }
+  *nd_out = nd;
+  *mat_out = mat;
+  return true;
+}
+
+static V3<float> edit_voxel_centre(const float bmin[3], float vs, uint32_t vx, uint32_t vy, uint32_t vz) {
+  // voxel_pos = brick_min + (v * vs) + splat(vs*0.5)   (cpu_apply.rs:52-55)
+  return add(add(v3<float>(bmin[0], bmin[1], bmin[2]),
+                 mul(v3<float>(static_cast<float>(vx), static_cast<float>(vy), static_cast<float>(vz)), vs)),
+             v3<float>(vs * 0.5f, vs * 0.5f, vs * 0.5f));
+}
+
 int orc_apply_edit_brick(uint32_t* words, const float bmin[3], float vs, const rkf_edit_op* op) {
   const float iq[4] = {-op->rotation[0], -op->rotation[1], -op->rotation[2], op->rotation[3]};
   const float max_extent = fmax_(fmax_(op->dimensions[0], op->dimensions[1]), op->dimensions[2]);
-  const V3<float> pos = v3<float>(op->position[0], op->position[1], op->position[2]);
   bool any_changed = false;
   for (uint32_t vz = 0; vz < 8; ++vz)
     for (uint32_t vy = 0; vy < 8; ++vy)
       for (uint32_t vx = 0; vx < 8; ++vx) {
-        // voxel_pos = brick_min + (v * vs) + splat(vs*0.5)   (cpu_apply.rs:52-55)
-        const V3<float> vp = add(add(v3<float>(bmin[0], bmin[1], bmin[2]),
-                                     mul(v3<float>(static_cast<float>(vx), static_cast<float>(vy),
-                                                   static_cast<float>(vz)), vs)),
-                                 v3<float>(vs * 0.5f, vs * 0.5f, vs * 0.5f));
-        const V3<float> el = quat_rotate(iq, sub(vp, pos));
-        const float ela[3] = {el.x, el.y, el.z};
-        const float shape_d = orc_evaluate_shape(op->shape_type, op->dimensions, ela);
-        const float dc = length(sub(vp, pos));
-        const float fw = orc_evaluate_falloff(op->falloff, dc, max_extent + op->blend_k);
-        if (fw <= 0.0f) continue;
         const uint32_t idx = vx + vy * 8 + vz * 64;
         const uint32_t w0 = words[2 * idx], w1 = words[2 * idx + 1];
         const float existing = f16_to_f32(static_cast<uint16_t>(w0 & 0xFFFFu));
         const uint32_t smat = (w0 >> 16) & 0x3Fu, ssec = (w0 >> 22) & 0x3Fu, sbl = w1 >> 24;
-        const float strength = op->strength * fw;
-        const float thr = vs * 0.1f;
-        float nd = existing;
-        uint32_t mat = smat;
-        switch (op->edit_type) {
-          case 0: {  // CsgUnion
-            const float e = shape_d + (1.0f - strength) * max_extent;
-            nd = fmin_(existing, e);
-            mat = e < existing ? op->material_id : ((nd < 0.0f && smat == 0) ? op->material_id : smat);
-            break;
-          }
-          case 1: {  // CsgSubtract
-            const float e = shape_d + (1.0f - strength) * max_extent;
-            nd = fmax_(existing, -e);
-            break;
-          }
-          case 2: {  // CsgIntersect
-            const float e = shape_d - (1.0f - strength) * max_extent;
-            nd = fmax_(existing, e);
-            break;
-          }
-          case 3: {  // SmoothUnion
-            const float k = fmax_(op->blend_k, 0.001f);
-            const float e = shape_d + (1.0f - strength) * max_extent;
-            nd = smin<float>(existing, e, k);
-            mat = e < existing ? op->material_id : ((nd < 0.0f && smat == 0) ? op->material_id : smat);
-            break;
-          }
-          case 4: {  // SmoothSubtract
-            const float k = fmax_(op->blend_k, 0.001f);
-            const float e = shape_d + (1.0f - strength) * max_extent;
-            nd = -smin<float>(-existing, e, k);
-            break;
-          }
-          default:
-            break;
-        }
+        float nd;
+        uint32_t mat;
+        if (!edit_voxel(op, max_extent, iq, edit_voxel_centre(bmin, vs, vx, vy, vz), existing, smat, &nd, &mat))
+          continue;
         words[2 * idx] = pack_word0(nd, mat, ssec);
         words[2 * idx + 1] = sbl << 24;
-        if (std::fabs(nd - existing) > thr) any_changed = true;
+        if (std::fabs(nd - existing) > vs * 0.1f) any_changed = true;
       }
   return any_changed ? 1 : 0;
+}
+
+// The same edit on a brick stored as planes with f32 distances (the f32 and
+// u8 pools: the distance the brush blends with is the decoded one, and the
+// result is kept unrounded).  mat holds material | secondary << 6; blend is
+// unchanged.  Returns 1 when some voxel moved by more than vs/10.
+int orc_apply_edit_planes(float* dist, uint16_t* mat, const float bmin[3], float vs, const rkf_edit_op* op) {
+  const float iq[4] = {-op->rotation[0], -op->rotation[1], -op->rotation[2], op->rotation[3]};
+  const float max_extent = fmax_(fmax_(op->dimensions[0], op->dimensions[1]), op->dimensions[2]);
+  bool any_changed = false;
+  for (uint32_t vz = 0; vz < 8; ++vz)
+    for (uint32_t vy = 0; vy < 8; ++vy)
+      for (uint32_t vx = 0; vx < 8; ++vx) {
+        const uint32_t idx = vx + vy * 8 + vz * 64;
+        const float existing = dist[idx];
+        const uint32_t smat = mat[idx] & 0x3Fu, ssec = (mat[idx] >> 6) & 0x3Fu;
+        float nd;
+        uint32_t m;
+        if (!edit_voxel(op, max_extent, iq, edit_voxel_centre(bmin, vs, vx, vy, vz), existing, smat, &nd, &m))
+          continue;
+        dist[idx] = nd;
+        mat[idx] = static_cast<uint16_t>((m & 0x3Fu) | (ssec << 6));
+        if (std::fabs(nd - existing) > vs * 0.1f) any_changed = true;
+      }
+  return any_changed ? 1 : 0;
+}
+
+// Band-normalised u8 code of one brick's 512 distances: B = min(band,
+// largest finite |d|) (at least 1e-6), step = B/127; toward zero:
+// |code| = min(floor(|d|/step), 127), less one where code*step rounds above
+// |d|; to nearest: min(rint(|d|/step), 127); with the sign of d.
+void orc_encode_u8(const float* dist, float band, int nearest, int8_t* code, float* step) {
+  float m = 0.0f;
+  for (int i = 0; i < 512; ++i) {
+    const float a = std::fabs(dist[i]);
+    if (a <= 3.0e38f && a > m) m = a;
+  }
+  const float range = std::fmax(std::fmin(m, band), 1e-6f);
+  const float st = range / 127.0f;
+  *step = st;
+  for (int i = 0; i < 512; ++i) {
+    const float a = std::fabs(dist[i]);
+    const float qa = a / st;
+    const float q = nearest ? std::nearbyint(qa) : std::floor(qa);
+    int c = q >= 127.0f ? 127 : static_cast<int>(q);
+    if (!nearest && c > 0 && static_cast<float>(c) * st > a) --c;
+    code[i] = static_cast<int8_t>(dist[i] < 0.0f ? -c : c);
+  }
 }
 
 void orc_fill_brick_with_brush(uint32_t* words, const float bmin[3], float vs,

@@ -74,6 +74,14 @@ struct EditKernelArgs {
   uint8_t* blend;
   uint2* aos;
   uint8_t* changed;
+  // the f32 and u8 pools: the brush blends with the decoded distance; an
+  // edited u8 brick is encoded again (band-normalised, per-brick step)
+  float* dist_f32;
+  int8_t* dist_u8;
+  float* brick_step;
+  uint32_t precision;
+  float u8_band;
+  uint32_t u8_nearest;
 };
 
 // One 512-thread block per candidate brick.
@@ -83,17 +91,25 @@ __global__ void __launch_bounds__(512) k_edit(EditKernelArgs a) {
   const uint32_t vx = v & 7, vy = (v >> 3) & 7, vz = v >> 6;
   const uint32_t src = a.src[c], dst = a.dst[c];
   const float vs = a.vs;
-  // existing voxel (a sentinel brick is materialised at its sampling value)
+  // existing voxel (a sentinel brick is materialised at its sampling value,
+  // at the pool's precision)
+  const bool f16 = a.precision == RKF_PRECISION_F16;
   uint32_t w0, w1;
+  float existing_plane = 0.0f;  // f32 / u8 pools: the decoded distance
   if (src == RKF_EMPTY_SLOT || src == RKF_INTERIOR_SLOT) {
     const float d = src == RKF_EMPTY_SLOT ? __fmul_rn(vs, 8.0f) : -__fmul_rn(vs, 2.0f);
     w0 = __half_as_ushort(__float2half_rn(d));
     w1 = 0;
+    existing_plane = d;
   } else {
     const size_t i = static_cast<size_t>(src) * 512 + v;
     const uint16_t m = a.mat[i];
-    w0 = static_cast<uint32_t>(a.dist_f16[i]) | ((m & 0x3Fu) << 16) | (((m >> 6) & 0x3Fu) << 22);
+    const uint32_t dbits = f16 ? static_cast<uint32_t>(a.dist_f16[i]) : 0u;
+    w0 = dbits | ((m & 0x3Fu) << 16) | (((m >> 6) & 0x3Fu) << 22);
     w1 = static_cast<uint32_t>(a.blend[i]) << 24;
+    if (a.precision == RKF_PRECISION_F32) existing_plane = a.dist_f32[i];
+    if (a.precision == RKF_PRECISION_U8)
+      existing_plane = __fmul_rn(static_cast<float>(a.dist_u8[i]), a.brick_step[src]);
   }
   const rkf_edit_op& op = a.op;
   // voxel_pos = brick_min + (v * vs) + splat(vs*0.5)  (cpu_apply.rs:52-55)
@@ -119,8 +135,9 @@ __global__ void __launch_bounds__(512) k_edit(EditKernelArgs a) {
   const float dc = len3(rx, ry, rz);
   const float fw = edit_falloff(op.falloff, dc, __fadd_rn(a.max_extent, op.blend_k));
   int changed = 0;
+  float out_d = f16 ? 0.0f : existing_plane;  // f32 / u8 pools: the voxel's new distance
   if (fw > 0.0f) {
-    const float existing = __half2float(__ushort_as_half(static_cast<uint16_t>(w0 & 0xFFFFu)));
+    const float existing = f16 ? __half2float(__ushort_as_half(static_cast<uint16_t>(w0 & 0xFFFFu))) : existing_plane;
     const uint32_t smat = (w0 >> 16) & 0x3Fu, ssec = (w0 >> 22) & 0x3Fu, sbl = w1 >> 24;
     const float strength = __fmul_rn(op.strength, fw);
     const float thr = __fmul_rn(vs, 0.1f);
@@ -158,12 +175,38 @@ __global__ void __launch_bounds__(512) k_edit(EditKernelArgs a) {
     w0 = static_cast<uint32_t>(__half_as_ushort(__float2half_rn(nd))) | ((mat & 0x3Fu) << 16) | (ssec << 22);
     w1 = sbl << 24;
     changed = fabsf(__fsub_rn(nd, existing)) > thr;
+    out_d = nd;
+  } else if (!f16) {
+    // an untouched voxel of an f32 / u8 brick: the reference words carry
+    // its distance in binary16
+    w0 = (w0 & 0xFFFF0000u) | static_cast<uint32_t>(__half_as_ushort(__float2half_rn(existing_plane)));
   }
   const size_t o = static_cast<size_t>(dst) * 512 + v;
-  a.dist_f16[o] = static_cast<uint16_t>(w0 & 0xFFFFu);
+  if (f16) a.dist_f16[o] = static_cast<uint16_t>(w0 & 0xFFFFu);
+  if (a.precision == RKF_PRECISION_F32) a.dist_f32[o] = out_d;
   a.mat[o] = static_cast<uint16_t>(((w0 >> 16) & 0x3Fu) | (((w0 >> 22) & 0x3Fu) << 6));
   a.blend[o] = static_cast<uint8_t>(w1 >> 24);
   if (a.aos) a.aos[o] = make_uint2(w0, w1);
+  if (a.precision == RKF_PRECISION_U8) {
+    // the brick's code: B = min(band, largest finite |d|), step = B/127
+    // (the encoding of the u8 pool, k_encode_u8)
+    __shared__ float red[16];
+    const float ad = fabsf(out_d);
+    float m = ad <= 3.0e38f ? ad : 0.0f;
+    for (int off = 16; off; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, off));
+    if ((v & 31) == 0) red[v >> 5] = m;
+    __syncthreads();
+    float mx = 0.0f;
+    for (int k = 0; k < 16; ++k) mx = fmaxf(mx, red[k]);
+    const float range = fmaxf(fminf(mx, a.u8_band), 1e-6f);
+    const float st = __fdiv_rn(range, 127.0f);
+    const float qa = __fdiv_rn(ad, st);
+    const float q = a.u8_nearest ? rintf(qa) : floorf(qa);
+    int code = q >= 127.0f ? 127 : static_cast<int>(q);
+    if (!a.u8_nearest && code > 0 && __fmul_rn(static_cast<float>(code), st) > ad) --code;
+    a.dist_u8[o] = static_cast<int8_t>(out_d < 0.0f ? -code : code);
+    if (v == 0) a.brick_step[dst] = st;
+  }
   const int any = __syncthreads_or(changed);
   if (v == 0) a.changed[c] = static_cast<uint8_t>(any != 0);
 }
@@ -215,8 +258,6 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   if (op.object_index >= c->obj_count()) return fail(RKF_INVALID_ARG, "rkf_edit_csg: object index out of range");
   if (op.edit_type > 4 || op.shape_type > 2 || op.falloff > 2)
     return fail(RKF_INVALID_ARG, "rkf_edit_csg: unsupported edit, shape or falloff type");
-  if (c->cfg.precision != RKF_PRECISION_F16)
-    return fail(RKF_UNSUPPORTED, "rkf_edit_csg: edits need the f16 pool (the reference storage)");
   const rkf_gpu_object& go = c->objects[op.object_index];
   if (go.sdf_type != RKF_SDF_VOXELIZED) return fail(RKF_INVALID_ARG, "rkf_edit_csg: object is not voxelized");
   const ObjDev& od = c->objdev_host[op.object_index];
@@ -335,6 +376,12 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   ka.blend = c->blend.as<uint8_t>();
   ka.aos = c->aos.as<uint2>();
   ka.changed = d_changed;
+  ka.dist_f32 = c->dist_f32.as<float>();
+  ka.dist_u8 = c->dist_u8.as<int8_t>();
+  ka.brick_step = c->brick_step.as<float>();
+  ka.precision = c->cfg.precision;
+  ka.u8_band = c->cfg.u8_band > 0.0f ? c->cfg.u8_band : 3.0f * vs;
+  ka.u8_nearest = c->cfg.u8_round == 1 ? 1u : 0u;
   detail::k_edit<<<n, 512, 0, st>>>(ka);
   RKF_CUDA_TRY(cudaGetLastError());
   std::vector<uint8_t> changed(n);

@@ -126,3 +126,98 @@ def test_csg_edits_match_oracle_and_march(oracle, small_scene):
                 continue
             assert_bits_equal(got[k], ref[k], k)
             assert_bits_equal(plain[k], ref[k], "plain " + k)
+
+
+@pytest.mark.parametrize("precision,u8_round", [("f32", 0), ("u8", 0), ("u8", 1)],
+                         ids=["f32", "u8_toward_zero", "u8_nearest"])
+def test_csg_edits_on_f32_and_u8_pools(oracle, small_scene, precision, u8_round):
+    """The same edits on pools stored in f32 and in band-normalised u8: the
+    brush blends with the decoded distance (apply_edit_cpu's arithmetic,
+    cpu_apply.rs:28-200) and an edited u8 brick is encoded again with its own
+    step.  Brick by brick against the oracle's restatement, then the march of
+    the edited scene against the oracle march over the exported planes."""
+    from rkifield_b200 import _abi as abi
+    from rkifield_b200 import scenes
+    from rkifield_b200.engine import Context
+    spec, prims, vp = small_scene["spec"], small_scene["prims"], small_scene["vp"]
+    vs = np.float32(spec.voxel_size)
+    cap = small_scene["vox"].n_bricks + 20000
+    ctx = Context(pool_capacity=cap, precision=precision, keep_reference_pool=False, u8_round=u8_round)
+    try:
+        ctx.voxelize(prims, vp)
+        obj = ctx.object(0)
+        dims = np.array(obj.brick_map_dims[:], np.uint32)
+        p0 = prims[3]
+        c = p0["centre"].astype(np.float64)
+        r = float(p0["bound_radius"])
+        ops = [_op(0, c + np.array([r, 0, 0]), 0.6, 7),
+               _op(1, c + np.array([0, r * 0.8, 0]), 0.5, 0),
+               _op(3, c + np.array([0, 0, r + 0.3]), 0.4, 9, blend_k=0.1, falloff=2),
+               _op(4, c - np.array([r * 0.5, 0, 0]), 0.7, 0, blend_k=0.1)]
+        L = oracle.lib()
+        for op in ops:
+            pl = ctx.export_planes(0, cap)
+            bxyz, origin, be = _bricks_in_range(op, dims, vs)
+            slots = ctx.brick_lookup(0, bxyz.ravel())
+            additive = op.edit_type in (0, 3)
+            exp = []
+            for b, s in zip(bxyz, slots):
+                if (s == abi.EMPTY_SLOT and not additive) or (s == abi.INTERIOR_SLOT and additive):
+                    exp.append((b, s, None))
+                    continue
+                if s >= abi.INTERIOR_SLOT:
+                    d = np.full(512, vs * np.float32(8) if s == abi.EMPTY_SLOT else -(vs * np.float32(2)), np.float32)
+                    m = np.zeros(512, np.uint16)
+                    bl = np.zeros(512, np.uint8)
+                else:
+                    sl = slice(512 * int(s), 512 * (int(s) + 1))
+                    d = (pl["dist"][sl].astype(np.float32) * pl["step"][int(s)]).astype(np.float32) \
+                        if precision == "u8" else pl["dist"][sl].copy()
+                    m = pl["mat"][sl].copy()
+                    bl = pl["blend"][sl].copy()
+                bmin = (origin + b.astype(np.float32) * be).astype(np.float32)
+                changed = L.orc_apply_edit_planes(d.ctypes.data, m.ctypes.data, bmin.ctypes.data, float(vs),
+                                                  C.byref(op))
+                if not changed:
+                    exp.append((b, s, None))
+                    continue
+                e = {"mat": m, "blend": bl}
+                if precision == "u8":
+                    code = np.zeros(512, np.int8)
+                    step = np.zeros(1, np.float32)
+                    L.orc_encode_u8(d.ctypes.data, float(np.float32(3.0) * vs), u8_round, code.ctypes.data,
+                                    step.ctypes.data)
+                    e.update(dist=code, step=step)
+                else:
+                    e["dist"] = d
+                exp.append((b, s, e))
+            assert any(x[2] is not None for x in exp), "the edit should change bricks"
+            ctx.edit(op)
+            after = ctx.brick_lookup(0, bxyz.ravel())
+            pl2 = ctx.export_planes(0, cap)
+            for (b, s_old, e), s_new in zip(exp, after):
+                if e is None:
+                    assert s_new == s_old, f"brick {b} should be untouched"
+                    continue
+                assert s_new < abi.INTERIOR_SLOT and s_new != s_old, f"brick {b} should move to a fresh slot"
+                sl = slice(512 * int(s_new), 512 * (int(s_new) + 1))
+                for k in ("dist", "mat", "blend"):
+                    assert_bits_equal(pl2[k][sl], e[k], f"brick {b} {k}")
+                if precision == "u8":
+                    assert_bits_equal(pl2["step"][int(s_new):int(s_new) + 1], e["step"], f"brick {b} step")
+        # the edited scene marches as the oracle does over the exported planes
+        idx = ctx.export_index()
+        pl = ctx.export_planes(0, cap)
+        code = {"f32": abi.RKF_PRECISION_F32, "u8": abi.RKF_PRECISION_U8}[precision]
+        kw = {"dist_f32": pl["dist"]} if precision == "f32" else {"dist_u8": pl["dist"], "brick_scale": pl["step"]}
+        sc = oracle.Scene([obj], top=idx["top"], leaves=idx["leaves"], obj_top_info=idx["obj_top_info"],
+                          mat_plane=pl["mat"], blend_plane=pl["blend"], precision=code, **kw)
+        cam = scenes.camera_uniforms(c + np.array([4.0, 2.0, 5.0]), c, 160, 120)
+        p = scenes.march_params(spec)
+        ref = oracle.march(sc, cam, p, 160, 120, with_reference_planes=True)
+        got = ctx.march(cam, p, 160, 120, reference_planes=True)
+        assert (ref["flags"] & 1).sum() > 1000
+        for k in ("t", "normal", "slot", "material", "flags", "position", "packed_material", "motion"):
+            assert_bits_equal(got[k], ref[k], f"{precision} edited march {k}")
+    finally:
+        ctx.close()
