@@ -687,7 +687,19 @@ def run_precision_report(args):
             np.linalg.norm(ng, axis=1) * np.linalg.norm(n64[nonz], axis=1), 1e-300), -1.0, 1.0)
         ang = np.arccos(cosang)
         del dirs_dot
-        entry = {"hit_agreement": float((hit == hit64).mean()),
+        # the same error on the rays none of whose FP64 decisions lies within
+        # m voxels of its threshold: a code error of m can flip no decision
+        # there, so what remains is the values' own error, not a step's jump
+        by_margin = {}
+        for m in (0.0118, 0.0236, 0.05):
+            keep = both & (ref["margin"] >= m * vs)
+            dm = np.abs(g["t"][keep].astype(np.float64) - ref["t64"][keep]) / vs
+            by_margin[str(m)] = {"hit_rays_kept": float(keep.sum() / max(1, both.sum())),
+                                 "p99": float(np.percentile(dm, 99)) if dm.size else None,
+                                 "mean": float(dm.mean()) if dm.size else None,
+                                 "within_0.01_voxel": float((dm <= 0.01).mean()) if dm.size else None}
+        entry = {"dt_voxels_by_decision_margin": by_margin,
+                 "hit_agreement": float((hit == hit64).mean()),
                  "hit_agreement_non_grazing": float((hit == hit64)[~graze].mean()),
                  "material_agreement": float((g["material"][both] == ref["material"][both]).mean()) if both.any() else None,
                  "grazing_fraction": float(graze.mean()),

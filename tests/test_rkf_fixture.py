@@ -48,9 +48,12 @@ def cross_prims_and_params(f):
 
 
 def test_fixture_matches_reference_file_when_present():
-    path = "/root/reference/scenes/test_cross.rkf"
-    if not os.path.exists(path):
-        pytest.skip("reference tree not present")
+    """The committed fixture equals the reference's own scenes/test_cross.rkf
+    when a checkout of the reference is named by RKF_REFERENCE_ROOT."""
+    root = os.environ.get("RKF_REFERENCE_ROOT", "")
+    path = os.path.join(root, "scenes", "test_cross.rkf") if root else ""
+    if not path or not os.path.exists(path):
+        pytest.skip("no reference checkout (set RKF_REFERENCE_ROOT)")
     from rkifield_b200.rkf_asset import read_rkf
     lod = read_rkf(path).lods[-1]
     f = fixture()
