@@ -48,9 +48,11 @@ struct ColdState {
   float lo, hi, mat_t, gpos, shadow;
   uint32_t tile_base, tile_count;  // tiled strategy: the ray's object list (kNoTiles: every object)
   bool hit, bisected, mat_ok;
-  // multi-object tiled empty-space path: the ray's object list holds the
-  // voxelized object.  (Also makes an odd number of words per lane: a warp's
-  // accesses hit 32 distinct banks.)
+  // multi-object empty-space path: bits 0-7, the voxelized objects of the
+  // path (KParams::ev) whose EMPTY runs the ray may take (under the tiled
+  // strategy, those its object list holds); bits 8-15, the one whose cube
+  // the ray is in (its last successful probe).  (Also makes an odd number of
+  // words per lane: a warp's accesses hit 32 distinct banks.)
   uint32_t vox_listed;
 };
 static_assert(sizeof(ColdState) % 8 == 4, "ColdState must span an odd number of 32-bit words");
@@ -71,6 +73,21 @@ static_assert(sizeof(ColdState) % 8 == 4, "ColdState must span an odd number of 
 struct FarBall {
   float c[3];  // world-space centre
   float a, b;  // radius a + b * P
+};
+
+// One voxelized object of the multi-object empty-space path: EMPTY runs on
+// its own field wherever the ray lies in one of its EMPTY cubes and outside
+// the balls of all the other objects (analytic or voxelized), where its
+// EMPTY value is the scene's minimum.
+constexpr uint32_t kMaxEmptyVox = 8;
+struct EmptyVox {
+  uint32_t obj;       // object index
+  uint32_t n_far;     // balls of the other objects
+  uint32_t plain;     // zero translation and unit scale
+  float probe_min;    // probe for a cube once a sample was at least this
+  float empty_lo;     // lower bound of every EMPTY value (times the scale)
+  float empty_lo_t, empty_hi;  // tight bounds of an EMPTY step
+  FarBall far[kMaxObjectsFast];
 };
 
 struct KParams {
@@ -97,11 +114,12 @@ struct KParams {
   const rkf_bvh_node* bvh; // BVH strategy: the imported tree, root first
   const uint32_t* bvh_next;  // per node: the walk's next node (bits 0-30), descend (bit 31)
   uint32_t use_bvh;
-  ObjDev vox;                     // multi-object empty-space path: the voxelized object
-  FarBall far[kMaxObjectsFast];   // multi-object empty-space path: the analytic objects' balls
-  uint32_t n_far;
-  uint32_t vox_i;                 // multi-object empty-space path: the voxelized object's index
+  // multi-object empty-space path: the voxelized objects that take EMPTY
+  // runs, each with the balls of every other object
+  EmptyVox ev[kMaxEmptyVox];
+  uint32_t n_ev;
 };
+static_assert(sizeof(KParams) <= 32000, "the launch parameters must fit the kernel parameter space");
 
 // The candidate loop of ray_march_bvh (ray_march.wgsl:672-721): a stack walk
 // of the tree from the root that skips every node whose AABB lies farther
@@ -644,16 +662,20 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                     cs.tile_count = __ldg(kp.td.tile_cnt + tl);
                   }
                   if (MULTI_TILED) {
-                    bool listed = cs.tile_count == kNoTiles;
-                    for (uint32_t j = 0; !listed && j < cs.tile_count; ++j)
-                      listed = __ldg(kp.td.tile_list + cs.tile_base + j) == kp.vox_i;
-                    cs.vox_listed = listed ? 1u : 0u;
+                    uint32_t listed = 0;
+                    for (uint32_t e = 0; e < kp.n_ev; ++e) {
+                      bool in = cs.tile_count == kNoTiles;
+                      for (uint32_t j = 0; !in && j < cs.tile_count; ++j)
+                        in = __ldg(kp.td.tile_list + cs.tile_base + j) == kp.ev[e].obj;
+                      if (in) listed |= 1u << e;
+                    }
+                    cs.vox_listed = listed;
                   }
                 }
               }
             } else {
               if (TILES) cs.tile_count = kNoTiles;
-              if (MULTI_TILED) cs.vox_listed = 1u;
+              if (MULTI_TILED) cs.vox_listed = (1u << kp.n_ev) - 1u;
               cs.idx = static_cast<uint32_t>(local);
               const size_t i3 = 3 * static_cast<size_t>(cs.idx);
               ox = __ldg(sg.origins + i3);
@@ -669,7 +691,10 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
               near = 0;
               step = 0;
               box_t = -1.0f;
-              if (MULTI_EMPTY) far_t = far_recheck = -1.0f;
+              if (MULTI_EMPTY) {
+                far_t = far_recheck = -1.0f;
+                if (!MULTI_TILED) cs.vox_listed = (1u << kp.n_ev) - 1u;
+              }
               prev_dist = kMaxFloat;
               cs.hit = cs.bisected = cs.mat_ok = false;
               if (mode == RKF_TRACE_SHADOW) {
@@ -704,10 +729,11 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
       bool full = true;  // take a full step (index lookups) this iteration
       // (a tiled step evaluates the ray's object list only: EMPTY runs need
       // the voxelized object in it)
-      if (EMPTY_PATH && (state == ST_MARCH || state == ST_SHADOW) && (!MULTI_TILED || cs.vox_listed)) {
+      if (EMPTY_PATH && (state == ST_MARCH || state == ST_SHADOW) && (!MULTI_EMPTY || (cs.vox_listed & 0xFFu))) {
         // empty-space run: inside a cube of EMPTY blocks every sample is
-        // empty_value(), so up to kp.budget steps run without the sampler
-        const ObjDev& o0 = MULTI_EMPTY ? kp.vox : sh_objs[0];
+        // empty_value(), so up to kp.budget steps run without the sampler.
+        // Several objects: a probe picks the first voxelized object of the
+        // path whose EMPTY cube holds the ray; its constants and balls apply.
         const bool sh = state == ST_SHADOW;
         const float dx = sh ? rdx : qdx, dy = sh ? rdy : qdy, dz = sh ? rdz : qdz;
         const uint32_t max_step = sh ? 256u : p.hard_max_steps;
@@ -716,17 +742,44 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
         const float brk = sh ? 0.02f : fmaxf(hit_thr, 0.0f);
         const float near_thr = sh ? -1.0f : p.near_surface_threshold;
         const float min_step = sh ? 0.005f : p.min_step;
-        const bool clean = kp.empty_lo >= brk && kp.empty_lo >= near_thr && kp.empty_lo >= min_step;
         // a ray that may be inside a ball takes full steps until it may have left
-        if (t > box_t && prev_dist >= kp.probe_min && (!MULTI_EMPTY || t > far_recheck)) {
-          box_t = probe_empty(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, t);
+        const bool probe = t > box_t && prev_dist >= kp.probe_min && (!MULTI_EMPTY || t > far_recheck);
+        if (MULTI_EMPTY && probe) {
+          // the first voxelized object of the path (that the ray may take runs
+          // on) whose EMPTY cube holds the ray
+          const uint32_t cur = cs.vox_listed >> 8;
+          uint32_t found = kMaxEmptyVox;
+          box_t = -1.0f;
+          for (uint32_t e = 0; e < kp.n_ev && found == kMaxEmptyVox; ++e) {
+            if (!((cs.vox_listed >> e) & 1u)) continue;
+            const float bt = probe_empty(sh_objs[kp.ev[e].obj], s.empty_dist, ox, oy, oz, dx, dy, dz, t);
+            if (t <= bt) {
+              found = e;
+              box_t = bt;
+            }
+          }
+          if (found != kMaxEmptyVox && found != cur) {
+            // another object's cube: the balls that bound it are others
+            cs.vox_listed = (cs.vox_listed & 0xFFu) | (found << 8);
+            far_t = far_recheck = -1.0f;
+          }
+        }
+        const EmptyVox& ev = kp.ev[MULTI_EMPTY ? (cs.vox_listed >> 8) : 0u];
+        const ObjDev& o0 = sh_objs[MULTI_EMPTY ? ev.obj : 0u];
+        const float e_lo = MULTI_EMPTY ? ev.empty_lo : kp.empty_lo;
+        const float e_hi = MULTI_EMPTY ? ev.empty_hi : kp.empty_hi;
+        const float e_lo_t = MULTI_EMPTY ? ev.empty_lo_t : kp.empty_lo_t;
+        const uint32_t plain = MULTI_EMPTY ? ev.plain : kp.plain_obj;
+        const bool clean = e_lo >= brk && e_lo >= near_thr && e_lo >= min_step;
+        if (probe) {
+          if (!MULTI_EMPTY) box_t = probe_empty(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, t);
           const float cube_t = box_t;
           if (MULTI_EMPTY) {
             // only positions outside every ball sample the EMPTY value.  far_t
             // (the first entry into a ball ahead) stays valid until the ray
             // passes it: balls ahead stay ahead, balls behind stay behind.
             if (t <= box_t && t > far_t)
-              far_t = far_limit(kp.far, kp.n_far, ox, oy, oz, dx, dy, dz, tmax, t, far_recheck);
+              far_t = far_limit(ev.far, ev.n_far, ox, oy, oz, dx, dy, dz, tmax, t, far_recheck);
             box_t = fminf(box_t, far_t);
           }
           if (t <= box_t && clean && kp.settle_links && step < max_step && near < max_near) {
@@ -742,8 +795,8 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
             // that bound (or tmax), the outcome is settled.
             const float k = static_cast<float>(max_step - step - 1);
             const float grow = (k + 4.0f) * 2.384185791015625e-7f;
-            const float t_hi = (t + k * kp.empty_hi) * (1.0f + grow);
-            const float t_lo = (t + k * kp.empty_lo_t) * (1.0f - grow);
+            const float t_hi = (t + k * e_hi) * (1.0f + grow);
+            const float t_lo = (t + k * e_lo_t) * (1.0f - grow);
             const bool out_of_steps = t_hi <= tmax;
             if (out_of_steps || t_lo > tmax) {
               const float need = out_of_steps ? t_hi : tmax;
@@ -770,12 +823,12 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
 #define RKF_RUN(P, CL, IN)                                                                                   \
   empty_run<P, CL, IN, MULTI_EMPTY>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n, brk, near_thr, min_step, \
                                     max_near, far_t, t, box_t, prev_t, prev_dist, near, stop_full)
-            if (kp.plain_obj && clean)
+            if (plain && clean)
               c = kp.run_probe ? empty_run_x2<true, MULTI_EMPTY>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n,
                                                                  far_t, t, box_t, prev_t, prev_dist, stop_full)
                                : empty_run_x2<false, MULTI_EMPTY>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n,
                                                                   far_t, t, box_t, prev_t, prev_dist, stop_full);
-            else if (kp.plain_obj)
+            else if (plain)
               c = kp.run_probe ? RKF_RUN(true, false, true) : RKF_RUN(true, false, false);
             else
               c = kp.run_probe ? RKF_RUN(false, false, true) : RKF_RUN(false, false, false);
@@ -1218,9 +1271,18 @@ double up_float(double v) {  // a float >= v
 // to 2^-16 of the magnitudes involved, a wide margin over the few 2^-24
 // roundings each step makes).  false when the object has no usable ball.
 bool far_ball(const ObjDev& o, float empty_hi, detail::FarBall* out) {
-  const double R = prim_radius(o);
+  // A voxelized object's sampler returns the distance to its clamped grid
+  // box (a box inside |l| <= |half_gs|) wherever that distance exceeds two
+  // brick extents (ray_march.wgsl:371-376), so beyond the ball of radius
+  // |half_gs| + max(2 * brick extent, EMPTY value / scale) its value is at
+  // least that distance times its scale, above every EMPTY value.
+  const bool vox = o.sdf_type == RKF_SDF_VOXELIZED;
+  const double R = vox ? std::sqrt(static_cast<double>(o.half_gs[0]) * o.half_gs[0] +
+                                   static_cast<double>(o.half_gs[1]) * o.half_gs[1] +
+                                   static_cast<double>(o.half_gs[2]) * o.half_gs[2])
+                       : prim_radius(o);
   const double s = o.min_scale;
-  if (R < 0.0 || !(s > 0.0) || !std::isfinite(s)) return false;
+  if (R < 0.0 || !std::isfinite(R) || !(s > 0.0) || !std::isfinite(s)) return false;
   double A[3][3], t[3];  // l_i = sum_k A[i][k] p_k + t_i (to_local)
   for (int i = 0; i < 3; ++i) {
     for (int k = 0; k < 3; ++k) A[i][k] = o.m[4 * k + i];
@@ -1249,8 +1311,9 @@ bool far_ball(const ObjDev& o, float empty_hi, detail::FarBall* out) {
   const double N = std::sqrt(nf), sigma = 1.0 / std::sqrt(nif);  // |A x| >= sigma |x|
   const double e16 = 0x1p-16, e20 = 0x1p-20;
   if (!(sigma > 0.0) || !(N / sigma <= 1024.0)) return false;
-  const double a = (R * (1.0 + e16) + e16 * std::sqrt(tn) + static_cast<double>(empty_hi) * (1.0 + e16) / s) / sigma +
-                   e20 * std::sqrt(cn);
+  double need = static_cast<double>(empty_hi) * (1.0 + e16) / s;  // local distance beyond R
+  if (vox) need = std::max(need, static_cast<double>(o.be2) * (1.0 + e16));
+  const double a = (R * (1.0 + e16) + e16 * std::sqrt(tn) + need) / sigma + e20 * std::sqrt(cn);
   const double b = e16 * N / sigma + e20;
   for (int i = 0; i < 3; ++i) out->c[i] = static_cast<float>(c[i]);
   out->a = static_cast<float>(up_float(a));
@@ -1260,37 +1323,47 @@ bool far_ball(const ObjDev& o, float empty_hi, detail::FarBall* out) {
 }
 
 // A scene of several objects the multi-object empty-space path can march:
-// exactly one object that is not analytic or of no type, which qualifies for
-// the empty-space path, and analytic objects that each have a ball (or whose
-// every value exceeds the EMPTY values).  Fills the voxelized object's index
-// and the balls when the pointers are given.
-bool multi_empty_scene(const Ctx* c, uint32_t* vi_out, detail::FarBall* far, uint32_t* n_far) {
+// one to kMaxEmptyVox voxelized objects that qualify for the empty-space path
+// (the first ones by index), each of which takes EMPTY runs on its own field,
+// and every other object -- analytic, voxelized (qualifying or not) or of no
+// type -- bounded by a ball outside which its value exceeds that object's
+// EMPTY values.  Fills ev (the path's objects with their balls) when given.
+bool multi_empty_scene(const Ctx* c, detail::EmptyVox* ev, uint32_t* n_ev) {
   const uint32_t n = c->obj_count();
   if (n < 2 || n > kMaxObjectsFast) return false;
-  uint32_t vi = n;
-  for (uint32_t i = 0; i < n; ++i) {
-    const uint32_t ty = c->objdev_host[i].sdf_type;
-    if (ty == RKF_SDF_NONE || ty == RKF_SDF_ANALYTICAL) continue;
-    if (vi != n) return false;
-    vi = i;
-  }
-  if (vi == n || !empty_object(c, c->objdev_host[vi])) return false;
-  const float hi = empty_hi_of(c->objdev_host[vi]);
-  uint32_t nb = 0;
-  for (uint32_t i = 0; i < n; ++i) {
-    const ObjDev& o = c->objdev_host[i];
-    if (i == vi || o.sdf_type == RKF_SDF_NONE) continue;  // no type: kMaxFloat
-    if (o.prim_type > RKF_PRIM_PLANE) {  // an unknown primitive: kMaxFloat * min_scale
-      if (static_cast<double>(kMaxFloat) * o.min_scale * (1.0 - 0x1p-20) >= hi) continue;
-      return false;
+  uint32_t q[detail::kMaxEmptyVox];
+  uint32_t nq = 0;
+  for (uint32_t i = 0; i < n && nq < detail::kMaxEmptyVox; ++i)
+    if (empty_object(c, c->objdev_host[i])) q[nq++] = i;
+  if (nq == 0) return false;
+  for (uint32_t j = 0; j < nq; ++j) {
+    const ObjDev& a = c->objdev_host[q[j]];
+    const float hi = empty_hi_of(a);
+    detail::EmptyVox e;
+    std::memset(&e, 0, sizeof(e));
+    e.obj = q[j];
+    for (uint32_t i = 0; i < n; ++i) {
+      const ObjDev& o = c->objdev_host[i];
+      if (i == q[j] || o.sdf_type == RKF_SDF_NONE) continue;  // no type: kMaxFloat
+      if (o.sdf_type == RKF_SDF_ANALYTICAL && o.prim_type > RKF_PRIM_PLANE) {
+        // an unknown primitive: kMaxFloat * min_scale
+        if (static_cast<double>(kMaxFloat) * o.min_scale * (1.0 - 0x1p-20) >= hi) continue;
+        return false;
+      }
+      detail::FarBall b;
+      if (!far_ball(o, hi, &b)) return false;
+      e.far[e.n_far++] = b;
     }
-    detail::FarBall b;
-    if (!far_ball(o, hi, &b)) return false;
-    if (far) far[nb] = b;
-    ++nb;
+    e.probe_min = 0.99f * a.be * a.min_scale;
+    // mix(c, c, t) three times stays within 12 roundings of c (relative
+    // 2^-24 each); 0.999 leaves a wide margin, 2^-16 a tight one
+    e.empty_lo = 0.999f * a.be * a.min_scale;
+    e.empty_lo_t = a.be * a.min_scale * (1.0f - 1.52587890625e-5f);
+    e.empty_hi = hi;
+    e.plain = (a.m[12] == 0.0f && a.m[13] == 0.0f && a.m[14] == 0.0f && a.min_scale == 1.0f) ? 1u : 0u;
+    if (ev) ev[j] = e;
   }
-  if (vi_out) *vi_out = vi;
-  if (n_far) *n_far = nb;
+  if (n_ev) *n_ev = nq;
   return true;
 }
 
@@ -1332,10 +1405,28 @@ bool bvh_reaches(const Ctx* c, uint32_t vi) {
   return false;
 }
 
+// The objects of the multi-object empty-space path of a launch, with their
+// balls, into kp.ev: those the BVH walk reaches everywhere in their grids
+// when the launch walks the tree.  false when none remains.
+bool fill_multi_empty(const Ctx* c, bool walk, detail::KParams& kp) {
+  detail::EmptyVox ev[detail::kMaxEmptyVox];
+  uint32_t n = 0;
+  if (!multi_empty_scene(c, ev, &n)) return false;
+  kp.n_ev = 0;
+  kp.probe_min = kMaxFloat;
+  for (uint32_t j = 0; j < n; ++j) {
+    if (walk && !bvh_reaches(c, ev[j].obj)) continue;
+    kp.ev[kp.n_ev] = ev[j];
+    kp.probe_min = std::min(kp.probe_min, ev[j].probe_min);
+    ++kp.n_ev;
+  }
+  return kp.n_ev > 0;
+}
+
 // Which kernel variant a launch over this context's objects uses.
 int object_set(const Ctx* c) {
   if (c->obj_count() != 1)
-    return multi_empty_scene(c, nullptr, nullptr, nullptr) ? detail::OBJ_MULTI_EMPTY : detail::OBJ_MULTI;
+    return multi_empty_scene(c, nullptr, nullptr) ? detail::OBJ_MULTI_EMPTY : detail::OBJ_MULTI;
   return empty_object(c, c->objdev_host[0]) ? detail::OBJ_SINGLE_EMPTY : detail::OBJ_SINGLE;
 }
 }  // namespace
@@ -1352,10 +1443,10 @@ bool empty_order_source(const Ctx* c, const rkf_march_params* p, const rkf_batch
     return true;
   }
   if (objs == detail::OBJ_MULTI_EMPTY) {
-    uint32_t vi = 0;
-    multi_empty_scene(c, &vi, nullptr, nullptr);
-    if (use_bvh && !bvh_reaches(c, vi)) return false;
-    *o = c->objdev_host[vi];
+    // the estimate walks the field of the path's first object
+    static thread_local detail::KParams kp;
+    if (!fill_multi_empty(c, use_bvh, kp)) return false;
+    *o = c->objdev_host[kp.ev[0].obj];
     return true;
   }
   return false;
@@ -1383,14 +1474,21 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
     if (objs == detail::OBJ_SINGLE_EMPTY) objs = detail::OBJ_SINGLE;
     if (objs == detail::OBJ_MULTI_EMPTY) objs = detail::OBJ_MULTI;
   }
-  uint32_t vi = 0;  // the object of the empty-space path
-  if (objs == detail::OBJ_MULTI_EMPTY) multi_empty_scene(c, &vi, nullptr, nullptr);
   if (tiled) {
     tiled_segs = segs_host;
     rkf_status s2 = prepare_tiled(c, tiled_segs, st, &td);
     if (s2 != RKF_OK) return s2;
+    // the tiled empty-space field of every object of the path
+    std::vector<uint32_t> path{0u};
+    if (objs == detail::OBJ_MULTI_EMPTY) {
+      detail::EmptyVox ev[detail::kMaxEmptyVox];
+      uint32_t n = 0;
+      multi_empty_scene(c, ev, &n);
+      path.clear();
+      for (uint32_t j = 0; j < n; ++j) path.push_back(ev[j].obj);
+    }
     if ((objs == detail::OBJ_SINGLE_EMPTY || objs == detail::OBJ_MULTI_EMPTY) &&
-        (s2 = prepare_tiled_empty(c, st, vi)) != RKF_OK)
+        (s2 = prepare_tiled_empty(c, st, path)) != RKF_OK)
       return s2;
   }
   // heaviest-first order of the views' tiles (a whole launch only: a band of
@@ -1446,25 +1544,22 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
     kp.s.empty_dist = c->tiled_empty_dist.as<uint8_t>();
   }
   // the multi-object empty-space path marches the brute and tiled
-  // strategies, and the BVH strategy on trees whose walk reaches the
-  // voxelized object everywhere in its grid
-  if (objs == detail::OBJ_MULTI_EMPTY) multi_empty_scene(c, nullptr, kp.far, &kp.n_far);
-  if (objs == detail::OBJ_MULTI_EMPTY && walk && !bvh_reaches(c, vi)) obj = detail::OBJ_MULTI;
+  // strategies, and the BVH strategy for the objects whose grids the tree's
+  // walk reaches everywhere
+  if (objs == detail::OBJ_MULTI_EMPTY && !fill_multi_empty(c, walk, kp)) obj = detail::OBJ_MULTI;
   if (obj == detail::OBJ_MULTI_EMPTY && tiled) {
     obj = detail::OBJ_MULTI_EMPTY_TILED;
     kp.s.empty_dist = c->tiled_empty_dist.as<uint8_t>();
   }
   const bool multi_empty = obj == detail::OBJ_MULTI_EMPTY || obj == detail::OBJ_MULTI_EMPTY_TILED;
-  kp.vox = multi_empty ? c->objdev_host[vi] : kp.objs[0];
-  kp.vox_i = vi;
   const bool empty = obj == detail::OBJ_SINGLE_EMPTY || obj == detail::OBJ_SINGLE_EMPTY_TILED || multi_empty;
   kp.td = td;
   kp.tiled = tiled ? 1u : 0u;
   kp.bvh = walk ? c->bvh.as<rkf_bvh_node>() : nullptr;
   kp.bvh_next = walk ? c->bvh_next.as<uint32_t>() : nullptr;
   kp.use_bvh = walk ? 1u : 0u;
-  const ObjDev& e0 = kp.vox;  // the object of the empty-space path
-  kp.probe_min = empty ? 0.99f * e0.be * e0.min_scale : kMaxFloat;
+  const ObjDev& e0 = kp.objs[0];  // the object of the single-object empty-space path
+  if (!multi_empty) kp.probe_min = empty ? 0.99f * e0.be * e0.min_scale : kMaxFloat;
   kp.budget = tu.step_budget ? tu.step_budget : 32;
   kp.refill_active = 32u - std::min<uint32_t>(tu.refill_idle ? tu.refill_idle : 32u, 32u);
   kp.run_probe = tu.probe_in_run ? 1u : 0u;
@@ -1544,16 +1639,11 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
   kp.p.scene.num_objects = c->obj_count();
   // without multi_empty, several objects march the plain multi-object kernel
   int obj = object_set(c);
-  if (obj == detail::OBJ_MULTI_EMPTY && !multi_empty) obj = detail::OBJ_MULTI;
+  if (obj == detail::OBJ_MULTI_EMPTY && (!multi_empty || !fill_multi_empty(c, false, kp))) obj = detail::OBJ_MULTI;
   const bool memp = obj == detail::OBJ_MULTI_EMPTY;
-  if (memp) {
-    uint32_t vi = 0;
-    multi_empty_scene(c, &vi, kp.far, &kp.n_far);
-    kp.vox = c->objdev_host[vi];
-  }
-  const ObjDev& e0 = memp ? kp.vox : kp.objs[0];  // the object of the empty-space path
+  const ObjDev& e0 = kp.objs[0];  // the object of the single-object empty-space path
   const bool empty = obj == detail::OBJ_SINGLE_EMPTY || memp;
-  kp.probe_min = empty ? 0.99f * e0.be * e0.min_scale : kMaxFloat;
+  if (!memp) kp.probe_min = empty ? 0.99f * e0.be * e0.min_scale : kMaxFloat;
   kp.budget = tu.step_budget ? tu.step_budget : 32;
   kp.refill_active = 32u - std::min<uint32_t>(tu.refill_idle ? tu.refill_idle : 32u, 32u);
   kp.run_probe = tu.probe_in_run ? 1u : 0u;

@@ -288,11 +288,10 @@ __global__ void k_tiled_mask(const __grid_constant__ SafeArgs a) {
 
 }  // namespace detail
 
-rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st, uint32_t vi) {
+rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st, const std::vector<uint32_t>& objs) {
   if (c->tiled_epoch == c->epoch && c->tiled_empty_dist.p) return RKF_OK;
   if (c->coarse_epoch != c->epoch || !c->coarse_tex.p)
     return fail(RKF_CUDA_ERROR, "tiled march: coarse field missing for the empty-space field");
-  const ObjDev& o = c->objdev_host[vi];
   const uint32_t cd[3] = {c->coarse_dims[0], c->coarse_dims[1], c->coarse_dims[2]};
   const uint32_t nt = cd[0] * cd[1] * cd[2];
   DevBuf pre, masked, field;
@@ -305,25 +304,29 @@ rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st, uint32_t vi) {
     const uint32_t lines = axis == 0 ? cd[1] * cd[2] : axis == 1 ? cd[0] * cd[2] : cd[0] * cd[1];
     detail::k_prefix_axis<<<(lines + 127) / 128, 128, 0, st>>>(pre.as<uint32_t>(), cd[0], cd[1], cd[2], axis);
   }
-  detail::SafeArgs a;
-  a.top = c->top.as<uint32_t>();
-  a.pre = pre.as<uint32_t>();
-  a.masked = masked.as<uint32_t>();
-  a.off = o.top_off;
-  a.tx = o.tdim[0];
-  a.ty = o.tdim[1];
-  a.tz = o.tdim[2];
-  for (int d = 0; d < 3; ++d) {
-    a.cd[d] = cd[d];
-    a.lo[d] = -static_cast<double>(o.half_gs[d]) - static_cast<double>(o.m[12 + d]);
-    a.corg[d] = c->coarse_origin[d];
+  RKF_CUDA_TRY(cudaMemsetAsync(field.p, 0, std::max<uint64_t>(c->top_len, 1), st));
+  for (uint32_t vi : objs) {
+    const ObjDev& o = c->objdev_host[vi];
+    detail::SafeArgs a;
+    a.top = c->top.as<uint32_t>();
+    a.pre = pre.as<uint32_t>();
+    a.masked = masked.as<uint32_t>();
+    a.off = o.top_off;
+    a.tx = o.tdim[0];
+    a.ty = o.tdim[1];
+    a.tz = o.tdim[2];
+    for (int d = 0; d < 3; ++d) {
+      a.cd[d] = cd[d];
+      a.lo[d] = -static_cast<double>(o.half_gs[d]) - static_cast<double>(o.m[12 + d]);
+      a.corg[d] = c->coarse_origin[d];
+    }
+    a.block = 64.0 * static_cast<double>(o.vs);
+    a.cvs = 0.32;
+    const uint64_t nb = static_cast<uint64_t>(a.tx) * a.ty * a.tz;
+    detail::k_tiled_mask<<<static_cast<unsigned>((nb + 255) / 256), 256, 0, st>>>(a);
+    RKF_CUDA_TRY(cudaGetLastError());
+    if ((s2 = build_empty_dist(o, masked.as<uint32_t>(), field.as<uint8_t>(), st)) != RKF_OK) return s2;
   }
-  a.block = 64.0 * static_cast<double>(o.vs);
-  a.cvs = 0.32;
-  const uint64_t nb = static_cast<uint64_t>(a.tx) * a.ty * a.tz;
-  detail::k_tiled_mask<<<static_cast<unsigned>((nb + 255) / 256), 256, 0, st>>>(a);
-  RKF_CUDA_TRY(cudaGetLastError());
-  if ((s2 = build_empty_dist(o, masked.as<uint32_t>(), field.as<uint8_t>(), st)) != RKF_OK) return s2;
   RKF_CUDA_TRY(cudaStreamSynchronize(st));
   std::swap(c->tiled_empty_dist.p, field.p);
   std::swap(c->tiled_empty_dist.bytes, field.bytes);

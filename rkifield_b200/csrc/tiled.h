@@ -30,15 +30,16 @@ struct TiledDev {
 // and field origin relative to its camera.  Enqueued on st.
 rkf_status prepare_tiled(Ctx* c, std::vector<Segment>& segs, cudaStream_t st, TiledDev* out);
 
-// The empty-space field the tiled march of a single voxelized object (a
-// translation-only object, the empty-space path's kind) runs its EMPTY runs
-// on: the object's field with every block treated as occupied that a sample
+// The empty-space field the tiled march of voxelized objects (translation-
+// only objects, the empty-space path's kind) runs its EMPTY runs on: each
+// listed object's field with every block treated as occupied that a sample
 // inside it could see a coarse value above kCoarseSafe through (so there the
-// tiled step evaluates the object, as the brute step does).  Built into
-// c->tiled_empty_dist when the scene epoch changed; needs the coarse field of
-// the same epoch.  Enqueued on st and synchronised.
+// tiled step evaluates the object, as the brute step does); the regions of
+// other objects hold 0 (no run).  Built into c->tiled_empty_dist when the
+// scene epoch changed; needs the coarse field of the same epoch.  Enqueued on
+// st and synchronised.
 constexpr float kCoarseSafe = 0.49f;  // below COARSE_NEAR_THRESHOLD with room for mix() rounding
-rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st, uint32_t vi = 0);
+rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st, const std::vector<uint32_t>& objs);
 
 // sample_coarse_field (ray_march.wgsl:228-235) at a camera-relative position:
 // 0 outside the field, else a linear, clamp-to-edge read of the texture, with

@@ -62,9 +62,9 @@ def large():
     ctx.close()
 
 
-def oracle_scene_of(oracle, ctx, objects=None):
+def oracle_scene_of(oracle, ctx, objects=None, bvh=None):
     """An oracle scene reading the context's own pool planes and index (the
-    inputs the device march reads), with its objects."""
+    inputs the device march reads), with its objects (and BVH nodes)."""
     idx = ctx.export_index()
     leaves = idx["leaves"]
     live = leaves[leaves < 0xFFFFFFFE]
@@ -73,7 +73,7 @@ def oracle_scene_of(oracle, ctx, objects=None):
     if objects is None:
         objects = [ctx.object(i) for i in range(ctx.info()["num_objects"])]
     return oracle.Scene(objects, top=idx["top"], leaves=leaves, obj_top_info=idx["obj_top_info"],
-                        dist_f16=pl["dist"], mat_plane=pl["mat"], blend_plane=pl["blend"])
+                        dist_f16=pl["dist"], mat_plane=pl["mat"], blend_plane=pl["blend"], bvh=bvh)
 
 
 @pytest.fixture(scope="session")

@@ -150,3 +150,55 @@ def test_large_view_with_analytic_objects_rows_bit_exact(oracle, large):
                 assert_bits_equal(got[k].reshape(H, -1)[r], ref[k].reshape(1, -1)[0], f"tiled, row {r} {k}")
     finally:
         ctx.update_objects([vox])
+
+
+def test_large_view_with_voxelized_props_bit_exact(oracle, large):
+    """Several voxelized objects at full size: the 1.1 M-brick object plus
+    three small voxelized objects and two analytic ones in front of the
+    camera (the multi-object empty-space path: EMPTY runs on each voxelized
+    object's own field, outside every other object's ball).  The whole
+    1920x1080 frame bit-exact against the oracle (brute strategy) and sampled
+    rows under the tiled strategy.  Own context: the shared scene is not
+    touched."""
+    from test_multi_vox_gpu import _moved
+    from test_tiled_gpu import _analytic
+    from rkifield_b200 import _abi as abi, scenes
+    from rkifield_b200.engine import Context
+    from conftest import oracle_scene_of
+    _, spec, cam, p = large
+    prims = scenes.make_prims(spec)
+    ctx = Context(pool_capacity=1_300_000, keep_reference_pool=False)
+    try:
+        ctx.voxelize(prims, scenes.voxelize_params(spec, prims))
+        pos = np.array(cam.position[:3], np.float64)
+        fwd, right, up = (np.array(v[:3], np.float64) for v in (cam.forward, cam.right, cam.up))
+        fwd, right, up = (v / np.linalg.norm(v) for v in (fwd, right, up))
+        objs = [ctx.object(0)]
+        for i, (dist, x, y) in enumerate([(14.0, -4.0, 1.0), (30.0, 6.0, -2.0), (55.0, -9.0, 3.0)]):
+            s2 = scenes.SceneSpec(f"prop{i}_prims8_cube4m_vs2cm", 8, 4.0, 0.02, seed=70 + i)
+            pr = scenes.make_prims(s2)
+            assert ctx.voxelize(pr, scenes.voxelize_params(s2, pr)) == i + 1
+            objs.append(_moved(ctx.object(i + 1), pos + fwd * dist + right * x + up * y, 40 + i))
+        objs.append(_analytic(0, tuple(float(v) for v in pos + fwd * 20 + right * 5), (1.5,), (1.5, 1.5, 1.5), 5, 50))
+        objs.append(_analytic(1, tuple(float(v) for v in pos + fwd * 40 - up * 4), (2.0, 1.0, 1.5), (2.0, 1.0, 1.5),
+                              6, 51))
+        ctx.update_objects(objs, [0, 1, 2, 3, -1, -1])
+        sc = oracle_scene_of(oracle, ctx)
+        got = ctx.march(cam, p, W, H, reference_planes=True)
+        assert ctx.lib.rkf_testing_last_variant(ctx.h) == 4
+        ref = oracle.march(sc, cam, p, W, H, with_reference_planes=True)
+        for k in PLANES:
+            assert_bits_equal(got[k], ref[k], f"voxelized props, full frame {k}")
+        hit = (ref["flags"] & 1) != 0
+        oid = (ref["packed_material"][hit] >> 24) & 0xFF
+        assert ((oid >= 40) & (oid < 43)).sum() > 1000, "the view should see the voxelized props"
+        pt = scenes.march_params(spec)
+        pt.strategy = abi.RKF_STRATEGY_TILED
+        got = ctx.march(cam, pt, W, H, reference_planes=True)
+        assert ctx.lib.rkf_testing_last_variant(ctx.h) == 5
+        for r in (0, 480, 541, 1079):
+            ref = oracle.march(sc, cam, pt, W, H, rows=(r, r + 1), with_reference_planes=True)
+            for k in PLANES:
+                assert_bits_equal(got[k].reshape(H, -1)[r], ref[k].reshape(1, -1)[0], f"tiled, row {r} {k}")
+    finally:
+        ctx.close()
