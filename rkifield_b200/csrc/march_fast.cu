@@ -71,23 +71,25 @@ static_assert(sizeof(ColdState) % 8 == 4, "ColdState must span an odd number of 
 // value, so wherever the voxelized object samples EMPTY, the minimum over
 // the scene is that sample, bit for bit.
 struct FarBall {
-  float c[3];  // world-space centre
-  float a, b;  // radius a + b * P
+  float c[3];     // world-space centre
+  float a, b;     // radius a + b * P (box: margin a + b * P beyond the half extents)
+  uint32_t path;  // the object's index in the empty-space path (KParams::ev), or ~0u
+  float h[3];     // box: world-space half extents
+  uint32_t box;   // 1: an axis-aligned box around c instead of a ball
 };
 
-// One voxelized object of the multi-object empty-space path: EMPTY runs on
-// its own field wherever the ray lies in one of its EMPTY cubes and outside
-// the balls of all the other objects (analytic or voxelized), where its
-// EMPTY value is the scene's minimum.
+// One voxelized object of the multi-object empty-space path.  Wherever the
+// ray lies in EMPTY cubes of a set of these objects (each on its own field)
+// and outside the balls of every other object (analytic or voxelized), each
+// object of the set samples its EMPTY value and every other object a larger
+// value, so the scene's minimum is the least EMPTY value of the set.
 constexpr uint32_t kMaxEmptyVox = 8;
 struct EmptyVox {
   uint32_t obj;       // object index
-  uint32_t n_far;     // balls of the other objects
   uint32_t plain;     // zero translation and unit scale
   float probe_min;    // probe for a cube once a sample was at least this
   float empty_lo;     // lower bound of every EMPTY value (times the scale)
   float empty_lo_t, empty_hi;  // tight bounds of an EMPTY step
-  FarBall far[kMaxObjectsFast];
 };
 
 struct KParams {
@@ -115,9 +117,12 @@ struct KParams {
   const uint32_t* bvh_next;  // per node: the walk's next node (bits 0-30), descend (bit 31)
   uint32_t use_bvh;
   // multi-object empty-space path: the voxelized objects that take EMPTY
-  // runs, each with the balls of every other object
+  // runs, and a ball for every object that needs one (bounding the largest
+  // EMPTY value of the path)
   EmptyVox ev[kMaxEmptyVox];
   uint32_t n_ev;
+  FarBall ball[kMaxObjectsFast];
+  uint32_t n_ball;
 };
 static_assert(sizeof(KParams) <= 32000, "the launch parameters must fit the kernel parameter space");
 
@@ -216,7 +221,8 @@ __device__ __forceinline__ void iv_sq(float lo, float hi, float& rlo, float& rhi
 }
 
 // Largest t' >= t such that every position of the ray o + d*u, u in [t, t'],
-// lies outside every ball (kMaxFloat when no ball lies ahead); -1 when the
+// lies outside every ball (kMaxFloat when no ball lies ahead), skipping the
+// balls of the path objects in `skip` (those the run's set samples); -1 when the
 // position at t may lie inside one, with *recheck set to the earliest time
 // the ray may leave the balls that may hold it (else -1).  Per ball, with
 // w = o - c: the line's squared distance to the centre is |w|^2 - (d.w)^2/|d|^2,
@@ -227,8 +233,8 @@ __device__ __forceinline__ void iv_sq(float lo, float hi, float& rlo, float& rhi
 // a zero direction) makes every ball near.  Out of line: the march loop
 // calls it about once per ray, and its code would otherwise sit among the
 // loop's hot paths (measured 3% faster out of line).
-__device__ __noinline__ float far_limit(const FarBall* __restrict__ far, uint32_t n, float ox, float oy,
-                                           float oz, float dx, float dy, float dz, float tmax, float t,
+__device__ __noinline__ float far_limit(const FarBall* __restrict__ far, uint32_t n, uint32_t skip, float ox,
+                                           float oy, float oz, float dx, float dy, float dz, float tmax, float t,
                                            float& recheck) {
   const float a_lo = __fadd_rd(__fadd_rd(__fmul_rd(dx, dx), __fmul_rd(dy, dy)), __fmul_rd(dz, dz));
   const float a_hi = __fadd_ru(__fadd_ru(__fmul_ru(dx, dx), __fmul_ru(dy, dy)), __fmul_ru(dz, dz));
@@ -240,6 +246,37 @@ __device__ __noinline__ float far_limit(const FarBall* __restrict__ far, uint32_
   recheck = kMaxFloat;
   for (uint32_t j = 0; j < n; ++j) {
     const FarBall& f = far[j];
+    if (f.path < 32u && ((skip >> f.path) & 1u)) continue;  // an object of the run's set
+    if (f.box) {
+      // slab test of the box [c - h - m, c + h + m], m = a + b*P: the entry
+      // time rounded down and the exit time rounded up
+      const float m = __fadd_ru(f.a, __fmul_ru(f.b, P));
+      const float o3[3] = {ox, oy, oz}, d3[3] = {dx, dy, dz};
+      float e = -kMaxFloat, x = kMaxFloat;
+      bool miss = false;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float hw = __fadd_ru(f.h[k], m);
+        const float lo = __fsub_rd(f.c[k], hw), hi = __fadd_ru(f.c[k], hw);
+        if (d3[k] > 0.0f) {
+          e = fmaxf(e, __fdiv_rd(__fsub_rd(lo, o3[k]), d3[k]));
+          x = fminf(x, __fdiv_ru(__fsub_ru(hi, o3[k]), d3[k]));
+        } else if (d3[k] < 0.0f) {
+          e = fmaxf(e, __fdiv_rd(__fsub_ru(hi, o3[k]), d3[k]));
+          x = fminf(x, __fdiv_ru(__fsub_rd(lo, o3[k]), d3[k]));
+        } else if (!(o3[k] >= lo && o3[k] <= hi)) {
+          miss = true;  // parallel to this slab and outside it (NaN: not a miss)
+        }
+      }
+      if (miss || e > x) continue;
+      if (t < e) {
+        lim = fminf(lim, e);
+      } else if (!(t > x)) {  // may be inside now (or NaN)
+        inside = true;
+        recheck = fminf(recheck, x);
+      }
+      continue;
+    }
     const float rho = __fadd_ru(f.a, __fmul_ru(f.b, P));
     const float rho2 = __fmul_ru(rho, rho);
     const float wxl = __fsub_rd(ox, f.c[0]), wxh = __fsub_ru(ox, f.c[0]);
@@ -576,6 +613,56 @@ __device__ __forceinline__ uint32_t empty_run_x2(const ObjDev& o, const uint8_t*
   return c;
 }
 
+// Up to n march steps through positions where every object of the set
+// (path objects, at least two) samples its EMPTY value and every other
+// object lies beyond its ball: each step's value is the least of the set's
+// EMPTY values, computed as eval_obj -> sample_vox would round it.  The run
+// stops at the end of the nearest cube (box_t, already clipped at the first
+// ball ahead), before a step whose value is below brk, and after the step
+// that makes max_near values below near_thr; CLEAN: the values clear every
+// threshold (a lower bound checked by the caller).  Returns the steps taken.
+template <bool CLEAN>
+__device__ __noinline__ uint32_t empty_run_set(const ObjDev* objs, const EmptyVox* ev, uint32_t set, uint32_t n_ev,
+                                               float ox, float oy, float oz, float dx, float dy, float dz, float tmax,
+                                               uint32_t n, float brk, float near_thr, float min_step,
+                                               uint32_t max_near, float& t, float box_t, float& prev_t,
+                                               float& prev_dist, uint32_t& near, bool& stop_full) {
+  uint32_t c = 0;
+  const float lim = fminf(box_t, tmax);
+  stop_full = false;
+  for (; c < n; ++c) {
+    if (t > lim) {
+      stop_full = t > tmax;
+      break;
+    }
+    float d = kMaxFloat;
+    for (uint32_t e = 0; e < n_ev; ++e) {
+      if (!((set >> e) & 1u)) continue;
+      const ObjDev& o = objs[ev[e].obj];
+      const float v = empty_value(o, grid_coord(ox, dx, t, o.m[12], o.half_gs[0]),
+                                  grid_coord(oy, dy, t, o.m[13], o.half_gs[1]),
+                                  grid_coord(oz, dz, t, o.m[14], o.half_gs[2]));
+      if (v < d) d = v;
+    }
+    if (!CLEAN && !(d >= brk)) {  // no step: the full step redoes this sample
+      stop_full = true;
+      break;
+    }
+    prev_t = t;
+    prev_dist = d;
+    if (CLEAN) {
+      t = __fadd_rn(t, d);
+      continue;
+    }
+    t = __fadd_rn(t, fmax_(d, min_step));
+    if (d < near_thr && ++near >= max_near) {
+      stop_full = true;
+      return c + 1;
+    }
+  }
+  return c;
+}
+
 template <int PREC, int OBJ>
 __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_constant__ KParams kp) {
   constexpr bool MULTI_TILED = OBJ == OBJ_MULTI_EMPTY_TILED;
@@ -745,44 +832,56 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
         // a ray that may be inside a ball takes full steps until it may have left
         const bool probe = t > box_t && prev_dist >= kp.probe_min && (!MULTI_EMPTY || t > far_recheck);
         if (MULTI_EMPTY && probe) {
-          // the first voxelized object of the path (that the ray may take runs
-          // on) whose EMPTY cube holds the ray
-          const uint32_t cur = cs.vox_listed >> 8;
-          uint32_t found = kMaxEmptyVox;
-          box_t = -1.0f;
-          for (uint32_t e = 0; e < kp.n_ev && found == kMaxEmptyVox; ++e) {
+          // the set of voxelized objects of the path (that the ray may take
+          // runs on) whose EMPTY cubes hold the ray; the run lasts while it is
+          // in all of them
+          uint32_t set = 0;
+          box_t = kMaxFloat;
+          for (uint32_t e = 0; e < kp.n_ev; ++e) {
             if (!((cs.vox_listed >> e) & 1u)) continue;
             const float bt = probe_empty(sh_objs[kp.ev[e].obj], s.empty_dist, ox, oy, oz, dx, dy, dz, t);
             if (t <= bt) {
-              found = e;
-              box_t = bt;
+              set |= 1u << e;
+              box_t = fminf(box_t, bt);
             }
           }
-          if (found != kMaxEmptyVox && found != cur) {
-            // another object's cube: the balls that bound it are others
-            cs.vox_listed = (cs.vox_listed & 0xFFu) | (found << 8);
+          if (!set) box_t = -1.0f;
+          if (set && set != (cs.vox_listed >> 8)) {
+            // other objects in the set: the balls that bound the run are others
+            cs.vox_listed = (cs.vox_listed & 0xFFu) | (set << 8);
             far_t = far_recheck = -1.0f;
           }
         }
-        const EmptyVox& ev = kp.ev[MULTI_EMPTY ? (cs.vox_listed >> 8) : 0u];
+        const uint32_t set = MULTI_EMPTY ? (cs.vox_listed >> 8) : 1u;
+        const bool one = (set & (set - 1u)) == 0u;  // one object's EMPTY value
+        const EmptyVox& ev = kp.ev[MULTI_EMPTY ? (__ffs(set | 1u) - 1) : 0];
         const ObjDev& o0 = sh_objs[MULTI_EMPTY ? ev.obj : 0u];
-        const float e_lo = MULTI_EMPTY ? ev.empty_lo : kp.empty_lo;
-        const float e_hi = MULTI_EMPTY ? ev.empty_hi : kp.empty_hi;
-        const float e_lo_t = MULTI_EMPTY ? ev.empty_lo_t : kp.empty_lo_t;
-        const uint32_t plain = MULTI_EMPTY ? ev.plain : kp.plain_obj;
+        float e_lo = MULTI_EMPTY ? ev.empty_lo : kp.empty_lo;
+        float e_hi = MULTI_EMPTY ? ev.empty_hi : kp.empty_hi;
+        float e_lo_t = MULTI_EMPTY ? ev.empty_lo_t : kp.empty_lo_t;
+        if (MULTI_EMPTY && !one) {
+          for (uint32_t e = 0; e < kp.n_ev; ++e) {
+            if (!((set >> e) & 1u)) continue;
+            e_lo = fminf(e_lo, kp.ev[e].empty_lo);
+            e_lo_t = fminf(e_lo_t, kp.ev[e].empty_lo_t);
+            e_hi = fmaxf(e_hi, kp.ev[e].empty_hi);
+          }
+        }
+        const uint32_t plain = MULTI_EMPTY ? (one ? ev.plain : 0u) : kp.plain_obj;
         const bool clean = e_lo >= brk && e_lo >= near_thr && e_lo >= min_step;
         if (probe) {
           if (!MULTI_EMPTY) box_t = probe_empty(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, t);
           const float cube_t = box_t;
           if (MULTI_EMPTY) {
-            // only positions outside every ball sample the EMPTY value.  far_t
-            // (the first entry into a ball ahead) stays valid until the ray
-            // passes it: balls ahead stay ahead, balls behind stay behind.
+            // only positions outside the balls of every object not in the set
+            // sample the set's EMPTY values.  far_t (the first entry into such
+            // a ball ahead) stays valid until the ray passes it: balls ahead
+            // stay ahead, balls behind stay behind.
             if (t <= box_t && t > far_t)
-              far_t = far_limit(ev.far, ev.n_far, ox, oy, oz, dx, dy, dz, tmax, t, far_recheck);
+              far_t = far_limit(kp.ball, kp.n_ball, set, ox, oy, oz, dx, dy, dz, tmax, t, far_recheck);
             box_t = fminf(box_t, far_t);
           }
-          if (t <= box_t && clean && kp.settle_links && step < max_step && near < max_near) {
+          if (t <= box_t && clean && one && kp.settle_links && step < max_step && near < max_near) {
             // Settle the ray if every sample it has left is the EMPTY value:
             // then no threshold acts on it, it misses, and its outputs do not
             // depend on its exact t.  t after k more steps lies in
@@ -819,7 +918,15 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
           const uint32_t n = step < max_step ? min(kp.budget, max_step - step) : 0u;
           uint32_t c = 0;
           bool stop_full = true;
-          if (near < max_near) {
+          if (near < max_near && MULTI_EMPTY && !one) {
+            // several objects: the least of their EMPTY values, to the end of
+            // the nearest cube
+            c = clean ? empty_run_set<true>(sh_objs, kp.ev, set, kp.n_ev, ox, oy, oz, dx, dy, dz, tmax, n, brk,
+                                            near_thr, min_step, max_near, t, box_t, prev_t, prev_dist, near, stop_full)
+                      : empty_run_set<false>(sh_objs, kp.ev, set, kp.n_ev, ox, oy, oz, dx, dy, dz, tmax, n, brk,
+                                             near_thr, min_step, max_near, t, box_t, prev_t, prev_dist, near,
+                                             stop_full);
+          } else if (near < max_near) {
 #define RKF_RUN(P, CL, IN)                                                                                   \
   empty_run<P, CL, IN, MULTI_EMPTY>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n, brk, near_thr, min_step, \
                                     max_near, far_t, t, box_t, prev_t, prev_dist, near, stop_full)
@@ -1275,8 +1382,33 @@ bool far_ball(const ObjDev& o, float empty_hi, detail::FarBall* out) {
   // box (a box inside |l| <= |half_gs|) wherever that distance exceeds two
   // brick extents (ray_march.wgsl:371-376), so beyond the ball of radius
   // |half_gs| + max(2 * brick extent, EMPTY value / scale) its value is at
-  // least that distance times its scale, above every EMPTY value.
+  // least that distance times its scale, above every EMPTY value.  With a
+  // translation-only transform the grid box is axis-aligned in world space,
+  // and the same holds outside the box widened by that distance (a position
+  // beyond it along one axis is that far from the box): the tighter bound.
   const bool vox = o.sdf_type == RKF_SDF_VOXELIZED;
+  std::memset(out, 0, sizeof(*out));
+  out->path = ~0u;
+  if (vox && o.translate_only) {
+    const double s = o.min_scale;
+    if (!(s > 0.0) || !std::isfinite(s)) return false;
+    const double e16 = 0x1p-16, e20 = 0x1p-20;
+    const double need = std::max(static_cast<double>(empty_hi) * (1.0 + e16) / s,
+                                 static_cast<double>(o.be2) * (1.0 + e16));
+    double tn = 0.0, hn = 0.0;
+    for (int i = 0; i < 3; ++i) {
+      out->c[i] = -o.m[12 + i];  // local = world + m: the local origin (grid centre) in world space
+      out->h[i] = static_cast<float>(up_float(static_cast<double>(o.half_gs[i]) * (1.0 + e16)));
+      tn += static_cast<double>(o.m[12 + i]) * o.m[12 + i];
+      hn += static_cast<double>(o.half_gs[i]) * o.half_gs[i];
+    }
+    out->a = static_cast<float>(up_float(need + e16 * (std::sqrt(tn) + std::sqrt(hn)) + e20 * std::sqrt(tn)));
+    out->b = static_cast<float>(up_float(3.0 * e16 + e20));
+    out->box = 1;
+    return std::isfinite(out->a) && std::isfinite(out->h[0]) && std::isfinite(out->h[1]) &&
+           std::isfinite(out->h[2]) && std::isfinite(out->c[0]) && std::isfinite(out->c[1]) &&
+           std::isfinite(out->c[2]);
+  }
   const double R = vox ? std::sqrt(static_cast<double>(o.half_gs[0]) * o.half_gs[0] +
                                    static_cast<double>(o.half_gs[1]) * o.half_gs[1] +
                                    static_cast<double>(o.half_gs[2]) * o.half_gs[2])
@@ -1325,45 +1457,58 @@ bool far_ball(const ObjDev& o, float empty_hi, detail::FarBall* out) {
 // A scene of several objects the multi-object empty-space path can march:
 // one to kMaxEmptyVox voxelized objects that qualify for the empty-space path
 // (the first ones by index), each of which takes EMPTY runs on its own field,
-// and every other object -- analytic, voxelized (qualifying or not) or of no
-// type -- bounded by a ball outside which its value exceeds that object's
-// EMPTY values.  Fills ev (the path's objects with their balls) when given.
-bool multi_empty_scene(const Ctx* c, detail::EmptyVox* ev, uint32_t* n_ev) {
+// and every object -- analytic, voxelized (on the path or not) or of no type
+// -- either bounded by a ball outside which its value exceeds every EMPTY
+// value of the path, or (no type, unknown primitives) never below them.
+// Fills ev and the balls (with each ball's path index) when given.
+bool multi_empty_scene(const Ctx* c, detail::EmptyVox* ev, uint32_t* n_ev, detail::FarBall* balls,
+                       uint32_t* n_ball) {
   const uint32_t n = c->obj_count();
   if (n < 2 || n > kMaxObjectsFast) return false;
   uint32_t q[detail::kMaxEmptyVox];
+  uint32_t path_of[kMaxObjectsFast];
   uint32_t nq = 0;
-  for (uint32_t i = 0; i < n && nq < detail::kMaxEmptyVox; ++i)
-    if (empty_object(c, c->objdev_host[i])) q[nq++] = i;
+  for (uint32_t i = 0; i < n; ++i) {
+    path_of[i] = ~0u;
+    if (nq < detail::kMaxEmptyVox && empty_object(c, c->objdev_host[i])) {
+      path_of[i] = nq;
+      q[nq++] = i;
+    }
+  }
   if (nq == 0) return false;
-  for (uint32_t j = 0; j < nq; ++j) {
+  float hi = 0.0f;  // the largest EMPTY value of the path
+  for (uint32_t j = 0; j < nq; ++j) hi = std::max(hi, empty_hi_of(c->objdev_host[q[j]]));
+  uint32_t nb = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const ObjDev& o = c->objdev_host[i];
+    if (o.sdf_type == RKF_SDF_NONE) continue;  // no type: kMaxFloat
+    if (o.sdf_type == RKF_SDF_ANALYTICAL && o.prim_type > RKF_PRIM_PLANE) {
+      // an unknown primitive: kMaxFloat * min_scale
+      if (static_cast<double>(kMaxFloat) * o.min_scale * (1.0 - 0x1p-20) >= hi) continue;
+      return false;
+    }
+    detail::FarBall b;
+    if (!far_ball(o, hi, &b)) return false;
+    b.path = path_of[i];
+    if (balls) balls[nb] = b;
+    ++nb;
+  }
+  for (uint32_t j = 0; ev && j < nq; ++j) {
     const ObjDev& a = c->objdev_host[q[j]];
-    const float hi = empty_hi_of(a);
     detail::EmptyVox e;
     std::memset(&e, 0, sizeof(e));
     e.obj = q[j];
-    for (uint32_t i = 0; i < n; ++i) {
-      const ObjDev& o = c->objdev_host[i];
-      if (i == q[j] || o.sdf_type == RKF_SDF_NONE) continue;  // no type: kMaxFloat
-      if (o.sdf_type == RKF_SDF_ANALYTICAL && o.prim_type > RKF_PRIM_PLANE) {
-        // an unknown primitive: kMaxFloat * min_scale
-        if (static_cast<double>(kMaxFloat) * o.min_scale * (1.0 - 0x1p-20) >= hi) continue;
-        return false;
-      }
-      detail::FarBall b;
-      if (!far_ball(o, hi, &b)) return false;
-      e.far[e.n_far++] = b;
-    }
     e.probe_min = 0.99f * a.be * a.min_scale;
     // mix(c, c, t) three times stays within 12 roundings of c (relative
     // 2^-24 each); 0.999 leaves a wide margin, 2^-16 a tight one
     e.empty_lo = 0.999f * a.be * a.min_scale;
     e.empty_lo_t = a.be * a.min_scale * (1.0f - 1.52587890625e-5f);
-    e.empty_hi = hi;
+    e.empty_hi = empty_hi_of(a);
     e.plain = (a.m[12] == 0.0f && a.m[13] == 0.0f && a.m[14] == 0.0f && a.min_scale == 1.0f) ? 1u : 0u;
-    if (ev) ev[j] = e;
+    ev[j] = e;
   }
   if (n_ev) *n_ev = nq;
+  if (n_ball) *n_ball = nb;
   return true;
 }
 
@@ -1411,22 +1556,29 @@ bool bvh_reaches(const Ctx* c, uint32_t vi) {
 bool fill_multi_empty(const Ctx* c, bool walk, detail::KParams& kp) {
   detail::EmptyVox ev[detail::kMaxEmptyVox];
   uint32_t n = 0;
-  if (!multi_empty_scene(c, ev, &n)) return false;
+  if (!multi_empty_scene(c, ev, &n, kp.ball, &kp.n_ball)) return false;
+  // an object the walk may not reach leaves the path (its ball still bounds
+  // the others' runs)
+  uint32_t remap[detail::kMaxEmptyVox];
   kp.n_ev = 0;
   kp.probe_min = kMaxFloat;
   for (uint32_t j = 0; j < n; ++j) {
+    remap[j] = ~0u;
     if (walk && !bvh_reaches(c, ev[j].obj)) continue;
+    remap[j] = kp.n_ev;
     kp.ev[kp.n_ev] = ev[j];
     kp.probe_min = std::min(kp.probe_min, ev[j].probe_min);
     ++kp.n_ev;
   }
+  for (uint32_t b = 0; b < kp.n_ball; ++b)
+    if (kp.ball[b].path < n) kp.ball[b].path = remap[kp.ball[b].path];
   return kp.n_ev > 0;
 }
 
 // Which kernel variant a launch over this context's objects uses.
 int object_set(const Ctx* c) {
   if (c->obj_count() != 1)
-    return multi_empty_scene(c, nullptr, nullptr) ? detail::OBJ_MULTI_EMPTY : detail::OBJ_MULTI;
+    return multi_empty_scene(c, nullptr, nullptr, nullptr, nullptr) ? detail::OBJ_MULTI_EMPTY : detail::OBJ_MULTI;
   return empty_object(c, c->objdev_host[0]) ? detail::OBJ_SINGLE_EMPTY : detail::OBJ_SINGLE;
 }
 }  // namespace
@@ -1483,7 +1635,7 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
     if (objs == detail::OBJ_MULTI_EMPTY) {
       detail::EmptyVox ev[detail::kMaxEmptyVox];
       uint32_t n = 0;
-      multi_empty_scene(c, ev, &n);
+      multi_empty_scene(c, ev, &n, nullptr, nullptr);
       path.clear();
       for (uint32_t j = 0; j < n; ++j) path.push_back(ev[j].obj);
     }
