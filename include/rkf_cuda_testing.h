@@ -58,6 +58,23 @@ RKF_API int rkf_testing_far_ball(const rkf_gpu_object* obj, float empty_hi, floa
  * while no edit runs (a serving session between requests, or no session). */
 RKF_API rkf_status rkf_testing_pool_state(rkf_ctx* ctx, uint32_t out[5]);
 
+/* Launch accounting.  enable = 1 starts timing the context's persistent
+ * march launches (the kernel of rkf_march, rkf_march_async,
+ * rkf_march_rays, rkf_march_batch and their variants) with a pair of CUDA
+ * events on each launch's stream around the kernel alone, discarding the
+ * launches timed before; 0 stops it.  At most 4096 launches are timed.
+ * RKF_BUSY while a serving session runs. */
+RKF_API rkf_status rkf_testing_march_timing(rkf_ctx* ctx, uint32_t enable);
+
+/* *launches (may be NULL): kernels the context has launched since it was
+ * created, on any stream (march, tile order, tiled-strategy preparation,
+ * voxelization, edits, imports, queries).  *n_timed (may be NULL): launches
+ * timed since timing was switched on; march_ms[i] receives the device time
+ * of the i-th of them, for i < min(cap, *n_timed), waiting for each to
+ * finish. */
+RKF_API rkf_status rkf_testing_launch_stats(rkf_ctx* ctx, uint64_t* launches, float* march_ms, uint32_t cap,
+                                            uint32_t* n_timed);
+
 #ifdef __cplusplus
 }
 #endif

@@ -252,6 +252,8 @@ SIGNATURES = {
     "rkf_testing_last_variant": (C.c_int, [_P]),
     "rkf_testing_far_ball": (C.c_int, [_P, C.c_float, _P]),
     "rkf_testing_pool_state": (_I, [_P, _P]),
+    "rkf_testing_march_timing": (_I, [_P, C.c_uint32]),
+    "rkf_testing_launch_stats": (_I, [_P, C.POINTER(C.c_uint64), _P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "rkf_world_relative": (None, [C.POINTER(rkf_world_pos), C.POINTER(rkf_world_pos),
                                   C.POINTER(C.c_double), C.POINTER(C.c_float)]),
     "rkf_scene_origin_set": (_I, [_P, C.POINTER(rkf_world_pos)]),

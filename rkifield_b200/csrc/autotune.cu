@@ -7,11 +7,15 @@
 // warp re-converges), the refill threshold (idle lanes that make a warp
 // refill), where a lane probes its next EMPTY cube (inside a run or between
 // runs), the block size, whether it runs EMPTY runs at all and whether views
-// hand out their heaviest ray tiles first.  rkf_autotune times candidates on the caller's
-// sample of the work with CUDA events: every tile x interval x block size at
-// the default budget and threshold, then every budget, then every threshold,
-// then the other probe placement, then the heaviest-first tile order, then
-// the march without EMPTY runs, each at the best so far.
+// hand out their heaviest ray tiles first.  rkf_autotune times candidates on
+// the caller's sample of the work with CUDA events: every tile x interval x
+// block size at the default budget and threshold, then the heaviest-first
+// tile order, then every budget, then every threshold, then the other probe
+// placement, then the march without EMPTY runs, each at the best so far.
+// Each timed launch starts with the L2 cache flushed (a write of twice its
+// size, outside the timed events), as a frame does after other work: with
+// the index left in L2 by the previous trial, the knobs that cut DRAM
+// traffic (tile shape, tile order) would look worth less than they are.
 // The fastest is kept in the context, where rkf_march and rkf_march_batch
 // use it.
 #include <cfloat>
@@ -42,12 +46,25 @@ extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t
   rkf_batch_tuning best = c->tuning;
   float best_ms = FLT_MAX;
   rkf_status st = RKF_OK;
-  // one untimed launch, then the best of two timed ones
+  // the flush buffer lives for this call only (no flush when the device has
+  // no room for it)
+  int l2_bytes = 0;
+  cudaDeviceGetAttribute(&l2_bytes, cudaDevAttrL2CacheSize, c->device);
+  DevBuf flush;
+  if (l2_bytes > 0 && flush.alloc(2 * static_cast<size_t>(l2_bytes)) != RKF_OK) {
+    flush.release();
+    cudaGetLastError();
+  }
+  // one untimed launch, then the best of two timed ones, each after a flush
   auto trial = [&](const rkf_batch_tuning& tu) {
     st = rkf_march_batch_async(ctx, views, n_views, batches, n_batches, p, &tu, nullptr);
     if (st != RKF_OK) return;
     float ms = FLT_MAX;
     for (int r = 0; r < 2; ++r) {
+      if (flush.p && cudaMemsetAsync(flush.p, r + 1, flush.bytes, c->stream) != cudaSuccess) {
+        st = fail(RKF_CUDA_ERROR, "rkf_autotune: L2 flush failed");
+        return;
+      }
       cudaEventRecord(e0, c->stream);
       st = rkf_march_batch_async(ctx, views, n_views, batches, n_batches, p, &tu, nullptr);
       if (st != RKF_OK) return;
@@ -69,6 +86,13 @@ extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t
     for (uint32_t iv : intervals)
       for (uint32_t th : threads)
         if (st == RKF_OK) trial(rkf_batch_tuning{tl[0], tl[1], 32, iv, 0, th, 32, 0, 0});
+  // heaviest tiles first (views on the empty-space path), before the
+  // finer knobs so that they are tuned with the order that wins
+  if (st == RKF_OK && n_views) {
+    rkf_batch_tuning tu = best;
+    tu.order_tiles = 1;
+    trial(tu);
+  }
   const rkf_batch_tuning base = best;
   for (uint32_t b : budgets) {
     if (st != RKF_OK) break;
@@ -86,12 +110,6 @@ extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t
   if (st == RKF_OK) {
     rkf_batch_tuning tu = best;
     tu.probe_in_run = 1;
-    trial(tu);
-  }
-  // heaviest tiles first (views on the empty-space path)
-  if (st == RKF_OK && n_views) {
-    rkf_batch_tuning tu = best;
-    tu.order_tiles = 1;
     trial(tu);
   }
   // where EMPTY runs do not pay (a camera outside a dense grid: short runs,

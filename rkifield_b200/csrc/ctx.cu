@@ -167,6 +167,7 @@ rkf_status Ctx::verify_exact_div() {
     RKF_CUDA_TRY(cudaMemsetAsync(bad.p, 0, 4, stream));
     detail::k_verify_div<<<sm_count * 8, 256, 0, stream>>>(d.vs, d.rcp_vs, b0, b1 - b0 + 1,
                                                           bad.as<unsigned int>());
+    counted();
     RKF_CUDA_TRY(cudaGetLastError());
     unsigned int nbad = 0;
     RKF_CUDA_TRY(cudaMemcpyAsync(&nbad, bad.p, 4, cudaMemcpyDeviceToHost, stream));
@@ -218,6 +219,21 @@ rkf_status Ctx::ensure_leaf_capacity(uint32_t need) {
 rkf_status Ctx::stage_bytes(size_t bytes) {
   if (stage.bytes >= bytes) return RKF_OK;
   return stage.alloc(bytes + bytes / 4);
+}
+
+rkf_status Ctx::march_event(cudaStream_t st, bool end) {
+  // (the serving loop's launches are not timed: its worker thread would
+  // share the event list with the caller)
+  if (!time_march || serve || march_timed >= kMaxTimed) return RKF_OK;
+  const size_t k = 2 * static_cast<size_t>(march_timed) + (end ? 1 : 0);
+  if (k >= march_ev.size()) {
+    cudaEvent_t e = nullptr;
+    RKF_CUDA_TRY(cudaEventCreate(&e));
+    march_ev.push_back(e);
+  }
+  RKF_CUDA_TRY(cudaEventRecord(march_ev[k], st));
+  if (end) ++march_timed;
+  return RKF_OK;
 }
 
 namespace detail {
@@ -275,6 +291,7 @@ rkf_status lookup_bricks(Ctx* c, uint32_t obj, const uint32_t* d_bxyz, uint32_t 
                          cudaStream_t st) {
   if (n == 0) return RKF_OK;
   detail::k_lookup<<<(n + 255) / 256, 256, 0, st>>>(c->scene_dev(), obj, d_bxyz, n, d_out);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   return RKF_OK;
 }
@@ -423,6 +440,7 @@ rkf_status rkf_destroy(rkf_ctx* ctx) {
   for (cudaEvent_t e : c->band_ev)
     if (e) cudaEventDestroy(e);
   if (c->segs_ev) cudaEventDestroy(c->segs_ev);
+  for (cudaEvent_t e : c->march_ev) cudaEventDestroy(e);
   delete c;
   return RKF_OK;
 }
@@ -438,6 +456,7 @@ rkf_status finish_pool_import(Ctx* c, uint32_t first_slot, uint32_t n_bricks) {
     k_encode_u8<<<n_bricks, 256, 0, c->stream>>>(nullptr, c->dist_f16.as<uint16_t>(), first_slot, n_bricks,
                                                  c->dist_u8.as<int8_t>(), c->brick_step.as<float>(), band,
                                                  c->cfg.u8_round == 1);
+    c->counted();
     RKF_CUDA_TRY(cudaGetLastError());
   }
   RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -475,6 +494,7 @@ rkf_status rkf_pool_import_soa(rkf_ctx* ctx, const uint16_t* dist_f16, const uin
       reinterpret_cast<const uint8_t*>(b + 2 * b16), nvox, static_cast<uint64_t>(first_slot) * 512,
       c->dist_f16.as<uint16_t>(), c->dist_f32.as<float>(), c->mat.as<uint16_t>(), c->blend.as<uint8_t>(),
       c->aos.as<uint2>());
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   return finish_pool_import(c, first_slot, n_bricks);
 }
@@ -498,6 +518,7 @@ rkf_status rkf_pool_import_voxelsample(rkf_ctx* ctx, const uint32_t* words, uint
                                                 c->dist_f16.as<uint16_t>(), c->dist_f32.as<float>(),
                                                 c->mat.as<uint16_t>(), c->blend.as<uint8_t>(),
                                                 c->aos.as<uint2>());
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   return finish_pool_import(c, first_slot, n_bricks);
 }
@@ -602,6 +623,7 @@ rkf_status rkf_objects_import(rkf_ctx* ctx, const rkf_gpu_object* objects, uint3
   if (!top.empty()) RKF_CUDA_TRY(cudaMemcpy(ntop.p, top.data(), top.size() * 4, cudaMemcpyHostToDevice));
   for (const ObjDev& d : od)
     if ((st = build_empty_dist(d, ntop.as<uint32_t>(), nfield.as<uint8_t>(), c->stream)) != RKF_OK) return st;
+    c->counted(3);
   std::vector<rkf_gpu_object> objects0(objects, objects + n);
   std::swap(c->objects, objects0);
   std::swap(c->objdev_host, od);
@@ -743,6 +765,29 @@ rkf_status rkf_testing_export_empty_dist(rkf_ctx* ctx, uint8_t* out, uint64_t* n
   return RKF_OK;
 }
 
+rkf_status rkf_testing_march_timing(rkf_ctx* ctx, uint32_t enable) {
+  if (!ctx || enable > 1) return fail(RKF_INVALID_ARG, "rkf_testing_march_timing: bad argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (c->serve) return fail(RKF_BUSY, "rkf_testing_march_timing: the context is serving");
+  c->time_march = enable != 0;
+  c->march_timed = 0;
+  return RKF_OK;
+}
+
+rkf_status rkf_testing_launch_stats(rkf_ctx* ctx, uint64_t* launches, float* march_ms, uint32_t cap,
+                                    uint32_t* n_timed) {
+  if (!ctx || (!march_ms && cap)) return fail(RKF_INVALID_ARG, "rkf_testing_launch_stats: null argument");
+  Ctx* c = reinterpret_cast<Ctx*>(ctx);
+  if (launches) *launches = c->launches.load();
+  if (n_timed) *n_timed = c->march_timed;
+  if (cap) RKF_CUDA_TRY(cudaSetDevice(c->device));
+  for (uint32_t i = 0; i < std::min(cap, c->march_timed); ++i) {
+    RKF_CUDA_TRY(cudaEventSynchronize(c->march_ev[2 * i + 1]));
+    RKF_CUDA_TRY(cudaEventElapsedTime(&march_ms[i], c->march_ev[2 * i], c->march_ev[2 * i + 1]));
+  }
+  return RKF_OK;
+}
+
 rkf_status rkf_brick_lookup(rkf_ctx* ctx, uint32_t obj, const uint32_t* bxyz, uint32_t n,
                             uint32_t* slots) {
   if (!ctx || ((!bxyz || !slots) && n)) return fail(RKF_INVALID_ARG, "rkf_brick_lookup: null argument");
@@ -758,6 +803,7 @@ rkf_status rkf_brick_lookup(rkf_ctx* ctx, uint32_t obj, const uint32_t* bxyz, ui
   uint32_t* dout = din + 3 * static_cast<size_t>(n);
   RKF_CUDA_TRY(cudaMemcpyAsync(din, bxyz, static_cast<size_t>(n) * 12, cudaMemcpyHostToDevice, c->stream));
   detail::k_lookup<<<(n + 255) / 256, 256, 0, c->stream>>>(c->scene_dev(), obj, din, n, dout);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   RKF_CUDA_TRY(cudaMemcpyAsync(slots, dout, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost, c->stream));
   RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));

@@ -134,13 +134,24 @@ struct Ctx {
   DevBuf order_buf;  // heaviest-first tile order of views (tile_order.h)
   DevBuf counters;   // work counters of the persistent kernels
   DevBuf seg_buf;    // segment table of the persistent kernel
-  DevBuf l2_flush;
 
   // batching
   rkf_batch_tuning tuning{};
   bool tuned = false;
 
   ServeState* serve = nullptr;  // owned; created by rkf_serve_start
+
+  // launch accounting (rkf_testing_launch_stats): every kernel the context
+  // launches is counted; while march timing is on, each persistent march
+  // launch is bracketed by a pair of events on its stream
+  static constexpr uint32_t kMaxTimed = 4096;
+  std::atomic<uint64_t> launches{0};
+  bool time_march = false;
+  std::vector<cudaEvent_t> march_ev;  // start, end of each timed launch
+  uint32_t march_timed = 0;           // launches timed since timing was switched on
+  void counted(uint32_t n = 1) { launches.fetch_add(n, std::memory_order_relaxed); }
+  // records the start (end = false) or end event of a timed march launch
+  rkf_status march_event(cudaStream_t st, bool end);
 
   SceneDev scene_dev() const;
   uint32_t obj_count() const { return static_cast<uint32_t>(objects.size()); }

@@ -383,6 +383,7 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   ka.u8_band = c->cfg.u8_band > 0.0f ? c->cfg.u8_band : 3.0f * vs;
   ka.u8_nearest = c->cfg.u8_round == 1 ? 1u : 0u;
   detail::k_edit<<<n, 512, 0, st>>>(ka);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   std::vector<uint8_t> changed(n);
   RKF_CUDA_TRY(cudaMemcpyAsync(changed.data(), d_changed, n, cudaMemcpyDeviceToHost, st));
@@ -437,6 +438,7 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   RKF_CUDA_TRY(cudaMemcpyAsync(d_blocks, blocks.data(), nb * 4ull, cudaMemcpyHostToDevice, st));
   detail::k_gather_blocks<<<nb, 128, 0, st>>>(c->top.as<uint32_t>(), c->leaves.as<uint32_t>(), d_blocks, nb,
                                               d_topv, d_leafs);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   std::vector<uint32_t> leafv(static_cast<size_t>(nb) * 512), oldtop(nb);
   RKF_CUDA_TRY(cudaMemcpyAsync(leafv.data(), d_leafs, leafv.size() * 4, cudaMemcpyDeviceToHost, st));
@@ -465,12 +467,14 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   RKF_CUDA_TRY(cudaMemcpyAsync(ntop, c->top.p, c->top_len * 4, cudaMemcpyDeviceToDevice, st));
   RKF_CUDA_TRY(cudaMemcpyAsync(d_topv, newtop.data(), nb * 4ull, cudaMemcpyHostToDevice, st));
   detail::k_scatter_top<<<(nb + 127) / 128, 128, 0, st>>>(ntop, d_blocks, d_topv, nb);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   // the touched blocks are leaf blocks now: lower the field around them
   if (!into && (s2 = out->new_empty_dist.alloc(std::max<uint64_t>(c->top_len, 1))) != RKF_OK) return s2;
   uint8_t* nfield = into ? out->field_dst : out->new_empty_dist.as<uint8_t>();
   RKF_CUDA_TRY(cudaMemcpyAsync(nfield, c->empty_dist.p, c->top_len, cudaMemcpyDeviceToDevice, st));
   if ((s2 = lower_empty_dist(od, nfield, d_blocks, blocks, st)) != RKF_OK) return s2;
+  c->counted(1);
   c->n_leaves += appended;
   // the reference flat map (read only by the plain march) is updated in place
   if (od.has_flat && !c->flat_host.empty()) {

@@ -131,6 +131,7 @@ extern "C" rkf_status rkf_march_batch_noalloc(rkf_ctx* ctx, const rkf_view* view
   const cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
   // the table and a cleared counter go in by value; the march then reads them
   k_noalloc_stage<<<1, 256, 0, s>>>(tbl, scratch);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   return launch_persistent_scratch(c, tbl.segs, nseg, first, p, tu, s, scratch->segs, &scratch->counter,
                                    /*segs_uploaded=*/true, /*multi_empty=*/true);

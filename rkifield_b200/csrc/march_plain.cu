@@ -471,6 +471,7 @@ rkf_status launch_trace_plain(Ctx* c, const float* o, const float* d, const floa
   r.mode = mode;
   const size_t smem = sizeof(ObjDev) * (c->obj_count() ? c->obj_count() : 1);
   detail::k_trace_plain<<<(n + 127) / 128, 128, smem, st>>>(r);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   return RKF_OK;
 }
@@ -507,6 +508,7 @@ rkf_status launch_plain(Ctx* c, const rkf_camera* cam, const rkf_march_params* p
   const dim3 grid((w + 7) / 8, (h + 7) / 8);
   const size_t smem = sizeof(ObjDev) * (c->obj_count() ? c->obj_count() : 1);
   detail::k_march_plain<<<grid, block, smem, st>>>(kp);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   return RKF_OK;
 }

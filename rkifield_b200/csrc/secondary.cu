@@ -167,6 +167,7 @@ extern "C" rkf_status rkf_secondary_rays(rkf_ctx* ctx, const rkf_camera* cam, ui
   k.hits = dh;
   const uint64_t n = static_cast<uint64_t>(w) * h;
   detail::k_secondary<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(k);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   RKF_CUDA_TRY(cudaMemcpyAsync(hit_pixels, dh, 4, cudaMemcpyDeviceToHost, st));
   RKF_CUDA_TRY(cudaStreamSynchronize(st));

@@ -191,10 +191,13 @@ rkf_status tile_order_enqueue(Ctx* c, OrderTable& tbl, const Segment* dev_segs, 
                                static_cast<size_t>(tbl.n_views) * 2 * detail::kOrderKeys * 4, st));
   const unsigned blocks = (tbl.total_tiles + 255) / 256;
   detail::k_tile_cost<<<blocks, 256, 0, st>>>(tbl);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   detail::k_tile_scan<<<1, 64, 0, st>>>(tbl);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   detail::k_tile_place<<<blocks, 256, 0, st>>>(tbl);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   return RKF_OK;
 }

@@ -155,6 +155,7 @@ rkf_status prepare_tiled(Ctx* c, std::vector<Segment>& segs, cudaStream_t st, Ti
     detail::k_coarse_build<<<static_cast<unsigned>((cells + 255) / 256), 256, 0, st>>>(
         a, c->coarse_origin[0], c->coarse_origin[1], c->coarse_origin[2], c->coarse_dims[0], c->coarse_dims[1],
         c->coarse_dims[2], vs, vs * static_cast<float>(dmax), nt.as<uint16_t>());
+    c->counted();
     RKF_CUDA_TRY(cudaGetLastError());
     RKF_CUDA_TRY(cudaStreamSynchronize(st));
     std::swap(c->coarse_tex.p, nt.p);
@@ -189,7 +190,10 @@ rkf_status prepare_tiled(Ctx* c, std::vector<Segment>& segs, cudaStream_t st, Ti
     v.tile_off = static_cast<uint32_t>(off);
     sg.tile_off = static_cast<uint32_t>(off);
     const uint32_t nt = v.tiles_x * ((sg.h + 15) / 16);
-    if (nt) detail::k_tile_cull<<<nt, 32, 0, st>>>(a, v, cnt, list);
+    if (nt) {
+      detail::k_tile_cull<<<nt, 32, 0, st>>>(a, v, cnt, list);
+      c->counted();
+    }
     RKF_CUDA_TRY(cudaGetLastError());
     off += nt;
   }
@@ -300,9 +304,11 @@ rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st, const std::vector<uint32
   if (s2 == RKF_OK) s2 = field.alloc(std::max<uint64_t>(c->top_len, 1));
   if (s2 != RKF_OK) return s2;
   detail::k_coarse_unsafe<<<(nt + 255) / 256, 256, 0, st>>>(c->coarse_tex.as<uint16_t>(), nt, pre.as<uint32_t>());
+  c->counted();
   for (uint32_t axis = 0; axis < 3; ++axis) {
     const uint32_t lines = axis == 0 ? cd[1] * cd[2] : axis == 1 ? cd[0] * cd[2] : cd[0] * cd[1];
     detail::k_prefix_axis<<<(lines + 127) / 128, 128, 0, st>>>(pre.as<uint32_t>(), cd[0], cd[1], cd[2], axis);
+    c->counted();
   }
   RKF_CUDA_TRY(cudaMemsetAsync(field.p, 0, std::max<uint64_t>(c->top_len, 1), st));
   for (uint32_t vi : objs) {
@@ -324,8 +330,10 @@ rkf_status prepare_tiled_empty(Ctx* c, cudaStream_t st, const std::vector<uint32
     a.cvs = 0.32;
     const uint64_t nb = static_cast<uint64_t>(a.tx) * a.ty * a.tz;
     detail::k_tiled_mask<<<static_cast<unsigned>((nb + 255) / 256), 256, 0, st>>>(a);
+    c->counted();
     RKF_CUDA_TRY(cudaGetLastError());
     if ((s2 = build_empty_dist(o, masked.as<uint32_t>(), field.as<uint8_t>(), st)) != RKF_OK) return s2;
+    c->counted(3);
   }
   RKF_CUDA_TRY(cudaStreamSynchronize(st));
   std::swap(c->tiled_empty_dist.p, field.p);

@@ -336,6 +336,7 @@ extern "C" rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, ui
   unsigned long long counts[2] = {0, 0};
   RKF_CUDA_TRY(cudaMemsetAsync(d_counts.p, 0, 16, c->stream));
   k_classify_centres<<<cgrid, cblock, 0, c->stream>>>(va, 0, d_counts.as<unsigned long long>(), nullptr, 0, nullptr, 0);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   RKF_CUDA_TRY(cudaMemcpyAsync(counts, d_counts.p, 16, cudaMemcpyDeviceToHost, c->stream));
   RKF_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -346,6 +347,7 @@ extern "C" rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, ui
   RKF_CUDA_TRY(cudaMemsetAsync(d_counts.p, 0, 16, c->stream));
   k_classify_centres<<<cgrid, cblock, 0, c->stream>>>(va, 1, d_counts.as<unsigned long long>(),
                                                       d_cand.as<uint64_t>(), n_cand, d_inter.as<uint64_t>(), n_int);
+  c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
 
   // ---- 3. populate candidates --------------------------------------------------
@@ -358,6 +360,7 @@ extern "C" rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, ui
     k_populate<<<static_cast<unsigned>(n_cand), 512, 0, c->stream>>>(va, d_cand.as<uint64_t>(), n_cand,
                                                                      d_dist.as<float>(), d_mat.as<uint16_t>(),
                                                                      d_blend.as<uint8_t>(), d_cls.as<uint8_t>());
+    c->counted();
     RKF_CUDA_TRY(cudaGetLastError());
   }
   std::vector<uint64_t> cand(n_cand), inter(n_int);
@@ -457,6 +460,7 @@ extern "C" rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, ui
                                               d_cidx.as<uint32_t>(), d_slots.as<uint32_t>(), n_alloc,
                                               c->dist_f16.as<uint16_t>(), c->dist_f32.as<float>(),
                                               c->mat.as<uint16_t>(), c->blend.as<uint8_t>(), c->aos.as<uint2>());
+    c->counted();
     RKF_CUDA_TRY(cudaGetLastError());
     if (c->cfg.precision == RKF_PRECISION_U8) {
       // encode each new brick from its f32 distances (staged per slot)
@@ -465,6 +469,7 @@ extern "C" rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, ui
       k_scatter<<<n_alloc, 512, 0, c->stream>>>(d_dist.as<float>(), d_mat.as<uint16_t>(), d_blend.as<uint8_t>(),
                                                 d_cidx.as<uint32_t>(), d_slots.as<uint32_t>(), n_alloc, nullptr,
                                                 tmp.as<float>(), c->mat.as<uint16_t>(), c->blend.as<uint8_t>(), nullptr);
+      c->counted();
       RKF_CUDA_TRY(cudaGetLastError());
       // the codes cover the narrow band: +-3 voxels unless configured
       const float band = c->cfg.u8_band > 0.0f ? c->cfg.u8_band : 3.0f * g.vs;
@@ -475,6 +480,7 @@ extern "C" rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, ui
         k_encode_u8<<<j - i, 256, 0, c->stream>>>(tmp.as<float>(), nullptr, slots[i], j - i,
                                                   c->dist_u8.as<int8_t>(), c->brick_step.as<float>(), band,
                                                   c->cfg.u8_round == 1);
+        c->counted();
         RKF_CUDA_TRY(cudaGetLastError());
         i = j;
       }
@@ -517,6 +523,7 @@ extern "C" rkf_status rkf_voxelize_prims(rkf_ctx* ctx, const rkf_prim* prims, ui
     if (top_off) RKF_CUDA_TRY(cudaMemcpyAsync(nf.p, c->empty_dist.p, top_off, cudaMemcpyDeviceToDevice, c->stream));
     RKF_CUDA_TRY(cudaMemcpyAsync(nt.as<uint32_t>() + top_off, top.data(), ntop * 4, cudaMemcpyHostToDevice, c->stream));
     if ((st = build_empty_dist(od, nt.as<uint32_t>(), nf.as<uint8_t>(), c->stream)) != RKF_OK) return st;
+    c->counted(3);
     std::swap(c->top.p, nt.p);
     std::swap(c->top.bytes, nt.bytes);
     std::swap(c->empty_dist.p, nf.p);
