@@ -13,7 +13,8 @@
 // field (one byte per 8^3-brick block: radius of the cube of EMPTY blocks
 // around it, empty_dist.h) from cube exit to cube exit, and counts the EMPTY
 // steps before the last block that is not EMPTY within the ray's reach, plus
-// a few steps per such block.  A counting sort (64 cost classes, heaviest
+// a few steps per such block; eight lanes walk the eight stretches of a ray
+// side by side.  A counting sort (64 cost classes, heaviest
 // first, separately within each group of tile rows) writes the permutation.
 #include <cmath>
 #include <cstring>
@@ -35,9 +36,20 @@ __device__ __forceinline__ uint32_t order_view_of(const OrderTable& t, uint32_t 
   return lo;
 }
 
-// EMPTY steps a tile's centre ray is expected to take (see above).
-__device__ float tile_cost(const OrderTable& t, const Segment& sg, uint32_t col, uint32_t row) {
+// Lanes that walk one tile's centre ray, each over its own stretch of the
+// ray's reach: the walk is a chain of dependent loads of the field (cold in
+// L2 at the start of a frame), so splitting it cuts the kernel's longest
+// chain by this factor.
+constexpr uint32_t kOrderLanes = 8;
+constexpr int kOrderLaneSteps = 32;  // cube jumps a lane takes at most
+
+// Part `lane` of the walk of a tile's centre ray (see above): the number of
+// non-EMPTY blocks it meets and the distance of the last of them (0: none).
+__device__ void tile_walk(const OrderTable& t, const Segment& sg, uint32_t col, uint32_t row, uint32_t lane,
+                          uint32_t* blocks_out, float* t_last_out) {
   const ObjDev& o = t.o;
+  *blocks_out = 0;
+  *t_last_out = 0.0f;
   const uint32_t px = min(col * t.tile_w + t.tile_w / 2, sg.w - 1);
   const uint32_t py = min(row * t.tile_h + t.tile_h / 2, sg.h - 1);
   const float u = (static_cast<float>(px) + 0.5f + sg.jitter[0]) / static_cast<float>(sg.w);
@@ -47,25 +59,28 @@ __device__ float tile_cost(const OrderTable& t, const Segment& sg, uint32_t col,
   for (int a = 0; a < 3; ++a) d[a] = sg.fwd[a] + sg.right[a] * nx + sg.up[a] * ny;
   const float il = rsqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
   // grid voxel coordinate along the ray: g(t) = a0 + a1 * t (t in metres)
-  float a0[3], a1[3];
+  float a0[3], a1[3], ia[3];
   float t0 = 0.0f, t1 = t.reach;
   for (int a = 0; a < 3; ++a) {
     a0[a] = (sg.pos[a] + o.m[12 + a] + o.half_gs[a]) * o.rcp_vs - 0.5f;
     a1[a] = d[a] * il * o.rcp_vs;
+    ia[a] = a1[a] != 0.0f ? 1.0f / a1[a] : 0.0f;
     const float tv = static_cast<float>(o.tv[a]);
     if (a1[a] != 0.0f) {
-      const float ta = -a0[a] / a1[a], tb = (tv - a0[a]) / a1[a];
+      const float ta = -a0[a] * ia[a], tb = (tv - a0[a]) * ia[a];
       t0 = fmaxf(t0, fminf(ta, tb));
       t1 = fminf(t1, fmaxf(ta, tb));
     } else if (!(a0[a] >= 0.0f && a0[a] < tv)) {
       t1 = -1.0f;
     }
   }
-  if (!(t0 < t1)) return 0.0f;  // the ray misses the grid
+  if (!(t0 < t1)) return;  // the ray misses the grid
+  const float len = (t1 - t0) * (1.0f / static_cast<float>(kOrderLanes));
+  const float s1 = lane + 1 == kOrderLanes ? t1 : t0 + len * static_cast<float>(lane + 1);
   const float eps = 0.01f * o.vs;
-  float tt = t0 + eps, t_last = 0.0f;
+  float tt = t0 + len * static_cast<float>(lane) + eps, t_last = 0.0f;
   uint32_t blocks = 0;
-  for (int it = 0; it < 128 && tt < t1; ++it) {
+  for (int it = 0; it < kOrderLaneSteps && tt < s1; ++it) {
     int k[3];
     for (int a = 0; a < 3; ++a) {
       const float g = fminf(fmaxf(a0[a] + a1[a] * tt, 0.0f), static_cast<float>(o.tv[a] - 1));
@@ -76,8 +91,8 @@ __device__ float tile_cost(const OrderTable& t, const Segment& sg, uint32_t col,
     float te = INFINITY;
     for (int a = 0; a < 3; ++a) {
       const float lo = static_cast<float>((k[a] - rad) * 64), hi = static_cast<float>((k[a] + rad + 1) * 64);
-      if (a1[a] > 0.0f) te = fminf(te, (hi - a0[a]) / a1[a]);
-      else if (a1[a] < 0.0f) te = fminf(te, (lo - a0[a]) / a1[a]);
+      if (a1[a] > 0.0f) te = fminf(te, (hi - a0[a]) * ia[a]);
+      else if (a1[a] < 0.0f) te = fminf(te, (lo - a0[a]) * ia[a]);
     }
     if (r == 0) {
       ++blocks;
@@ -85,23 +100,54 @@ __device__ float tile_cost(const OrderTable& t, const Segment& sg, uint32_t col,
     }
     tt = fmaxf(te, tt) + eps;
   }
-  return t_last / t.step + 6.0f * static_cast<float>(blocks);
+  *blocks_out = blocks;
+  *t_last_out = t_last;
 }
 
+// Adds n to *addr once per distinct address among the active lanes that
+// pass want (the counters are few and every tile hits one of them: one
+// atomic per tile serialises on the busiest address).  Returns, to every
+// wanting lane, the counter's old value plus the count of lanes below it
+// with the same address: a distinct slot per lane.
+__device__ __forceinline__ uint32_t warp_add(uint32_t* addr, bool want) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const unsigned long long key = want ? reinterpret_cast<unsigned long long>(addr) : ~0ull;
+  const uint32_t peers = __match_any_sync(0xffffffffu, key);
+  const uint32_t leader = __ffs(peers) - 1;
+  uint32_t base = 0;
+  if (want && lane == leader) base = atomicAdd(addr, static_cast<uint32_t>(__popc(peers)));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return base + static_cast<uint32_t>(__popc(peers & ((1u << lane) - 1u)));
+}
+
+// kOrderLanes lanes per tile (a warp holds whole tiles): the tile's cost,
+// EMPTY steps before its last non-EMPTY block plus 6 per such block, gives
+// its class; the first lane keys the tile and counts it.
 __global__ void k_tile_cost(const __grid_constant__ OrderTable t) {
-  const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gi >= t.total_tiles) return;
+  const uint64_t th = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint32_t lane = static_cast<uint32_t>(th % kOrderLanes);
+  const uint64_t tile = th / kOrderLanes;
+  const bool live = tile < t.total_tiles;  // every lane takes part in the shuffles
+  const uint32_t gi = live ? static_cast<uint32_t>(tile) : 0u;
   const uint32_t vi = order_view_of(t, gi);
   const OrderView& v = t.v[vi];
   const uint32_t li = gi - v.tile_base;
   const uint32_t row = li / v.tiles_x, col = li % v.tiles_x;
-  const float cost = tile_cost(t, t.segs[v.seg], col, row);
+  uint32_t blocks = 0;
+  float t_last = 0.0f;
+  if (live) tile_walk(t, t.segs[v.seg], col, row, lane, &blocks, &t_last);
+  for (uint32_t m = kOrderLanes / 2; m; m >>= 1) {
+    blocks += __shfl_xor_sync(0xffffffffu, blocks, m, kOrderLanes);
+    t_last = fmaxf(t_last, __shfl_xor_sync(0xffffffffu, t_last, m, kOrderLanes));
+  }
+  const bool first = live && lane == 0;
+  const float cost = t_last / t.step + 6.0f * static_cast<float>(blocks);
   const uint32_t cls = kOrderBuckets - 1 - min(kOrderBuckets - 1, static_cast<uint32_t>(cost * (1.0f / 16.0f)));
   uint32_t g = 0;
   while (g + 1 < v.n_groups && row >= v.group_row[g + 1]) ++g;
   const uint32_t key = g * kOrderBuckets + cls;
-  t.key[gi] = key;
-  atomicAdd(t.count + static_cast<size_t>(vi) * 2 * kOrderKeys + key, 1u);
+  if (first) t.key[gi] = key;
+  warp_add(t.count + static_cast<size_t>(vi) * 2 * kOrderKeys + key, first);
 }
 
 // One thread per view: exclusive prefix of the counters (groups in order,
@@ -119,13 +165,14 @@ __global__ void k_tile_scan(const __grid_constant__ OrderTable t) {
 }
 
 __global__ void k_tile_place(const __grid_constant__ OrderTable t) {
-  const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gi >= t.total_tiles) return;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = tid < t.total_tiles;  // every lane takes part in warp_add
+  const uint32_t gi = live ? tid : 0u;
   const uint32_t vi = order_view_of(t, gi);
   const OrderView& v = t.v[vi];
   uint32_t* off = t.count + static_cast<size_t>(vi) * 2 * kOrderKeys + kOrderKeys;
-  const uint32_t pos = atomicAdd(off + t.key[gi], 1u);
-  t.perm[v.tile_base + pos] = gi - v.tile_base;
+  const uint32_t pos = warp_add(off + (live ? t.key[gi] : 0u), live);
+  if (live) t.perm[v.tile_base + pos] = gi - v.tile_base;
 }
 
 }  // namespace detail
@@ -190,7 +237,9 @@ rkf_status tile_order_enqueue(Ctx* c, OrderTable& tbl, const Segment* dev_segs, 
   RKF_CUDA_TRY(cudaMemsetAsync(tbl.count, 0,
                                static_cast<size_t>(tbl.n_views) * 2 * detail::kOrderKeys * 4, st));
   const unsigned blocks = (tbl.total_tiles + 255) / 256;
-  detail::k_tile_cost<<<blocks, 256, 0, st>>>(tbl);
+  const unsigned cost_blocks =
+      static_cast<unsigned>((static_cast<uint64_t>(tbl.total_tiles) * detail::kOrderLanes + 255) / 256);
+  detail::k_tile_cost<<<cost_blocks, 256, 0, st>>>(tbl);
   c->counted();
   RKF_CUDA_TRY(cudaGetLastError());
   detail::k_tile_scan<<<1, 64, 0, st>>>(tbl);
