@@ -69,6 +69,9 @@ def parse():
                     help="arrival rate of a last serving run that saturates the loop (0 = skip)")
     ap.add_argument("--cs-budget", type=int, default=32768, help="serving memory budget, MiB")
     ap.add_argument("--pool-bricks", type=int, default=0, help="brick slots to reserve (0 = default)")
+    ap.add_argument("--tuning", default="",
+                    help="launch tuning of the headline view as comma-separated rkf_batch_tuning fields "
+                         "(tile_w,tile_h,step_budget,...); skips the autotuner")
     ap.add_argument("--no-reference-pool", action="store_true",
                     help="keep no AoS reference pool (implies --no-plain; smaller device footprint)")
     ap.add_argument("--report", default="", choices=["", "precision"],
@@ -975,9 +978,14 @@ def run_b200(args, world, rank, local, dist):
     vw[0].out.mem = abi.RKF_MEM_DEVICE
     tu = abi.rkf_batch_tuning()
     t0 = time.perf_counter()
-    abi.check(ctx.lib.rkf_autotune(ctx.h, vw, 1, None, 0, C.byref(p), C.byref(tu)), "autotune")
+    if args.tuning:
+        tu = abi.rkf_batch_tuning(*[int(x) for x in args.tuning.split(",")])
+        ctx.set_tuning(tu)
+    else:
+        abi.check(ctx.lib.rkf_autotune(ctx.h, vw, 1, None, 0, C.byref(p), C.byref(tu)), "autotune")
     tuning = {k: getattr(tu, k) for k, _ in abi.rkf_batch_tuning._fields_}
     tuning["tune_s"] = time.perf_counter() - t0
+    tuning["source"] = "--tuning" if args.tuning else "rkf_autotune"
 
     def launch_stats(cap: int):
         n_launch, n_timed = C.c_uint64(0), C.c_uint32(0)

@@ -521,6 +521,13 @@ typedef struct rkf_batch_tuning {
                                  /* heaviest first, by an estimate of their  */
                                  /* empty-space steps (0: row order); the    */
                                  /* outputs are the same either way          */
+    uint32_t tail_share;         /* once a warp has no work left to fetch    */
+                                 /* and at most this many of its lanes still */
+                                 /* march (1..32), the warp's 32 lanes take  */
+                                 /* those lanes' EMPTY runs together, one    */
+                                 /* run at a time, up to 32 steps a round;   */
+                                 /* 0: off.  Single-object empty-space path; */
+                                 /* the outputs are the same either way      */
 } rkf_batch_tuning;
 
 /* Run every view and ray batch in one persistent work-stealing launch.

@@ -145,7 +145,7 @@ class rkf_batch_tuning(C.Structure):
                 ("compact_interval", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("threads_per_block", C.c_uint32), ("refill_idle", C.c_uint32),
                 ("probe_in_run", C.c_uint32), ("no_empty_path", C.c_uint32),
-                ("order_tiles", C.c_uint32)]
+                ("order_tiles", C.c_uint32), ("tail_share", C.c_uint32)]
 
 
 class rkf_request(C.Structure):

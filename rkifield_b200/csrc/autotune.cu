@@ -1,17 +1,19 @@
 // autotune.cu — pick the persistent march's launch tuning for a workload.
 //
-// The batched march has eight knobs that change speed but never results:
+// The batched march has nine knobs that change speed but never results:
 // the ray-tile shape that orders a view's work ids (the spatial coherence of
 // the rays a warp holds), the compaction interval (march iterations between
 // lane refills), the step budget (empty-space steps a lane runs before its
 // warp re-converges), the refill threshold (idle lanes that make a warp
 // refill), where a lane probes its next EMPTY cube (inside a run or between
-// runs), the block size, whether it runs EMPTY runs at all and whether views
-// hand out their heaviest ray tiles first.  rkf_autotune times candidates on
+// runs), the block size, whether it runs EMPTY runs at all, whether views
+// hand out their heaviest ray tiles first and whether the warps of the
+// launch's tail share their EMPTY runs.  rkf_autotune times candidates on
 // the caller's sample of the work with CUDA events: every tile x interval x
 // block size at the default budget and threshold, then the heaviest-first
 // tile order, then every budget, then every threshold, then the other probe
-// placement, then the march without EMPTY runs, each at the best so far.
+// placement, then warp-shared EMPTY runs in the launch's tail, then the march
+// without EMPTY runs, each at the best so far.
 // Each timed launch starts with the L2 cache flushed (a write of twice its
 // size, outside the timed events), as a frame does after other work: with
 // the index left in L2 by the previous trial, the knobs that cut DRAM
@@ -112,6 +114,12 @@ extern "C" rkf_status rkf_autotune(rkf_ctx* ctx, const rkf_view* views, uint32_t
     tu.probe_in_run = 1;
     trial(tu);
   }
+  // the warp-shared EMPTY runs of the launch's tail
+  if (st == RKF_OK) {
+    rkf_batch_tuning tu = best;
+    tu.tail_share = 2;
+    trial(tu);
+  }
   // where EMPTY runs do not pay (a camera outside a dense grid: short runs,
   // probes that mostly fail), the full sampler alone is faster
   if (st == RKF_OK) {
@@ -133,7 +141,8 @@ extern "C" rkf_status rkf_tuning_set(rkf_ctx* ctx, const rkf_batch_tuning* tunin
   const rkf_batch_tuning& tu = *tuning;
   const uint32_t threads = tu.threads_per_block ? tu.threads_per_block : 256;
   if ((tu.tile_w == 0) != (tu.tile_h == 0) || tu.tile_w * tu.tile_h > 4096 || threads > 256 || threads % 32 ||
-      tu.refill_idle > 32 || tu.probe_in_run > 1 || tu.no_empty_path > 1 || tu.order_tiles > 1)
+      tu.refill_idle > 32 || tu.probe_in_run > 1 || tu.no_empty_path > 1 || tu.order_tiles > 1 ||
+      tu.tail_share > 32)
     return fail(RKF_INVALID_ARG, "rkf_tuning_set: bad tuning");
   Ctx* c = reinterpret_cast<Ctx*>(ctx);
   if (c->serve) return fail(RKF_BUSY, "rkf_tuning_set: the context is serving");

@@ -108,6 +108,7 @@ struct KParams {
   uint32_t plain_obj;  // object 0 has zero translation and unit scale
   uint32_t refill_active;  // leave the march loop once at most this many lanes march
   uint32_t run_probe;      // empty-space path: probe the next cube inside a run
+  uint32_t tail_share;     // empty-space path: warp-shared EMPTY runs once at most this many lanes march
   TiledDev td;             // tiled strategy inputs (views of a tiled launch)
   uint32_t tiled;
   float empty_lo;          // empty-space path: lower bound of every EMPTY value
@@ -602,6 +603,76 @@ __device__ __forceinline__ uint32_t empty_run_x2(const ObjDev& o, const uint8_t*
   return c;
 }
 
+// empty_run_x2<INRUN=false>'s run taken by a whole warp, for the lanes that
+// pass pend, one lane's run after another (the launch's tail: few lanes
+// still march and the others have no work left).  Lane j of a round samples
+// the j-th step ahead.  Within t's binade [2^e, 2^(e+1)), whose spacing is u,
+// every t' is a multiple of u, so fl(t' + c) = t' + r with r = fl(t + c) - t
+// (c rounded to a multiple of u) unless c lies exactly halfway between two
+// multiples, where the rounding would depend on t' itself.  Away from such a
+// tie the serial positions while every value is c are therefore exactly
+// t + j*r (j*r and the sum are exact while t + j*r < 2^(e+1)), and lane j
+// computes its own without waiting for the others.  A round accepts the
+// steps up to the first value that is not c (that step is taken with its
+// value), or up to the first position past the binade, the run's end
+// (t > lim) or its budget (n steps), and the next position comes from the
+// last accepted step as the serial loop makes it.  A tie, or t too small
+// for this arithmetic, leaves lane 0 alone: one serial step per round.
+// Every lane of the warp must call this.
+__device__ __noinline__ void shared_runs(const ObjDev& o, bool pend, float ox, float oy, float oz, float dx,
+                                         float dy, float dz, float lim, float tmax, uint32_t n, float& t,
+                                         float& prev_t, float& prev_dist, uint32_t& c_out, bool& stop_full) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const f2 h01 = f2_pack(o.half_gs[0], o.half_gs[1]);
+  const f2 r2 = f2_pack(o.rcp_vs, o.rcp_vs), nvs2 = f2_pack(-o.vs, -o.vs), half2 = f2_pack(0.5f, 0.5f);
+  const float hz = o.half_gs[2], vs = o.vs, rcp = o.rcp_vs, be = o.be;
+  const float fj = static_cast<float>(lane);
+  for (uint32_t todo = __ballot_sync(kFull, pend); todo; todo &= todo - 1u) {
+    const uint32_t L = __ffs(todo) - 1u;
+    const float rox = __shfl_sync(kFull, ox, L), roy = __shfl_sync(kFull, oy, L), roz = __shfl_sync(kFull, oz, L);
+    const float rdx = __shfl_sync(kFull, dx, L), rdy = __shfl_sync(kFull, dy, L), rdz = __shfl_sync(kFull, dz, L);
+    const float rlim = __shfl_sync(kFull, lim, L), rtmax = __shfl_sync(kFull, tmax, L);
+    const uint32_t rn = __shfl_sync(kFull, n, L);
+    float rt = __shfl_sync(kFull, t, L);
+    const f2 o01 = f2_pack(rox, roy), d01 = f2_pack(rdx, rdy);
+    uint32_t c = 0;
+    float pt = 0.0f, pd = 0.0f;
+    bool sf = false;
+    for (;;) {
+      const uint32_t bits = __float_as_uint(rt) & 0x7f800000u;  // t >= 0
+      const float top = __uint_as_float(bits + 0x00800000u);    // 2^(e+1)
+      const float u = __uint_as_float(bits - (23u << 23));      // spacing of [2^e, 2^(e+1))
+      const float r = __fsub_rn(__fadd_rn(rt, be), rt);
+      const bool wide = rt >= 1.0e-30f && !(fabsf(__fsub_rn(be, r)) == __fmul_rn(0.5f, u));
+      const float tj = lane == 0 ? rt : __fadd_rn(rt, __fmul_rn(fj, r));
+      const bool ok = (lane == 0 || (wide && tj < top)) && !(tj > rlim) && c + lane < rn;
+      const float ej = empty_value_x2(o01, d01, h01, r2, nvs2, half2, roz, rdz, hz, vs, rcp, be, tj);
+      const uint32_t m_stop = __ballot_sync(kFull, !ok);
+      const uint32_t m_odd = __ballot_sync(kFull, ok && ej != be);
+      const uint32_t first_stop = m_stop ? __ffs(m_stop) - 1u : 32u;
+      const uint32_t first_odd = m_odd ? __ffs(m_odd) - 1u : 32u;
+      const uint32_t steps = first_odd < first_stop ? first_odd + 1u : first_stop;
+      if (steps == 0) {  // lane 0 stopped: the run ends here, as the serial loop ends it
+        sf = c < rn && rt > rtmax;
+        break;
+      }
+      pt = __shfl_sync(kFull, tj, steps - 1u);
+      pd = __shfl_sync(kFull, ej, steps - 1u);
+      c += steps;
+      rt = __fadd_rn(pt, pd);
+    }
+    if (lane == L) {
+      t = rt;
+      c_out = c;
+      stop_full = sf;
+      if (c) {
+        prev_t = pt;
+        prev_dist = pd;
+      }
+    }
+  }
+}
+
 // Up to n march steps through positions where every object of the set
 // (path objects, at least two) samples its EMPTY value and every other
 // object lies beyond its ball: each step's value is the least of the set's
@@ -660,6 +731,8 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
   constexpr bool EMPTY_PATH = OBJ == OBJ_SINGLE_EMPTY || OBJ == OBJ_SINGLE_EMPTY_TILED || MULTI_EMPTY;
   // tile bookkeeping of tiled launches
   constexpr bool TILES = OBJ != OBJ_SINGLE_EMPTY && OBJ != OBJ_MULTI_EMPTY;
+  // warp-shared EMPTY runs in the launch's tail (shared_runs)
+  constexpr bool SHARE = OBJ == OBJ_SINGLE_EMPTY;
   const ObjDev* sh_objs = kp.objs;
   const SceneDev& s = kp.s;
   const rkf_march_params& p = kp.p;
@@ -803,6 +876,15 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
 #pragma unroll 1
     for (uint32_t k = 0; k < kp.interval; ++k) {
       bool full = true;  // take a full step (index lookups) this iteration
+      // the launch's tail: no work is left to fetch and few lanes march, so
+      // the warp takes their plain clean EMPTY runs together (after the
+      // per-lane block below, where every lane meets again)
+      const bool share = SHARE && exhausted && kp.tail_share && !kp.run_probe &&
+                         static_cast<uint32_t>(__popc(__ballot_sync(kFull, state == ST_MARCH || state == ST_SHADOW))) <=
+                             kp.tail_share;
+      bool pend = false;
+      float pend_lim = 0.0f, pend_dx = 0.0f, pend_dy = 0.0f, pend_dz = 0.0f;
+      uint32_t pend_n = 0;
       // (a tiled step evaluates the ray's object list only: EMPTY runs need
       // the voxelized object in it)
       if (EMPTY_PATH && (state == ST_MARCH || state == ST_SHADOW) && (!MULTI_EMPTY || (cs.vox_listed & 0xFFu))) {
@@ -919,7 +1001,16 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
 #define RKF_RUN(P, CL, IN)                                                                                   \
   empty_run<P, CL, IN, MULTI_EMPTY>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n, brk, near_thr, min_step, \
                                     max_near, far_t, t, box_t, prev_t, prev_dist, near, stop_full)
-            if (plain && clean)
+            if (plain && clean && share) {
+              // the whole run at once (the budget only paces warps that share
+              // nothing); taken with the warp below
+              pend = true;
+              pend_lim = fminf(box_t, tmax);
+              pend_n = step < max_step ? max_step - step : 0u;
+              pend_dx = dx;
+              pend_dy = dy;
+              pend_dz = dz;
+            } else if (plain && clean)
               c = kp.run_probe ? empty_run_x2<true, MULTI_EMPTY>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n,
                                                                  far_t, t, box_t, prev_t, prev_dist, stop_full)
                                : empty_run_x2<false, MULTI_EMPTY>(o0, s.empty_dist, ox, oy, oz, dx, dy, dz, tmax, n,
@@ -935,6 +1026,18 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
           // between probes, continues next iteration unless a limit ends the
           // ray; any other stop needs the full step's decision
           full = stop_full || step >= max_step || t > tmax || near >= max_near;
+        }
+      }
+      if (share) {  // warp-uniform: every lane is here
+        uint32_t c = 0;
+        bool stop_full = false;
+        shared_runs(sh_objs[0], pend, ox, oy, oz, pend_dx, pend_dy, pend_dz, pend_lim, tmax, pend_n, t, prev_t,
+                    prev_dist, c, stop_full);
+        if (pend) {
+          const bool sh = state == ST_SHADOW;
+          step += c;
+          full = stop_full || step >= (sh ? 256u : p.hard_max_steps) || t > tmax ||
+                 near >= (sh ? 32u : p.scene.max_steps);
         }
       }
       if (!full) {
@@ -1704,6 +1807,7 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   kp.budget = tu.step_budget ? tu.step_budget : 32;
   kp.refill_active = 32u - std::min<uint32_t>(tu.refill_idle ? tu.refill_idle : 32u, 32u);
   kp.run_probe = tu.probe_in_run ? 1u : 0u;
+  kp.tail_share = std::min<uint32_t>(tu.tail_share, 32u);
   // mix(c, c, t) three times stays within 12 roundings of c (relative 2^-24
   // each); 0.999 leaves a wide margin
   kp.empty_lo = empty ? 0.999f * e0.be * e0.min_scale : 0.0f;
@@ -1791,6 +1895,7 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
   kp.budget = tu.step_budget ? tu.step_budget : 32;
   kp.refill_active = 32u - std::min<uint32_t>(tu.refill_idle ? tu.refill_idle : 32u, 32u);
   kp.run_probe = tu.probe_in_run ? 1u : 0u;
+  kp.tail_share = std::min<uint32_t>(tu.tail_share, 32u);
   // mix(c, c, t) three times stays within 12 roundings of c (relative 2^-24
   // each); 0.999 leaves a wide margin
   kp.empty_lo = empty ? 0.999f * e0.be * e0.min_scale : 0.0f;

@@ -30,18 +30,20 @@ def test_large_view_full_frame_bit_exact(oracle, large, large_oracle, w, h):
     flags = ref["flags"]
     assert (flags & 1).sum() > 0.01 * w * h, "the view should hit geometry"
     assert (flags & 4).sum() > 0.5 * w * h, "most rays should run out of steps in empty space"
-    # heaviest tiles first, one launch and in three bands of host outputs
+    # heaviest tiles first, one launch and in three bands of host outputs;
+    # warp-shared EMPTY runs in the launch's tail (with 32, every warp that
+    # has no work left shares)
     from rkifield_b200 import _abi as abi
     tu0 = ctx.tuning()
-    tu = abi.rkf_batch_tuning.from_buffer_copy(tu0)
-    tu.order_tiles = 1
     try:
-        ctx.set_tuning(tu)
-        for bands in (1, 3):
+        for order, share, bands in ((1, 0, 1), (1, 0, 3), (1, 4, 1), (0, 32, 3), (1, 32, 1)):
+            tu = abi.rkf_batch_tuning.from_buffer_copy(tu0)
+            tu.order_tiles, tu.tail_share = order, share
+            ctx.set_tuning(tu)
             ctx.lib.rkf_testing_set_host_bands(bands)
             got = ctx.march(cam, p, w, h, reference_planes=True)
             for k in PLANES:
-                assert_bits_equal(got[k], ref[k], f"{w}x{h} heaviest tiles first, {bands} bands, {k}")
+                assert_bits_equal(got[k], ref[k], f"{w}x{h} order {order} tail share {share}, {bands} bands, {k}")
     finally:
         ctx.lib.rkf_testing_set_host_bands(-1)
         ctx.set_tuning(tu0)
@@ -72,11 +74,22 @@ def test_large_rays_around_the_step_budget_bit_exact(oracle, large, large_oracle
     span = np.float32(1024 * 8 * spec.voxel_size)
     tmax = (span * rng.uniform(0.97, 1.03, n)).astype(np.float32)
     tmax[:200] = span  # on the boundary itself
+    tu0 = ctx.tuning()
     for mode in (abi.RKF_TRACE_CLOSEST, abi.RKF_TRACE_ANY, abi.RKF_TRACE_SHADOW):
         ref = oracle.trace(large_oracle, o.ravel(), d.ravel(), tmax, mode, p)
         got = ctx.trace(o.ravel(), d.ravel(), tmax, mode, p)
         for k in ("t", "flags"):
             assert_bits_equal(got[k], ref[k], f"mode {mode} {k}")
+        # every warp that has no work left takes its lanes' EMPTY runs together
+        tu = abi.rkf_batch_tuning.from_buffer_copy(tu0)
+        tu.tail_share = 32
+        try:
+            ctx.set_tuning(tu)
+            got = ctx.trace(o.ravel(), d.ravel(), tmax, mode, p)
+        finally:
+            ctx.set_tuning(tu0)
+        for k in ("t", "flags"):
+            assert_bits_equal(got[k], ref[k], f"mode {mode} tail share {k}")
         if mode == abi.RKF_TRACE_CLOSEST:
             steps_out = (ref["flags"] & 4) != 0
             assert steps_out.sum() > 200 and (ref["flags"] == 0).sum() > 200, "both miss endings must occur"

@@ -109,9 +109,11 @@ def test_batch_equals_separate_calls(small_scene, small_ctx):
             setattr(batches[j].out, k, a.ptr)
         batches[j].out.mem = abi.RKF_MEM_DEVICE
     # (tile_w, tile_h, step_budget, compact_interval, blocks_per_sm, threads_per_block, refill_idle,
-    #  probe_in_run, no_empty_path, order_tiles)
+    #  probe_in_run, no_empty_path, order_tiles, tail_share)
     for tu in (None, (16, 2, 0, 4, 0, 128, 0, 0), (4, 8, 0, 64, 1, 256, 0, 1), (8, 4, 3, 16, 0, 256, 32, 0),
-               (4, 8, 200, 8, 0, 64, 1, 1), (8, 4, 0, 128, 0, 256, 0, 0, 0, 1), (16, 2, 24, 32, 0, 128, 8, 1, 0, 1)):
+               (4, 8, 200, 8, 0, 64, 1, 1), (8, 4, 0, 128, 0, 256, 0, 0, 0, 1), (16, 2, 24, 32, 0, 128, 8, 1, 0, 1),
+               (8, 4, 32, 128, 0, 256, 32, 0, 0, 1, 4), (4, 8, 5, 16, 0, 128, 8, 0, 0, 0, 32),
+               (8, 4, 0, 64, 0, 256, 0, 1, 0, 1, 32)):
         tuning = None
         if tu is not None:
             tuning = abi.rkf_batch_tuning(*tu)
