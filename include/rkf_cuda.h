@@ -225,6 +225,74 @@ RKF_API rkf_status rkf_objects_import(rkf_ctx* ctx, const rkf_gpu_object* object
 RKF_API rkf_status rkf_objects_update(rkf_ctx* ctx, const rkf_gpu_object* objects, uint32_t n,
                                       const int32_t* index_source);
 
+/* ------------------------------------------------------------------------ */
+/* Object records from a node tree: transform flattening                    */
+/* (crates/rkf-core/src/transform_flatten.rs:23-110 and                     */
+/* crates/rkf-render/src/gpu_object.rs:135-266).  Host only.                */
+/* ------------------------------------------------------------------------ */
+#define RKF_NO_PARENT 0xFFFFFFFFu
+/* blend_mode of rkf_gpu_object and rkf_scene_node (gpu_object.rs:123-133) */
+#define RKF_BLEND_SMOOTH_UNION 0u
+#define RKF_BLEND_UNION        1u
+#define RKF_BLEND_SUBTRACT     2u
+#define RKF_BLEND_INTERSECT    3u
+
+/* One node of an object's tree (SceneNode, scene_node.rs): its local
+ * transform (Transform::to_matrix = scale, then rotation, then translation),
+ * whether it is visible (NodeMetadata::visible, scene_node.rs:178), how it blends with its
+ * siblings and its SDF source.  A tree is passed in depth-first pre-order --
+ * a node, then the subtree of each child in order -- each node naming its
+ * parent's index (RKF_NO_PARENT for the root, which comes first). */
+typedef struct rkf_scene_node {
+    float position[3];
+    float rotation[4];         /* quaternion x, y, z, w, used as given        */
+    float scale[3];
+    uint32_t parent;
+    uint32_t visible;          /* 0: the node and its subtree are left out   */
+                               /* (the root is always kept)                   */
+    uint32_t sdf_type;         /* RKF_SDF_NONE / ANALYTICAL / VOXELIZED       */
+    uint32_t primitive_type;   /* analytical: RKF_PRIM_*                      */
+    float params[4];           /* analytical: primitive_params order          */
+    uint32_t material_id;      /* analytical                                  */
+    uint32_t brick_map_offset; /* voxelized: BrickMapHandle                   */
+    uint32_t brick_map_dims[3];
+    float voxel_size;          /* voxelized                                   */
+    uint32_t blend_mode;       /* RKF_BLEND_*                                 */
+    float blend_radius;        /* smooth union only                           */
+} rkf_scene_node;
+
+/* FlatNode (transform_flatten.rs:23-38) with the index of its source node. */
+typedef struct rkf_flat_node {
+    float inverse_world[16];   /* column-major                                */
+    float accumulated_scale[3];
+    uint32_t depth;            /* 0 for the root                              */
+    uint32_t parent_index;     /* in the flat array; RKF_NO_PARENT: root      */
+    uint32_t node;             /* the rkf_scene_node it came from             */
+} rkf_flat_node;
+
+/* flatten_object (transform_flatten.rs:56-110): walks the tree depth-first with
+ * world = parent world * local, starting from the object's own transform
+ * (object_scale, object_rotation, then world_position: the object's baked
+ * world-space, or camera-relative, position), and writes one flat node per
+ * visible node in pre-order, with the inverse of its world matrix and the
+ * product of the scales from the object down to it.  The products and the
+ * inverse are computed in double precision and rounded to float once.
+ * out holds n_nodes entries; *n_out receives the count written.
+ * RKF_INVALID_ARG for a tree not in pre-order, a parent index out of range or
+ * a singular world matrix. */
+RKF_API rkf_status rkf_flatten_object(const rkf_scene_node* nodes, uint32_t n_nodes,
+                                      const float object_rotation[4], const float object_scale[3],
+                                      const float world_position[3], rkf_flat_node* out, uint32_t* n_out);
+
+/* GpuObject::from_flat_node (gpu_object.rs:141-220, 233-266): the record of a flat
+ * node whose source is `source`; analytic sources keep their primitive type,
+ * parameters and material, voxelized ones their brick map handle and voxel
+ * size, and a smooth union its radius (other modes get 0). */
+RKF_API rkf_status rkf_gpu_object_from_flat_node(const rkf_flat_node* flat, const rkf_scene_node* source,
+                                                 uint32_t object_id, const float aabb_min[4],
+                                                 const float aabb_max[4], const float geometry_aabb_min[3],
+                                                 const float geometry_aabb_max[3], rkf_gpu_object* out);
+
 /* One BVH node as the shader reads it (GpuBvhNode, gpu_bvh.rs:24-41;
  * BvhNode, ray_march.wgsl:99-108): 32 bytes. */
 #define RKF_BVH_INVALID 0xFFFFFFFFu

@@ -27,6 +27,9 @@ INTERIOR_SLOT = 0xFFFFFFFE
 MAX_FLOAT = np.float32(3.402823e38)
 
 RKF_SDF_NONE, RKF_SDF_ANALYTICAL, RKF_SDF_VOXELIZED = 0, 1, 2
+RKF_PRIM_SPHERE, RKF_PRIM_BOX, RKF_PRIM_CAPSULE, RKF_PRIM_TORUS, RKF_PRIM_CYLINDER, RKF_PRIM_PLANE = range(6)
+RKF_NO_PARENT = 0xFFFFFFFF
+RKF_BLEND_SMOOTH_UNION, RKF_BLEND_UNION, RKF_BLEND_SUBTRACT, RKF_BLEND_INTERSECT = 0, 1, 2, 3
 RKF_PRECISION_F16, RKF_PRECISION_F32, RKF_PRECISION_U8 = 0, 1, 2
 RKF_MEM_HOST, RKF_MEM_DEVICE = 0, 1
 RKF_BAND_VOXELS, RKF_BAND_REFERENCE = 0, 1
@@ -73,6 +76,19 @@ class rkf_config(C.Structure):
                 ("precision", C.c_uint32), ("keep_reference_pool", C.c_uint32),
                 ("mem_budget_bytes", C.c_uint64), ("max_inflight", C.c_uint32),
                 ("u8_band", C.c_float), ("u8_round", C.c_uint32), ("reserved", C.c_uint32 * 5)]
+
+
+class rkf_scene_node(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("rotation", C.c_float * 4), ("scale", C.c_float * 3),
+                ("parent", C.c_uint32), ("visible", C.c_uint32), ("sdf_type", C.c_uint32),
+                ("primitive_type", C.c_uint32), ("params", C.c_float * 4), ("material_id", C.c_uint32),
+                ("brick_map_offset", C.c_uint32), ("brick_map_dims", C.c_uint32 * 3),
+                ("voxel_size", C.c_float), ("blend_mode", C.c_uint32), ("blend_radius", C.c_float)]
+
+
+class rkf_flat_node(C.Structure):
+    _fields_ = [("inverse_world", C.c_float * 16), ("accumulated_scale", C.c_float * 3),
+                ("depth", C.c_uint32), ("parent_index", C.c_uint32), ("node", C.c_uint32)]
 
 
 class rkf_bvh_node(C.Structure):
@@ -199,6 +215,8 @@ SIGNATURES = {
     "rkf_objects_import": (_I, [_P, _P, _U32]),
     "rkf_bvh_import": (_I, [_P, _P, _U32]),
     "rkf_objects_update": (_I, [_P, _P, _U32, _P]),
+    "rkf_flatten_object": (_I, [_P, _U32, _P, _P, _P, _P, C.POINTER(C.c_uint32)]),
+    "rkf_gpu_object_from_flat_node": (_I, [_P, _P, _U32, _P, _P, _P, _P, _P]),
     "rkf_batch_graph_create": (_I, [_P, C.POINTER(rkf_view), _U32, C.POINTER(rkf_ray_batch), _U32,
                                     C.POINTER(rkf_march_params), C.POINTER(rkf_batch_tuning), C.POINTER(_P)]),
     "rkf_batch_graph_set_cameras": (_I, [_P, C.POINTER(rkf_camera), _U32]),

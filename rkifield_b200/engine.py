@@ -49,6 +49,52 @@ def object_bvh(objects) -> C.Array:
     return build_bvh((i, o.aabb_min, o.aabb_max) for i, o in enumerate(objects))
 
 
+def scene_node(parent: int = abi.RKF_NO_PARENT, position=(0.0, 0.0, 0.0), rotation=(0.0, 0.0, 0.0, 1.0),
+               scale=(1.0, 1.0, 1.0), visible: bool = True, sdf_type: int = abi.RKF_SDF_NONE,
+               primitive_type: int = 0, params=(0.0, 0.0, 0.0, 0.0), material_id: int = 0,
+               brick_map_offset: int = 0, brick_map_dims=(0, 0, 0), voxel_size: float = 0.0,
+               blend_mode: int = abi.RKF_BLEND_SMOOTH_UNION, blend_radius: float = 0.1) -> abi.rkf_scene_node:
+    """One node of an object's tree (SceneNode, scene_node.rs); the defaults
+    are SceneNode::new's: identity transform, visible, no SDF source, smooth
+    union of radius 0.1 (BlendMode::default, scene_node.rs:124-128)."""
+    nd = abi.rkf_scene_node()
+    nd.position[:], nd.rotation[:], nd.scale[:] = list(position), list(rotation), list(scale)
+    nd.parent, nd.visible, nd.sdf_type, nd.primitive_type = int(parent), int(bool(visible)), sdf_type, primitive_type
+    nd.params[:], nd.material_id = list(params), material_id
+    nd.brick_map_offset, nd.brick_map_dims[:], nd.voxel_size = brick_map_offset, list(brick_map_dims), voxel_size
+    nd.blend_mode, nd.blend_radius = blend_mode, blend_radius
+    return nd
+
+
+def flatten_object(nodes, rotation=(0.0, 0.0, 0.0, 1.0), scale=(1.0, 1.0, 1.0),
+                   position=(0.0, 0.0, 0.0)) -> list:
+    """``flatten_object`` (transform_flatten.rs:56-110) of a tree given as
+    scene nodes in depth-first pre-order, the object's own rotation and
+    scale, and its baked (camera-relative) position: the flat nodes of the
+    visible nodes, through rkf_flatten_object."""
+    nodes = list(nodes)
+    arr = (abi.rkf_scene_node * max(1, len(nodes)))(*nodes)
+    out = (abi.rkf_flat_node * max(1, len(nodes)))()
+    n = C.c_uint32()
+    fl = lambda v: (C.c_float * len(v))(*[float(x) for x in v])  # noqa: E731
+    check(abi.load_library().rkf_flatten_object(arr, len(nodes), fl(rotation), fl(scale), fl(position), out,
+                                                C.byref(n)), "rkf_flatten_object")
+    return [out[i] for i in range(n.value)]
+
+
+def gpu_object_from_flat_node(flat: abi.rkf_flat_node, source: abi.rkf_scene_node, object_id: int,
+                              aabb_min=(0.0,) * 4, aabb_max=(0.0,) * 4, geometry_aabb_min=(0.0,) * 3,
+                              geometry_aabb_max=(0.0,) * 3) -> abi.rkf_gpu_object:
+    """``GpuObject::from_flat_node`` (gpu_object.rs:141-220) through
+    rkf_gpu_object_from_flat_node."""
+    fl = lambda v: (C.c_float * len(v))(*[float(x) for x in v])  # noqa: E731
+    o = abi.rkf_gpu_object()
+    check(abi.load_library().rkf_gpu_object_from_flat_node(
+        C.byref(flat), C.byref(source), int(object_id), fl(aabb_min), fl(aabb_max), fl(geometry_aabb_min),
+        fl(geometry_aabb_max), C.byref(o)), "rkf_gpu_object_from_flat_node")
+    return o
+
+
 def gbuffer_host(n: int, reference_planes: bool = False) -> dict:
     out = {"t": np.zeros(n, np.float32), "normal": np.zeros(3 * n, np.float32),
            "slot": np.zeros(n, np.uint32), "material": np.zeros(n, np.uint16),

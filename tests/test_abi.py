@@ -55,15 +55,17 @@ def test_c_header_layout_matches_ctypes(tmp_path):
     """Compile a C program against include/rkf_cuda.h and compare sizeof."""
     src = tmp_path / "sz.c"
     src.write_text('#include "rkf_cuda.h"\n#include <stdio.h>\n'
-                   'int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(rkf_camera),'
+                   'int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(rkf_camera),'
                    ' sizeof(rkf_scene_uniforms), sizeof(rkf_gpu_object), sizeof(rkf_march_params),'
-                   ' sizeof(rkf_config), sizeof(rkf_prim), sizeof(rkf_edit_op), sizeof(rkf_request));}\n')
+                   ' sizeof(rkf_config), sizeof(rkf_prim), sizeof(rkf_edit_op), sizeof(rkf_request),'
+                   ' sizeof(rkf_batch_tuning), sizeof(rkf_scene_node), sizeof(rkf_flat_node));}\n')
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     got = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()))
     want = [C.sizeof(t) for t in (abi.rkf_camera, abi.rkf_scene_uniforms, abi.rkf_gpu_object,
                                   abi.rkf_march_params, abi.rkf_config, abi.rkf_prim,
-                                  abi.rkf_edit_op, abi.rkf_request)]
+                                  abi.rkf_edit_op, abi.rkf_request, abi.rkf_batch_tuning,
+                                  abi.rkf_scene_node, abi.rkf_flat_node)]
     assert got == want
 
 

@@ -285,3 +285,53 @@ def test_poll_timeout_status(small_scene):
     finally:
         srv.stop()
         ctx.close()
+
+
+def test_objects_update_between_sessions(small_scene):
+    """The runtime's per-frame object upload (rkf_objects_update) is refused
+    while a serving session runs (RKF_BUSY, nothing changes), and is taken
+    between sessions: the next session renders the moved object exactly as
+    the direct march does, and differently from before the move."""
+    from rkifield_b200 import _abi as abi
+    from rkifield_b200 import engine, scenes
+    from rkifield_b200.engine import RkfError, Server
+    spec = small_scene["spec"]
+    ctx = _fresh_ctx(small_scene)
+    p = scenes.march_params(spec)
+    w, h = 160, 96
+    cam = scenes.seeded_camera(spec, w, h, seed=11)
+
+    def served():
+        srv = Server(ctx, p)
+        try:
+            out = engine.render_out(w * h)
+            t = srv.submit_render(cam, w, h, out)
+            res = srv.poll(t, 60_000_000)
+            assert res is not None and res["status"] == 0
+            return out
+        finally:
+            srv.stop()
+
+    try:
+        before = served()
+        moved = abi.rkf_gpu_object.from_buffer_copy(small_scene["obj"])
+        for a, d in enumerate((0.75, -0.5, 0.25)):  # inverse_world translation: the object moves by -d
+            moved.inverse_world[12 + a] += d
+            moved.aabb_min[a] -= d
+            moved.aabb_max[a] -= d
+        srv = Server(ctx, p)
+        try:
+            with pytest.raises(RkfError) as e:
+                ctx.update_objects([moved])
+            assert e.value.status == abi.RKF_BUSY
+        finally:
+            srv.stop()
+        assert all((served()[k].view(np.uint8) == before[k].view(np.uint8)).all() for k in before)
+        ctx.update_objects([moved])
+        after = served()
+        direct = ctx.march(cam, p, w, h)
+        for k in after:
+            assert (after[k].view(np.uint8) == direct[k].view(np.uint8)).all(), k
+        assert not (after["t"].view(np.uint8) == before["t"].view(np.uint8)).all()
+    finally:
+        ctx.close()
