@@ -529,7 +529,9 @@ RKF_API rkf_status rkf_sdf_ao(rkf_ctx* ctx, const float* pos, const float* norma
 typedef struct rkf_edit_op {
     uint32_t object_index;   /* index into the object table                  */
     uint32_t edit_type;      /* EditType: 0 union 1 subtract 2 intersect     */
-                             /* 3 smooth union 4 smooth subtract             */
+                             /* 3 smooth union 4 smooth subtract 5 smooth    */
+                             /* brush 6 flatten 7 paint (8 color paint:      */
+                             /* RKF_UNSUPPORTED, no companion color pool)    */
     uint32_t shape_type;     /* ShapeType: 0 sphere 1 box 2 capsule          */
     uint32_t falloff;        /* FalloffCurve: 0 linear 1 smooth 2 sharp      */
     float position[3];       /* object-local                                 */
@@ -542,9 +544,12 @@ typedef struct rkf_edit_op {
 } rkf_edit_op;
 
 /* Apply one edit on the device: touched allocated bricks are rewritten into
- * fresh slots (copy-on-write), EMPTY/INTERIOR bricks the brush reaches are
- * allocated and filled, and a new index epoch is published.  Requests
- * admitted before the call keep reading the previous epoch. */
+ * fresh slots (copy-on-write), EMPTY (union, smooth union) or INTERIOR
+ * (subtract, intersect, smooth subtract) bricks the brush reaches are
+ * allocated and filled, and a new index epoch is published.  The smooth
+ * brush, flatten and paint act on allocated bricks only, as
+ * find_affected_bricks (edit_op.rs:97-141) hands them to apply_edit_cpu.
+ * Requests admitted before the call keep reading the previous epoch. */
 RKF_API rkf_status rkf_edit_csg(rkf_ctx* ctx, const rkf_edit_op* op, uint64_t* new_epoch);
 
 /* ------------------------------------------------------------------------ */

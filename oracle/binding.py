@@ -82,7 +82,7 @@ def lib() -> C.CDLL:
         L.orc_apply_edit_brick.argtypes = [P, P, C.c_float, P]
         L.orc_fill_brick_with_brush.argtypes = [P, P, C.c_float, P]
         L.orc_apply_edit_planes.restype = I
-        L.orc_apply_edit_planes.argtypes = [P, P, P, C.c_float, P]
+        L.orc_apply_edit_planes.argtypes = [P, P, P, P, C.c_float, P]
         L.orc_encode_u8.argtypes = [P, C.c_float, I, P, P]
         L.orc_evaluate_falloff.restype = C.c_float
         L.orc_evaluate_falloff.argtypes = [U32, C.c_float, C.c_float]

@@ -1620,7 +1620,7 @@ float orc_evaluate_falloff(uint32_t curve, float distance, float radius) {  // c
 // the voxel centre vp blended into the existing distance and material.
 // Returns false where the falloff is zero (the voxel keeps its values).
 static bool edit_voxel(const rkf_edit_op* op, float max_extent, const float iq[4], V3<float> vp,
-                       float existing, uint32_t smat, float* nd_out, uint32_t* mat_out) {
+                       float existing, uint32_t smat, float* nd_out, uint32_t* mat_out, bool* painted) {
   const V3<float> pos = v3<float>(op->position[0], op->position[1], op->position[2]);
   const V3<float> el = quat_rotate(iq, sub(vp, pos));
   const float ela[3] = {el.x, el.y, el.z};
@@ -1661,9 +1661,18 @@ static bool edit_voxel(const rkf_edit_op* op, float max_extent, const float iq[4
       nd = -smin<float>(-existing, e, k);
       break;
     }
+    case 5:  // Smooth (:151-157)
+      nd = existing * (1.0f - strength * 0.3f);
+      break;
+    case 6:  // Flatten (:158-165): lerp(a, b, t) = a + (b - a) * t (:285-288) toward the plane y = 0
+      nd = existing + (el.y - existing) * (strength * 0.5f);
+      break;
     default:
       break;
   }
+  // Paint (:166-173): VoxelSample::new(existing, material, 0) near the surface
+  *painted = op->edit_type == 7 && std::fabs(existing) < op->dimensions[0] * 2.0f;
+  if (*painted) mat = op->material_id;
   *nd_out = nd;
   *mat_out = mat;
   return true;
@@ -1689,20 +1698,24 @@ int orc_apply_edit_brick(uint32_t* words, const float bmin[3], float vs, const r
         const uint32_t smat = (w0 >> 16) & 0x3Fu, ssec = (w0 >> 22) & 0x3Fu, sbl = w1 >> 24;
         float nd;
         uint32_t mat;
-        if (!edit_voxel(op, max_extent, iq, edit_voxel_centre(bmin, vs, vx, vy, vz), existing, smat, &nd, &mat))
+        bool painted;
+        if (!edit_voxel(op, max_extent, iq, edit_voxel_centre(bmin, vs, vx, vy, vz), existing, smat, &nd, &mat,
+                        &painted))
           continue;
-        words[2 * idx] = pack_word0(nd, mat, ssec);
-        words[2 * idx + 1] = sbl << 24;
-        if (std::fabs(nd - existing) > vs * 0.1f) any_changed = true;
+        words[2 * idx] = pack_word0(nd, mat, painted ? 0u : ssec);
+        words[2 * idx + 1] = painted ? 0u : sbl << 24;
+        if (painted || std::fabs(nd - existing) > vs * 0.1f) any_changed = true;
       }
   return any_changed ? 1 : 0;
 }
 
 // The same edit on a brick stored as planes with f32 distances (the f32 and
 // u8 pools: the distance the brush blends with is the decoded one, and the
-// result is kept unrounded).  mat holds material | secondary << 6; blend is
-// unchanged.  Returns 1 when some voxel moved by more than vs/10.
-int orc_apply_edit_planes(float* dist, uint16_t* mat, const float bmin[3], float vs, const rkf_edit_op* op) {
+// result is kept unrounded).  mat holds material | secondary << 6; blend
+// (may be null) changes only where paint clears it.  Returns 1 when some
+// voxel moved by more than vs/10 or was painted.
+int orc_apply_edit_planes(float* dist, uint16_t* mat, uint8_t* blend, const float bmin[3], float vs,
+                          const rkf_edit_op* op) {
   const float iq[4] = {-op->rotation[0], -op->rotation[1], -op->rotation[2], op->rotation[3]};
   const float max_extent = fmax_(fmax_(op->dimensions[0], op->dimensions[1]), op->dimensions[2]);
   bool any_changed = false;
@@ -1714,11 +1727,14 @@ int orc_apply_edit_planes(float* dist, uint16_t* mat, const float bmin[3], float
         const uint32_t smat = mat[idx] & 0x3Fu, ssec = (mat[idx] >> 6) & 0x3Fu;
         float nd;
         uint32_t m;
-        if (!edit_voxel(op, max_extent, iq, edit_voxel_centre(bmin, vs, vx, vy, vz), existing, smat, &nd, &m))
+        bool painted;
+        if (!edit_voxel(op, max_extent, iq, edit_voxel_centre(bmin, vs, vx, vy, vz), existing, smat, &nd, &m,
+                        &painted))
           continue;
         dist[idx] = nd;
-        mat[idx] = static_cast<uint16_t>((m & 0x3Fu) | (ssec << 6));
-        if (std::fabs(nd - existing) > vs * 0.1f) any_changed = true;
+        mat[idx] = static_cast<uint16_t>((m & 0x3Fu) | ((painted ? 0u : ssec) << 6));
+        if (painted && blend) blend[idx] = 0;
+        if (painted || std::fabs(nd - existing) > vs * 0.1f) any_changed = true;
       }
   return any_changed ? 1 : 0;
 }

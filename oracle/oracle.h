@@ -170,7 +170,8 @@ void orc_sdf_ao(const orc_scene* s, const float* pos, const float* normal, uint3
 int orc_apply_edit_brick(uint32_t* words, const float brick_local_min[3], float vs,
                          const rkf_edit_op* op);
 // The edit on a brick of planes with f32 distances (f32 and u8 pools).
-int orc_apply_edit_planes(float* dist, uint16_t* mat, const float bmin[3], float vs, const rkf_edit_op* op);
+int orc_apply_edit_planes(float* dist, uint16_t* mat, uint8_t* blend, const float bmin[3], float vs,
+                          const rkf_edit_op* op);
 // Band-normalised u8 code of one brick (the u8 pool's encoding).
 void orc_encode_u8(const float* dist, float band, int nearest, int8_t* code, float* step);
 /* fill_brick_with_brush_sdf (cpu_apply.rs:204-229). */

@@ -169,12 +169,23 @@ __global__ void __launch_bounds__(512) k_edit(EditKernelArgs a) {
         nd = -smin_e(-existing, __fadd_rn(shape_d, shift), k);
         break;
       }
+      case 5:  // Smooth (cpu_apply.rs:151-157): d * (1 - 0.3 strength)
+        nd = __fmul_rn(existing, __fsub_rn(1.0f, __fmul_rn(strength, 0.3f)));
+        break;
+      case 6:  // Flatten (:158-165): lerp toward the brush's local plane y = 0
+        nd = __fadd_rn(existing, __fmul_rn(__fsub_rn(ey, existing), __fmul_rn(strength, 0.5f)));
+        break;
       default:
         break;
     }
-    w0 = static_cast<uint32_t>(__half_as_ushort(__float2half_rn(nd))) | ((mat & 0x3Fu) << 16) | (ssec << 22);
-    w1 = sbl << 24;
-    changed = fabsf(__fsub_rn(nd, existing)) > thr;
+    // Paint (:166-173): near-surface voxels take the brush material as
+    // VoxelSample::new(d, material, 0) -- secondary and blend cleared
+    const bool paint = op.edit_type == 7 && fabsf(existing) < __fmul_rn(op.dimensions[0], 2.0f);
+    if (paint) mat = op.material_id;
+    const uint32_t sec_out = paint ? 0u : ssec, blend_out = paint ? 0u : sbl;
+    w0 = static_cast<uint32_t>(__half_as_ushort(__float2half_rn(nd))) | ((mat & 0x3Fu) << 16) | (sec_out << 22);
+    w1 = blend_out << 24;
+    changed = paint || fabsf(__fsub_rn(nd, existing)) > thr;
     out_d = nd;
   } else if (!f16) {
     // an untouched voxel of an f32 / u8 brick: the reference words carry
@@ -256,7 +267,9 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
   out->retired.clear();
   out->retired_leaves.clear();
   if (op.object_index >= c->obj_count()) return fail(RKF_INVALID_ARG, "rkf_edit_csg: object index out of range");
-  if (op.edit_type > 4 || op.shape_type > 2 || op.falloff > 2)
+  if (op.edit_type == 8)
+    return fail(RKF_UNSUPPORTED, "rkf_edit_csg: color paint writes a companion color pool this library does not keep");
+  if (op.edit_type > 8 || op.shape_type > 2 || op.falloff > 2)
     return fail(RKF_INVALID_ARG, "rkf_edit_csg: unsupported edit, shape or falloff type");
   const rkf_gpu_object& go = c->objects[op.object_index];
   if (go.sdf_type != RKF_SDF_VOXELIZED) return fail(RKF_INVALID_ARG, "rkf_edit_csg: object is not voxelized");
@@ -314,10 +327,14 @@ rkf_status apply_edit(Ctx* c, const rkf_edit_op& op, cudaStream_t st, EditOutcom
     RKF_CUDA_TRY(cudaStreamSynchronize(st));
   }
   const bool additive = op.edit_type == 0 || op.edit_type == 3;
+  // smooth, flatten and paint act on allocated bricks only, the bricks
+  // find_affected_bricks hands apply_edit_cpu (edit_op.rs:97-141)
+  const bool allocated_only = op.edit_type >= 5;
   std::vector<uint32_t> src, dst, cidx;
   std::vector<float> cmin;
   for (uint32_t i = 0; i < ncand_all; ++i) {
     const uint32_t s = cur[i];
+    if (allocated_only && (s == RKF_EMPTY_SLOT || s == RKF_INTERIOR_SLOT)) continue;
     if (s == RKF_EMPTY_SLOT && !additive) continue;
     if (s == RKF_INTERIOR_SLOT && additive) continue;
     src.push_back(s);

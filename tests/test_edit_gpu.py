@@ -53,6 +53,9 @@ def _expected(oracle, ctx, op, dims, vs, words_by_slot):
     additive = op.edit_type in (0, 3)
     exp = []
     for b, s in zip(bxyz, slots):
+        if op.edit_type >= 5 and s >= 0xFFFFFFFE:  # smooth, flatten, paint: allocated bricks only
+            exp.append((b, s, None))
+            continue
         if s == 0xFFFFFFFF:
             if not additive:
                 exp.append((b, s, None))
@@ -91,7 +94,10 @@ def test_csg_edits_match_oracle_and_march(oracle, small_scene):
                _op(1, c + np.array([0, r * 0.8, 0]), 0.5, 0),    # carve
                _op(3, c + np.array([0, 0, r + 0.3]), 0.4, 9, blend_k=0.1, falloff=2),
                _op(4, c - np.array([r * 0.5, 0, 0]), 0.7, 0, blend_k=0.1),
-               _op(0, c + np.array([-3.0, 2.0, 1.0]), 0.3, 11, shape=1, dims=(0.3, 0.2, 0.4))]
+               _op(0, c + np.array([-3.0, 2.0, 1.0]), 0.3, 11, shape=1, dims=(0.3, 0.2, 0.4)),
+               _op(5, c + np.array([r, 0, 0]), 0.5, 0),                      # smooth brush
+               _op(6, c + np.array([0, r, 0]), 0.6, 0, falloff=0),          # flatten
+               _op(7, c + np.array([0, 0, -r]), 0.3, 13)]                    # paint
         for op in ops:
             words = ctx.export_pool(0, cap)
             exp = _expected(oracle, ctx, op, v.dims, spec.voxel_size,
@@ -126,6 +132,15 @@ def test_csg_edits_match_oracle_and_march(oracle, small_scene):
                 continue
             assert_bits_equal(got[k], ref[k], k)
             assert_bits_equal(plain[k], ref[k], "plain " + k)
+        # color paint writes a companion color pool this library does not keep
+        from rkifield_b200 import _abi as abi
+        from rkifield_b200.engine import RkfError
+        e0 = ctx.info()["epoch"]
+        for kind, status in ((8, abi.RKF_UNSUPPORTED), (9, abi.RKF_INVALID_ARG)):
+            with pytest.raises(RkfError) as e:
+                ctx.edit(_op(kind, c, 0.3, 1))
+            assert e.value.status == status
+        assert ctx.info()["epoch"] == e0
 
 
 @pytest.mark.parametrize("precision,u8_round", [("f32", 0), ("u8", 0), ("u8", 1)],
@@ -153,7 +168,10 @@ def test_csg_edits_on_f32_and_u8_pools(oracle, small_scene, precision, u8_round)
         ops = [_op(0, c + np.array([r, 0, 0]), 0.6, 7),
                _op(1, c + np.array([0, r * 0.8, 0]), 0.5, 0),
                _op(3, c + np.array([0, 0, r + 0.3]), 0.4, 9, blend_k=0.1, falloff=2),
-               _op(4, c - np.array([r * 0.5, 0, 0]), 0.7, 0, blend_k=0.1)]
+               _op(4, c - np.array([r * 0.5, 0, 0]), 0.7, 0, blend_k=0.1),
+               _op(5, c + np.array([r, 0, 0]), 0.5, 0),
+               _op(6, c + np.array([0, r, 0]), 0.6, 0, falloff=0),
+               _op(7, c + np.array([0, 0, -r]), 0.3, 13)]
         L = oracle.lib()
         for op in ops:
             pl = ctx.export_planes(0, cap)
@@ -162,7 +180,8 @@ def test_csg_edits_on_f32_and_u8_pools(oracle, small_scene, precision, u8_round)
             additive = op.edit_type in (0, 3)
             exp = []
             for b, s in zip(bxyz, slots):
-                if (s == abi.EMPTY_SLOT and not additive) or (s == abi.INTERIOR_SLOT and additive):
+                if (s == abi.EMPTY_SLOT and not additive) or (s == abi.INTERIOR_SLOT and additive) or \
+                        (op.edit_type >= 5 and s >= abi.INTERIOR_SLOT):
                     exp.append((b, s, None))
                     continue
                 if s >= abi.INTERIOR_SLOT:
@@ -176,8 +195,8 @@ def test_csg_edits_on_f32_and_u8_pools(oracle, small_scene, precision, u8_round)
                     m = pl["mat"][sl].copy()
                     bl = pl["blend"][sl].copy()
                 bmin = (origin + b.astype(np.float32) * be).astype(np.float32)
-                changed = L.orc_apply_edit_planes(d.ctypes.data, m.ctypes.data, bmin.ctypes.data, float(vs),
-                                                  C.byref(op))
+                changed = L.orc_apply_edit_planes(d.ctypes.data, m.ctypes.data, bl.ctypes.data, bmin.ctypes.data,
+                                                  float(vs), C.byref(op))
                 if not changed:
                     exp.append((b, s, None))
                     continue

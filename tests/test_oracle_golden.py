@@ -226,6 +226,50 @@ def test_edit_sphere_subtract_carves(oracle):  # sphere_subtract_carves
     assert f32(oracle, int(w[2 * i]) & 0xFFFF) > -0.5
 
 
+def test_edit_paint_sets_material_near_surface(oracle):  # paint_sets_material_near_surface
+    """Paint (cpu_apply.rs:166-173): voxels with |d| < 2 dims.x take the
+    brush material as VoxelSample::new(d, material, 0) -- secondary material
+    and blend weight cleared, distance kept -- and the brick counts as
+    modified; the others keep everything."""
+    w = brick_words(oracle, lambda x, y, z: 0.01 if (y == 4 and z == 4) else 1.0, lambda x, y, z: 1)
+    w[0::2] |= np.uint32(9 << 22)
+    w[1::2] = np.uint32(200 << 24)
+    before = w.copy()
+    op = edit_op(7, (0.2, 0.2, 0.2), 0.5, 0.0, 42)
+    mod = oracle.lib().orc_apply_edit_brick(w.ctypes.data, np.zeros(3, np.float32).ctypes.data, 0.05, C.byref(op))
+    assert mod == 1
+    i = 4 + 4 * 8 + 4 * 64
+    assert (int(w[2 * i]) >> 16) & 0x3F == 42 and (int(w[2 * i]) >> 22) & 0x3F == 0 and int(w[2 * i + 1]) == 0
+    assert int(w[2 * i]) & 0xFFFF == int(before[2 * i]) & 0xFFFF
+    j = 1 + 2 * 8 + 3 * 64  # |d| = 1.0, not below 2 * 0.5
+    assert w[2 * j] == before[2 * j] and w[2 * j + 1] == before[2 * j + 1]
+
+
+def test_edit_smooth_scales_distance(oracle):  # smooth_operation_reduces_distance
+    w = brick_words(oracle, lambda x, y, z: (x - 3.5) * 0.1, lambda x, y, z: 1)
+    before = w.copy()
+    op = edit_op(5, (0.2, 0.2, 0.2), 0.5, 0.0, 0)
+    mod = oracle.lib().orc_apply_edit_brick(w.ctypes.data, np.zeros(3, np.float32).ctypes.data, 0.05, C.byref(op))
+    assert mod == 1
+    for x in (0, 7):
+        i = x + 4 * 8 + 4 * 64
+        assert abs(f32(oracle, int(w[2 * i]) & 0xFFFF)) < abs(f32(oracle, int(before[2 * i]) & 0xFFFF))
+
+
+def test_edit_flatten_pulls_toward_plane(oracle):
+    """Flatten (cpu_apply.rs:158-165): d moves toward the brush's local
+    plane distance (edit-local y) by half the strength at the voxel."""
+    w = brick_words(oracle, lambda x, y, z: 1.0, lambda x, y, z: 1)
+    op = edit_op(6, (0.2, 0.2, 0.2), 0.5, 0.0, 0)
+    mod = oracle.lib().orc_apply_edit_brick(w.ctypes.data, np.zeros(3, np.float32).ctypes.data, 0.05, C.byref(op))
+    assert mod == 1
+    for y in (0, 7):
+        i = 4 + y * 8 + 4 * 64
+        plane = (y + 0.5) * 0.05 - 0.2
+        d = f32(oracle, int(w[2 * i]) & 0xFFFF)
+        assert plane < d < 1.0
+
+
 def test_edit_shape_and_falloff(oracle):
     L = oracle.lib()
     z = np.zeros(3, np.float32)
