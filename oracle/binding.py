@@ -78,6 +78,8 @@ def lib() -> C.CDLL:
         L.orc_march.argtypes = [P, P, P, U32, U32, I, I, U32, U32] + [P] * 12 + [I, P]
         L.orc_trace_rays.argtypes = [P, P, P, P, U32, U32, P, I, I] + [P] * 7
         L.orc_query_points.argtypes = [P, P, U32, P, P, P, I]
+        L.orc_shadow_shader.argtypes = [P, P, P, P, U32, P, I, P]
+        L.orc_sdf_ao_shader.argtypes = [P, P, P, U32, P, I, P]
         L.orc_apply_edit_brick.restype = I
         L.orc_apply_edit_brick.argtypes = [P, P, C.c_float, P]
         L.orc_fill_brick_with_brush.argtypes = [P, P, C.c_float, P]
@@ -318,6 +320,30 @@ def sdf_ao(scene: Scene, pos, normal, threads: int | None = None):
     normal = np.ascontiguousarray(normal, np.float32).ravel()
     out = np.zeros(pos.size // 3, np.float32)
     lib().orc_sdf_ao(C.byref(scene.s), ptr(pos), ptr(normal), out.size, ptr(out), threads or nthreads())
+    return out
+
+
+def shadow_shader(scene: Scene, origins, dirs, tmax, cam_pos, threads: int | None = None):
+    """soft_shadow through the shading pass's coarse-field sample_sdf, seen
+    from the camera at cam_pos (orc_shadow_shader)."""
+    origins = np.ascontiguousarray(origins, np.float32).ravel()
+    dirs = np.ascontiguousarray(dirs, np.float32).ravel()
+    tmax = np.ascontiguousarray(tmax, np.float32).ravel()
+    cam = np.ascontiguousarray(cam_pos[:3], np.float32)
+    out = np.zeros(tmax.size, np.float32)
+    lib().orc_shadow_shader(C.byref(scene.s), ptr(origins), ptr(dirs), ptr(tmax), tmax.size, ptr(cam),
+                            threads or nthreads(), ptr(out))
+    return out
+
+
+def sdf_ao_shader(scene: Scene, pos, normal, cam_pos, threads: int | None = None):
+    """sdf_ao through the shading pass's coarse-field sample_sdf (orc_sdf_ao_shader)."""
+    pos = np.ascontiguousarray(pos, np.float32).ravel()
+    normal = np.ascontiguousarray(normal, np.float32).ravel()
+    cam = np.ascontiguousarray(cam_pos[:3], np.float32)
+    out = np.zeros(pos.size // 3, np.float32)
+    lib().orc_sdf_ao_shader(C.byref(scene.s), ptr(pos), ptr(normal), out.size, ptr(cam), threads or nthreads(),
+                            ptr(out))
     return out
 
 

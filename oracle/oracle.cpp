@@ -1573,6 +1573,83 @@ void orc_sdf_ao(const orc_scene* s, const float* pos, const float* normal, uint3
   });
 }
 
+// The shading pass's own sample_sdf (shade_common.wgsl:521-572): the coarse
+// field at the camera-relative position first (sample_coarse_field, :504-511,
+// the filter model of coarse_sample), its value where above
+// COARSE_NEAR_THRESHOLD 0.5 (:291), else the minimum of evaluate_object over
+// the objects (the shader walks the BVH for it; on scenes whose objects'
+// distances are at least their box distances the walk's minimum is the
+// same).  The library's SHADOW mode and rkf_sdf_ao use the minimum
+// everywhere (the coarse value comes from a texture unit and cannot be
+// pinned); these two let the tests bound the difference.
+static float shader_sample_sdf(Marcher<float>& mc, const orc_scene* s, const CoarseField& cf, const float ocr[3],
+                               const float cam[3], V3<float> q) {
+  const float cd = coarse_sample(cf, ocr, q.x - cam[0], q.y - cam[1], q.z - cam[2]);
+  if (cd > 0.5f) return cd;
+  float d = kMaxFloat;
+  for (uint32_t oi = 0; oi < s->num_objects; ++oi) {
+    uint32_t m;
+    const float e = mc.evaluate(q, oi, &m, false);
+    d = e < d ? e : d;
+  }
+  return d;
+}
+
+// soft_shadow (shade_common_shading.wgsl:9-33) through the shader's sample_sdf.
+void orc_shadow_shader(const orc_scene* s, const float* origins, const float* dirs, const float* tmax, uint32_t n,
+                       const float cam[3], int threads, float* shadow) {
+  const CoarseField cf = coarse_build(s);
+  float ocr[3];
+  for (int a = 0; a < 3; ++a) ocr[a] = cf.origin[a] - cam[a];
+  parallel_for(n, threads, [&](uint64_t i, int) {
+    Tracker tr;
+    Marcher<float> mc{s, &tr, nullptr};
+    const V3<float> o = v3<float>(origins[3 * i], origins[3 * i + 1], origins[3 * i + 2]);
+    const V3<float> ld = v3<float>(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]);
+    float sh = 1.0f, t = 0.005f;
+    uint32_t near_steps = 0;
+    bool blocked = false;
+    for (uint32_t k = 0; k < 256u; ++k) {
+      if (near_steps >= 32u || t > tmax[i]) break;
+      const float d = shader_sample_sdf(mc, s, cf, ocr, cam, add(o, mul(ld, t)));
+      if (d < 0.005f) {
+        blocked = true;
+        break;
+      }
+      if (d < 0.02f) {
+        sh = fmin_(sh, 16.0f * d / t);
+        near_steps++;
+      }
+      t += fmax_(d, 0.005f);
+    }
+    shadow[i] = blocked ? 0.0f : clampf(sh, 0.0f, 1.0f);
+  });
+}
+
+// sdf_ao (shade_common_shading.wgsl:37-47) through the shader's sample_sdf.
+void orc_sdf_ao_shader(const orc_scene* s, const float* pos, const float* normal, uint32_t n, const float cam[3],
+                       int threads, float* ao) {
+  const CoarseField cf = coarse_build(s);
+  float ocr[3];
+  for (int a = 0; a < 3; ++a) ocr[a] = cf.origin[a] - cam[a];
+  parallel_for(n, threads, [&](uint64_t i, int) {
+    Tracker tr;
+    Marcher<float> mc{s, &tr, nullptr};
+    const V3<float> p = v3<float>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+    const V3<float> nv = v3<float>(normal[3 * i], normal[3 * i + 1], normal[3 * i + 2]);
+    float acc = 0.0f, scale = 1.0f;
+    for (uint32_t k = 1; k <= 4; ++k) {
+      const float dist = 0.12f * static_cast<float>(k);
+      const float d = shader_sample_sdf(mc, s, cf, ocr, cam, add(p, mul(nv, dist)));
+      acc = acc + scale * (dist - d);
+      scale = scale * 0.5f;
+    }
+    const float v = 1.0f - 0.7f * acc;
+    const float lo = v < 0.0f ? 0.0f : v;
+    ao[i] = lo > 1.0f ? 1.0f : lo;
+  });
+}
+
 // ---------------------------------------------------------------------------
 // CSG edits (crates/rkf-edit/src/cpu_apply.rs)
 // ---------------------------------------------------------------------------

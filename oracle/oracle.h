@@ -164,6 +164,15 @@ void orc_query_points(const orc_scene* s, const float* points, uint32_t n,
 void orc_sdf_ao(const orc_scene* s, const float* pos, const float* normal, uint32_t n, float* ao,
                 int threads);
 
+/* soft_shadow and sdf_ao through the shading pass's own sample_sdf
+ * (shade_common.wgsl:521-572: the coarse field beyond 0.5 m, seen from the
+ * camera at cam), for bounding how far the library's exact-distance forms
+ * move from it. */
+void orc_shadow_shader(const orc_scene* s, const float* origins, const float* dirs, const float* tmax, uint32_t n,
+                       const float cam[3], int threads, float* shadow);
+void orc_sdf_ao_shader(const orc_scene* s, const float* pos, const float* normal, uint32_t n, const float cam[3],
+                       int threads, float* ao);
+
 /* CPU CSG edit on one brick (cpu_apply.rs:28-200): rewrites the 1024 words
  * of the brick in place; brick_local_min as find_affected_bricks computes
  * it.  Returns 1 when the brick counts as modified. */
