@@ -723,6 +723,33 @@ __device__ __noinline__ uint32_t empty_run_set(const ObjDev* objs, const EmptyVo
   return c;
 }
 
+constexpr uint32_t kRefillRounds = 8;
+
+// The outputs of a ray that ends at its first check, unhit, with no step
+// taken (its tmax is below its starting t): what the epilogue writes for it.
+__device__ __noinline__ void write_unmarched(const Segment& sg, uint32_t idx, uint32_t mode,
+                                             const rkf_march_params& p) {
+  if (mode == RKF_TRACE_SHADOW) {
+    sg.t[idx] = 1.0f;  // clampf(1, 0, 1)
+    if (sg.flags) sg.flags[idx] = 0;
+    return;
+  }
+  const uint16_t flags = (0u >= p.hard_max_steps || 0u >= p.scene.max_steps) ? RKF_FLAG_STEPS_OUT : 0;
+  sg.t[idx] = kMaxFloat;
+  if (sg.flags) sg.flags[idx] = flags;
+  if (mode == RKF_TRACE_ANY) return;
+  if (sg.normal) {
+    sg.normal[3 * static_cast<size_t>(idx)] = 0.0f;
+    sg.normal[3 * static_cast<size_t>(idx) + 1] = 0.0f;
+    sg.normal[3 * static_cast<size_t>(idx) + 2] = 0.0f;
+  }
+  if (sg.slot) sg.slot[idx] = RKF_EMPTY_SLOT;
+  if (sg.material) sg.material[idx] = 0;
+  if (sg.position) reinterpret_cast<float4*>(sg.position)[idx] = make_float4(0.f, 0.f, 0.f, kMaxFloat);
+  if (sg.packed) sg.packed[idx] = 0u;
+  if (sg.motion) reinterpret_cast<float4*>(sg.motion)[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
 template <int PREC, int OBJ>
 __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_constant__ KParams kp) {
   constexpr bool MULTI_TILED = OBJ == OBJ_MULTI_EMPTY_TILED;
@@ -757,9 +784,14 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
 
   for (;;) {
     // ---- 1. refill idle lanes ------------------------------------------------
-    {
+    // A ray that ends before its first sample (tmax below its starting t:
+    // the secondary rays of pixels that missed) takes its outputs here and
+    // its lane takes the next id at once, for up to kRefillRounds rounds, so
+    // that such rays do not leave lanes idle through the march loop.
+    for (uint32_t round = 0; round < kRefillRounds; ++round) {
       const bool idle = state == ST_IDLE;
       const uint32_t need = __ballot_sync(kFull, idle);
+      bool again = false;  // this lane's id ended at once (or is off the view)
       if (need && !exhausted) {
         const uint32_t leader = __ffs(need) - 1;
         unsigned long long base = 0;
@@ -857,14 +889,26 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
                 // a tile with no objects is sky (ray_march.wgsl:895-897)
                 state = (TILES && cs.tile_count == 0) ? ST_EPI : ST_MARCH;
               }
+              if (state != ST_EPI && t > tmax) {
+                // its first check ends it unhit with no step taken: the
+                // epilogue's outputs for that (shadow 1; t max, normal 0,
+                // EMPTY slot, material 0, STEPS_OUT only when the near-step
+                // limit is 0, the miss position and motion)
+                write_unmarched(sg, cs.idx, mode, p);
+                state = ST_IDLE;
+                again = true;
+              }
+            } else {
+              again = true;
             }
           }
         }
       }
-      if (__all_sync(kFull, state == ST_IDLE)) {
-        if (exhausted) break;
-        continue;
-      }
+      if (!__any_sync(kFull, again)) break;
+    }
+    if (__all_sync(kFull, state == ST_IDLE)) {
+      if (exhausted) break;
+      continue;
     }
     // the march steps along the safe direction (ray_march.wgsl:784); cs.hit
     // positions use the raw direction (:1068)

@@ -46,6 +46,42 @@ def test_trace_rays_bit_exact(oracle, small_scene, small_ctx, mode):
     assert 100 < hits < 20000
 
 
+@pytest.mark.parametrize("mode", [0, 1, 2], ids=["closest", "any", "shadow"])
+@pytest.mark.parametrize("max_steps", [None, 0], ids=["default", "no_near_steps"])
+def test_rays_ending_at_their_first_check(oracle, small_scene, small_ctx, mode, max_steps):
+    """Rays whose tmax lies below their starting t (0, or 0.005 for soft
+    shadows) end unhit at their first check; the kernel writes their outputs
+    while refilling and hands the lane the next id.  Mixed with live rays
+    (many such rays in a row, as the secondary rays of pixels that missed),
+    with tmax just around the starting t, -0, NaN and infinity, and with a
+    near-step limit of 0 (every ray then ends with STEPS_OUT): bit-exact
+    with the oracle in every mode."""
+    from rkifield_b200 import scenes
+    v = small_scene["vox"]
+    sc = oracle.Scene([small_scene["obj"]], pool_words=v.words, brick_maps=v.map)
+    o, d, tmax = _rays(12000, seed=40 + mode)
+    rng = np.random.default_rng(77)
+    dead = rng.random(tmax.size) < 0.85
+    tmax[dead] = -1.0
+    special = np.float32([0.0, -0.0, 1e-30, -1e-30, 0.003, 0.005, 0.0051, np.nan, np.inf, -np.inf])
+    tmax[:special.size] = special
+    tmax[5000:8000] = -1.0  # a long run of them
+    p = scenes.march_params(scenes.SCENE_SMALL)
+    if max_steps is not None:
+        p.scene.max_steps = max_steps
+    ref = oracle.trace(sc, o.ravel(), d.ravel(), tmax, mode, p)
+    got = small_ctx.trace(o, d, tmax, mode, p)
+    for k in ref:
+        if k in got:
+            assert_bits_equal(got[k], ref[k], k)
+    # also alone: every ray of a batch ends at once
+    ref = oracle.trace(sc, o[:512].ravel(), d[:512].ravel(), np.full(512, -2.0, np.float32), mode, p)
+    got = small_ctx.trace(o[:512], d[:512], np.full(512, -2.0, np.float32), mode, p)
+    for k in ref:
+        if k in got:
+            assert_bits_equal(got[k], ref[k], "all ending at once " + k)
+
+
 def test_trace_zero_rays(small_ctx):
     from rkifield_b200 import scenes
     out = small_ctx.trace(np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32),
