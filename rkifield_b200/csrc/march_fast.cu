@@ -71,11 +71,12 @@ static_assert(sizeof(ColdState) % 8 == 4, "ColdState must span an odd number of 
 // value, so wherever the voxelized object samples EMPTY, the minimum over
 // the scene is that sample, bit for bit.
 struct FarBall {
-  float c[3];     // world-space centre
-  float a, b;     // radius a + b * P (box: margin a + b * P beyond the half extents)
+  float c[3];     // world-space centre (half-space: the coefficients G)
+  float a, b;     // radius a + b * P (box: margin a + b * P beyond the half extents;
+                  // half-space: G.w + H <= a + b * P)
   uint32_t path;  // the object's index in the empty-space path (KParams::ev), or ~0u
-  float h[3];     // box: world-space half extents
-  uint32_t box;   // 1: an axis-aligned box around c instead of a ball
+  float h[3];     // box: world-space half extents (half-space: h[0] = H)
+  uint32_t box;   // 1: an axis-aligned box around c instead of a ball; 2: a half-space
 };
 
 // One voxelized object of the multi-object empty-space path.  Wherever the
@@ -248,6 +249,28 @@ __device__ __noinline__ float far_limit(const FarBall* __restrict__ far, uint32_
   for (uint32_t j = 0; j < n; ++j) {
     const FarBall& f = far[j];
     if (f.path < 32u && ((skip >> f.path) & 1u)) continue;  // an object of the run's set
+    if (f.box == 2) {
+      // half-space G.w + H <= m, m = a + b*P (a plane's small values lie in
+      // it): along the ray its coordinate G.(o + d u) + H - m is at least
+      // s0 + s1 u for u >= 0, both rounded down
+      const float m = __fadd_ru(f.a, __fmul_ru(f.b, P));
+      const float s0 = __fsub_rd(__fadd_rd(__fadd_rd(__fadd_rd(__fmul_rd(f.c[0], ox), __fmul_rd(f.c[1], oy)),
+                                                     __fmul_rd(f.c[2], oz)), f.h[0]), m);
+      const float s1 = __fadd_rd(__fadd_rd(__fmul_rd(f.c[0], dx), __fmul_rd(f.c[1], dy)), __fmul_rd(f.c[2], dz));
+      const float now = __fadd_rd(s0, __fmul_rd(s1, t));  // t >= 0
+      if (s1 >= 0.0f) {
+        if (now > 0.0f) continue;  // outside and not approaching: never inside
+        inside = true;             // may be inside now
+        // s0 <= now <= 0: outside again for u > -s0 / s1
+        if (s1 > 0.0f) recheck = fminf(recheck, __fdiv_ru(-s0, s1));
+      } else if (s1 < 0.0f && now > 0.0f) {
+        // approaching, outside now (s0 > 0): inside no earlier than s0 / -s1
+        lim = fminf(lim, fmaxf(t, __fdiv_rd(s0, -s1)));
+      } else {  // inside from now on, or NaN
+        inside = true;
+      }
+      continue;
+    }
     if (f.box) {
       // slab test of the box [c - h - m, c + h + m], m = a + b*P: the entry
       // time rounded down and the exit time rounded up
@@ -1590,6 +1613,48 @@ bool far_ball(const ObjDev& o, float empty_hi, detail::FarBall* out) {
          std::isfinite(out->b);
 }
 
+// The half-space of an analytic plane for EMPTY values up to empty_hi.  The
+// plane's value (ray_march.wgsl:206-208, 257-258) is s * n.l with n the
+// normalised normal and l = A w + t the local position: exactly G.w + H with
+// G = s A^T n, H = s n.t.  The computed value differs from that by at most
+// 2^-16 s (|A|_F |w| + |t|) -- about twenty roundings of 2^-24 each over the
+// local transform, the normalisation and the dot product -- and the sample
+// positions from the line by 2^-16 |w|, so wherever G.w + H exceeds
+// empty_hi (1 + 2^-16) + 2^-16 (s |t| + (s |A|_F + |G|) |w|) the plane's value
+// exceeds every EMPTY value; |w| <= P along the ray.  Refused for a zero or
+// non-finite normal or transform.
+bool far_plane(const ObjDev& o, float empty_hi, detail::FarBall* out) {
+  std::memset(out, 0, sizeof(*out));
+  out->path = ~0u;
+  const double s = o.min_scale;
+  const double nl = std::sqrt(static_cast<double>(o.params[0]) * o.params[0] +
+                              static_cast<double>(o.params[1]) * o.params[1] +
+                              static_cast<double>(o.params[2]) * o.params[2]);
+  if (!(nl > 0.0) || !std::isfinite(nl) || !(s > 0.0) || !std::isfinite(s)) return false;
+  double n[3], G[3] = {0.0, 0.0, 0.0}, H = 0.0, fa = 0.0, tn = 0.0, gn = 0.0;
+  for (int i = 0; i < 3; ++i) n[i] = static_cast<double>(o.params[i]) / nl;
+  for (int i = 0; i < 3; ++i) {  // l_i = sum_k m[4k + i] w_k + m[12 + i]
+    for (int k = 0; k < 3; ++k) {
+      const double aik = o.m[4 * k + i];
+      G[k] += s * n[i] * aik;
+      fa += aik * aik;
+    }
+    H += s * n[i] * o.m[12 + i];
+    tn += static_cast<double>(o.m[12 + i]) * o.m[12 + i];
+  }
+  for (int k = 0; k < 3; ++k) gn += G[k] * G[k];
+  const double e16 = 0x1p-16, e20 = 0x1p-20;
+  const double a = static_cast<double>(empty_hi) * (1.0 + e16) + e16 * s * std::sqrt(tn) + e20;
+  const double b = e16 * (s * std::sqrt(fa) + std::sqrt(gn)) + e20;
+  for (int k = 0; k < 3; ++k) out->c[k] = static_cast<float>(G[k]);
+  out->h[0] = static_cast<float>(H);
+  out->a = static_cast<float>(up_float(a));
+  out->b = static_cast<float>(up_float(b));
+  out->box = 2;
+  return std::isfinite(out->c[0]) && std::isfinite(out->c[1]) && std::isfinite(out->c[2]) &&
+         std::isfinite(out->h[0]) && std::isfinite(out->a) && std::isfinite(out->b);
+}
+
 // A scene of several objects the multi-object empty-space path can march:
 // one to kMaxEmptyVox voxelized objects that qualify for the empty-space path
 // (the first ones by index), each of which takes EMPTY runs on its own field,
@@ -1624,7 +1689,8 @@ bool multi_empty_scene(const Ctx* c, detail::EmptyVox* ev, uint32_t* n_ev, detai
       return false;
     }
     detail::FarBall b;
-    if (!far_ball(o, hi, &b)) return false;
+    const bool plane = o.sdf_type == RKF_SDF_ANALYTICAL && o.prim_type == RKF_PRIM_PLANE;
+    if (!(plane ? far_plane(o, hi, &b) : far_ball(o, hi, &b))) return false;
     b.path = path_of[i];
     if (balls) balls[nb] = b;
     ++nb;

@@ -112,9 +112,9 @@ def test_large_view_tiled_rows_bit_exact(oracle, large, large_oracle):
 
 def test_large_view_with_analytic_objects_rows_bit_exact(oracle, large):
     """The multi-object empty-space path at full size: analytic objects in
-    front of the camera (spheres, a rotated and scaled box) and one far away,
-    beside the voxelized object; EMPTY runs and settling chains stop at each
-    object's ball.  The whole frame (brute strategy) and sampled rows (tiled
+    front of the camera (spheres, a rotated and scaled box), one far away and
+    a ground plane below the cube, beside the voxelized object; EMPTY runs and
+    settling chains stop at each object's ball or the plane's half-space.  The whole frame (brute strategy) and sampled rows (tiled
     strategy) bit-exact against the oracle reading the same planes and index.
     The scene is restored afterwards."""
     from test_multi_empty_gpu import _rotation, _transformed
@@ -135,6 +135,9 @@ def test_large_view_with_analytic_objects_rows_bit_exact(oracle, large):
     props.append(_transformed(1, tuple(float(v) for v in c), (2.0, 1.0, 1.5), _rotation((1, 2, 3), 0.7),
                               (1.5, 0.7, 1.2), 7, 20))
     props.append(_analytic(0, (0.0, 0.0, 500.0), (1.0,), (1.0, 1.0, 1.0), 5, 21))
+    # a ground plane just below the cube: the runs stop at its half-space
+    from test_multi_empty_gpu import _plane
+    props.append(_plane((0.0, 1.0, 0.0), (0.0, -spec.cube * 0.5 - 1.0, 0.0), 9, 22))
     try:
         ctx.update_objects([vox] + props, [0] + [-1] * len(props))
         n = ctx.info()["pool_bricks_used"]

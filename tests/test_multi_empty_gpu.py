@@ -7,8 +7,8 @@ output stays bit-exact against the oracle: views, and ray casts in the three
 modes (closest, any hit, soft shadow), with analytic objects outside the
 grid, just beyond it and inside it, rotated and non-uniformly scaled, and the
 voxelized object not first in the list, under the brute, tiled and BVH
-strategies.  Scenes the path does not cover (a plane) march the plain
-multi-object kernel.  A tuning without the empty path marches the
+strategies.  A plane bounds the runs by the half-space where its value may
+fall to an EMPTY value.  A tuning without the empty path marches the
 full sampler only, with the same outputs, and the autotuner may pick it."""
 import ctypes as C
 
@@ -148,33 +148,65 @@ def test_rays_bit_exact(oracle, small_scene, mode):
         ctx.close()
 
 
-def test_scenes_outside_the_path_march_the_plain_kernel(oracle, small_scene):
+def _plane(normal, point, mat, oid, rot=None):
+    """An analytic plane through `point` (world) with local normal `normal`,
+    optionally rotated: inverse_world maps world to local, l = R^T (p - point)."""
+    o = _analytic(5, point, tuple(normal), (60.0, 60.0, 60.0), mat, oid)
+    if rot is not None:
+        a = rot.T
+        t = -a @ np.asarray(point, np.float64)
+        for i in range(3):
+            for k in range(3):
+                o.inverse_world[4 * k + i] = float(a[i, k])
+            o.inverse_world[12 + i] = float(t[i])
+    return o
+
+
+@pytest.mark.parametrize("case", ["ground_below", "tilted_through", "above_camera_side"])
+def test_scenes_with_a_plane_take_the_multi_object_path(oracle, small_scene, case):
+    """A plane (ray_march.wgsl:206-208, 257-258) bounds the EMPTY runs by the
+    half-space where its value may drop to an EMPTY value; views under the
+    brute and tiled strategies and ray casts in the three modes, bit-exact
+    with the oracle: a ground plane below the grid, a tilted plane through
+    it, and a plane whose near side holds the camera."""
     from rkifield_b200 import _abi as abi
+    from rkifield_b200 import scenes
     v = small_scene["vox"]
-    w, h = 96, 64
-    cam = _camera(4, w, h)
-    # a plane has no ball
-    objs = _scene_objects(small_scene) + [_analytic(5, (0.0, -17.0, 0.0), (0.0, 1.0, 0.0), (50.0, 0.1, 50.0), 3, 8)]
+    w, h = 120, 80
+    plane = {"ground_below": _plane((0.0, 1.0, 0.0), (0.0, -17.0, 0.0), 3, 8),
+             "tilted_through": _plane((0.0, 1.0, 0.0), (2.0, -3.0, 1.0), 3, 8, rot=_rotation((1.0, 0.0, 0.4), 0.5)),
+             "above_camera_side": _plane((0.0, -1.0, 0.0), (0.0, 24.0, 0.0), 3, 8)}[case]
+    objs = _scene_objects(small_scene) + [plane]
     sc = oracle.Scene(objs, pool_words=v.words, brick_maps=v.map)
     ctx = _context(small_scene, objs)
     try:
+        hits = 0
+        for strategy, variant in ((0, VARIANT_MULTI_EMPTY), (abi.RKF_STRATEGY_TILED, VARIANT_MULTI_EMPTY_TILED)):
+            p = _params(strategy)
+            for seed in (4, 6):
+                cam = _camera(seed, w, h)
+                ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
+                got = ctx.march(cam, p, w, h, reference_planes=True)
+                assert ctx.lib.rkf_testing_last_variant(ctx.h) == variant
+                for k in PLANES:
+                    assert_bits_equal(got[k], ref[k], f"{case} strategy {strategy} seed {seed}: {k}")
+                hits += int(((ref["packed_material"] >> 24) & 0xFF == 8).sum())
+        # a camera inside the grid looking down at the ground plane
+        cam = scenes.camera_uniforms((3.0, 6.0, 9.0), (0.0, -17.0, 0.0), w, h)
         p = _params(0)
         ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
         got = ctx.march(cam, p, w, h, reference_planes=True)
-        assert ctx.lib.rkf_testing_last_variant(ctx.h) == VARIANT_MULTI
         for k in PLANES:
-            assert_bits_equal(got[k], ref[k], f"with a plane: {k}")
-    finally:
-        ctx.close()
-    # the tiled strategy over a scene with a plane: the plain kernel's tiled steps
-    ctx = _context(small_scene, objs)
-    try:
-        p = _params(abi.RKF_STRATEGY_TILED)
-        ref = oracle.march(sc, cam, p, w, h, with_reference_planes=True)
-        got = ctx.march(cam, p, w, h, reference_planes=True)
-        assert ctx.lib.rkf_testing_last_variant(ctx.h) == VARIANT_MULTI
-        for k in PLANES:
-            assert_bits_equal(got[k], ref[k], f"tiled with a plane: {k}")
+            assert_bits_equal(got[k], ref[k], f"{case} looking down: {k}")
+        hits += int(((ref["packed_material"] >> 24) & 0xFF == 8).sum())
+        assert hits > 50, "the views should see the plane"
+        o, d, tmax = _rays(6000, seed=9)
+        for mode in (abi.RKF_TRACE_CLOSEST, abi.RKF_TRACE_ANY, abi.RKF_TRACE_SHADOW):
+            ref = oracle.trace(sc, o.ravel(), d.ravel(), tmax, mode, _params(0))
+            got = ctx.trace(o, d, tmax, mode, _params(0))
+            assert ctx.lib.rkf_testing_last_variant(ctx.h) == VARIANT_MULTI_EMPTY
+            for k in got:
+                assert_bits_equal(got[k], ref[k], f"{case} rays mode {mode}: {k}")
     finally:
         ctx.close()
 
