@@ -783,7 +783,10 @@ __global__ void __launch_bounds__(256, 4) k_march_persistent(const __grid_consta
   constexpr bool TILES = OBJ != OBJ_SINGLE_EMPTY && OBJ != OBJ_MULTI_EMPTY;
   // warp-shared EMPTY runs in the launch's tail (shared_runs)
   constexpr bool SHARE = OBJ == OBJ_SINGLE_EMPTY;
-  const ObjDev* sh_objs = kp.objs;
+  // the object table: the launch parameters hold up to kMaxObjectsFast
+  // records; a larger scene (the plain multi-object variant only) reads the
+  // device copy
+  const ObjDev* sh_objs = (OBJ == OBJ_MULTI && kp.s.n_objs > kMaxObjectsFast) ? kp.s.objs : kp.objs;
   const SceneDev& s = kp.s;
   const rkf_march_params& p = kp.p;
   const uint32_t lane = threadIdx.x & 31;
@@ -1814,8 +1817,6 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
                              const rkf_march_params* p, const rkf_batch_tuning& tu,
                              cudaStream_t st, DevBuf* seg_buf, unsigned long long* counter, uint64_t id0,
                              bool segs_resident) {
-  if (c->obj_count() > kMaxObjectsFast)
-    return fail(RKF_UNSUPPORTED, "march: more objects than the persistent kernel holds");
   if (c->obj_count() == 0) return fail(RKF_INVALID_ARG, "march: the scene has no objects");
   const bool tiled = p->strategy == RKF_STRATEGY_TILED;
   const bool use_bvh = p->strategy == RKF_STRATEGY_BVH;
@@ -1874,7 +1875,8 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
   RKF_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
   detail::KParams kp;
   std::memset(&kp, 0, sizeof(kp));
-  std::memcpy(kp.objs, c->objdev_host.data(), sizeof(ObjDev) * c->obj_count());
+  // beyond kMaxObjectsFast objects the kernel reads the device table
+  std::memcpy(kp.objs, c->objdev_host.data(), sizeof(ObjDev) * std::min<uint32_t>(c->obj_count(), kMaxObjectsFast));
   kp.s = c->scene_dev();
   kp.segs = seg_buf->as<Segment>();
   kp.nseg = static_cast<uint32_t>(segs_host.size());
@@ -1963,8 +1965,6 @@ rkf_status launch_persistent(Ctx* c, const std::vector<Segment>& segs_host, uint
 rkf_status check_persistent_scratch(const Ctx* c, const rkf_march_params* p, const rkf_batch_tuning& tu) {
   if (p->strategy != RKF_STRATEGY_BRUTE)
     return fail(RKF_UNSUPPORTED, "march: this launch path runs the brute strategy only");
-  if (c->obj_count() > kMaxObjectsFast)
-    return fail(RKF_UNSUPPORTED, "march: more objects than the persistent kernel holds");
   if (c->obj_count() == 0) return fail(RKF_INVALID_ARG, "march: the scene has no objects");
   const uint32_t threads = tu.threads_per_block ? tu.threads_per_block : 256;
   if (threads > 256 || threads % 32)
@@ -1984,7 +1984,8 @@ rkf_status launch_persistent_scratch(Ctx* c, const Segment* segs_host, uint32_t 
   RKF_CUDA_TRY(cudaMemsetAsync(dev_counter, 0, sizeof(unsigned long long), st));
   detail::KParams kp;
   std::memset(&kp, 0, sizeof(kp));
-  std::memcpy(kp.objs, c->objdev_host.data(), sizeof(ObjDev) * c->obj_count());
+  // beyond kMaxObjectsFast objects the kernel reads the device table
+  std::memcpy(kp.objs, c->objdev_host.data(), sizeof(ObjDev) * std::min<uint32_t>(c->obj_count(), kMaxObjectsFast));
   kp.s = c->scene_dev();
   kp.segs = dev_segs;
   kp.nseg = nseg;
