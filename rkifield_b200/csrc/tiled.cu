@@ -28,13 +28,14 @@ namespace rkf {
 
 namespace detail {
 
-constexpr uint32_t kMaxAabbs = 64;
+constexpr uint32_t kMaxAabbs = 256;  // objects of a tiled launch (28 B each in the launch parameters)
 
 struct Aabbs {
   float lo[kMaxAabbs][3], hi[kMaxAabbs][3];
   uint32_t none[kMaxAabbs];  // sdf_type NONE (skipped by the cull, kept by the field)
   uint32_t n;
 };
+static_assert(sizeof(Aabbs) <= 16384, "the AABB table must fit the kernel parameter space with room to spare");
 
 __global__ void k_coarse_build(const __grid_constant__ Aabbs a, float ox, float oy, float oz, uint32_t dx,
                                uint32_t dy, uint32_t dz, float vs, float start, uint16_t* __restrict__ tex) {

@@ -3,7 +3,7 @@ multi-object kernel reads the records from the device table.  The voxelized
 small scene beside 39 and 69 analytic primitives (spheres, boxes, capsules
 and a plane scattered through and around its grid), views under the brute,
 BVH and tiled strategies and ray casts in the three modes, bit-exact with
-the oracle; the tiled strategy's object table holds 64 objects and refuses
+the oracle; the tiled strategy's object table holds 256 objects and refuses
 more."""
 import numpy as np
 import pytest
@@ -47,7 +47,7 @@ def _context(small_scene, objs):
     return ctx
 
 
-@pytest.mark.parametrize("n_extra", [39, 69])
+@pytest.mark.parametrize("n_extra", [39, 69, 299])
 def test_many_objects_bit_exact(oracle, small_scene, n_extra):
     from rkifield_b200 import _abi as abi
     from rkifield_b200 import engine, scenes
@@ -64,7 +64,7 @@ def test_many_objects_bit_exact(oracle, small_scene, n_extra):
         for strategy in (abi.RKF_STRATEGY_BRUTE, abi.RKF_STRATEGY_BVH, abi.RKF_STRATEGY_TILED):
             p = _params(strategy)
             cam = scenes.camera_uniforms((45.0, 22.0, 55.0), (0.0, -4.0, 0.0), w, h)  # above the plane
-            if strategy == abi.RKF_STRATEGY_TILED and len(objs) > 64:
+            if strategy == abi.RKF_STRATEGY_TILED and len(objs) > 256:
                 with pytest.raises(RkfError) as e:
                     ctx.march(cam, p, w, h)
                 assert e.value.status == abi.RKF_UNSUPPORTED
