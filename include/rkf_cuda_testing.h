@@ -52,6 +52,13 @@ RKF_API int rkf_testing_last_variant(rkf_ctx* ctx);
  * transform, a non-positive scale or non-finite parameters. */
 RKF_API int rkf_testing_far_ball(const rkf_gpu_object* obj, float empty_hi, float out[5]);
 
+/* The multi-object empty-space path's half-space of an analytic plane, for
+ * EMPTY values up to empty_hi: out = {G x, y, z, H, a, b}; wherever a
+ * position w with |w|_1 <= P has G.w + H > a + b*P, the plane's value
+ * exceeds empty_hi.  Host only.  1 for a plane with a finite transform and
+ * a non-zero normal, else 0. */
+RKF_API int rkf_testing_far_plane(const rkf_gpu_object* obj, float empty_hi, float out[6]);
+
 /* Brick-pool and index-leaf bookkeeping: out = {pool capacity, live bricks
  * (pool_bricks_used), free slots, leaf blocks allocated, free leaf blocks}.
  * Slots neither live nor free are held for work of older epochs.  Read it

@@ -269,6 +269,7 @@ SIGNATURES = {
     "rkf_testing_export_coarse": (_I, [_P, _P, _P, _P, C.POINTER(C.c_uint64)]),
     "rkf_testing_last_variant": (C.c_int, [_P]),
     "rkf_testing_far_ball": (C.c_int, [_P, C.c_float, _P]),
+    "rkf_testing_far_plane": (C.c_int, [_P, C.c_float, _P]),
     "rkf_testing_pool_state": (_I, [_P, _P]),
     "rkf_testing_march_timing": (_I, [_P, C.c_uint32]),
     "rkf_testing_launch_stats": (_I, [_P, C.POINTER(C.c_uint64), _P, C.c_uint32, C.POINTER(C.c_uint32)]),

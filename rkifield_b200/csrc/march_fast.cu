@@ -2141,6 +2141,21 @@ extern "C" int rkf_testing_last_variant(rkf_ctx* ctx) {
   return ctx ? reinterpret_cast<rkf::Ctx*>(ctx)->last_variant : -1;
 }
 
+extern "C" int rkf_testing_far_plane(const rkf_gpu_object* obj, float empty_hi, float out[6]) {
+  if (!obj || !out) return 0;
+  const rkf::ObjDev od = rkf::make_objdev(*obj, 0, 0);
+  if (od.sdf_type != RKF_SDF_ANALYTICAL || od.prim_type != RKF_PRIM_PLANE) return 0;
+  rkf::detail::FarBall b;
+  if (!rkf::far_plane(od, empty_hi, &b)) return 0;
+  out[0] = b.c[0];
+  out[1] = b.c[1];
+  out[2] = b.c[2];
+  out[3] = b.h[0];
+  out[4] = b.a;
+  out[5] = b.b;
+  return 1;
+}
+
 extern "C" int rkf_testing_far_ball(const rkf_gpu_object* obj, float empty_hi, float out[5]) {
   if (!obj || !out) return 0;
   const rkf::ObjDev od = rkf::make_objdev(*obj, 0, 0);

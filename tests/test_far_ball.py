@@ -5,7 +5,9 @@ every FP32 value of evaluate_object exceeds the EMPTY values.  Checked here
 with the oracle's FP32 evaluation (bit-identical to the device's) at points
 just outside the balls of random spheres, boxes, capsules, tori and
 cylinders, rotated, non-uniformly scaled and moved; planes, singular
-transforms and non-positive scales have no ball.  Host only: no GPU."""
+transforms and non-positive scales have no ball.  A plane has a half-space
+instead (rkf_testing_far_plane), checked the same way just outside its
+boundary.  Host only: no GPU."""
 import ctypes as C
 
 import numpy as np
@@ -72,3 +74,60 @@ def test_objects_without_a_ball(oracle):
     assert _ball(lib, neg)[0] == 0  # min_scale <= 0
     inf = _transformed(1, (1.0, 2.0, 3.0), (np.inf, 1.0, 1.0), np.eye(3), (1.0, 1.0, 1.0), 1, 1)
     assert _ball(lib, inf)[0] == 0
+
+
+def _plane_bound(lib, obj, empty_hi=EMPTY_HI):
+    out = (C.c_float * 6)()
+    ok = lib.rkf_testing_far_plane(C.byref(obj), C.c_float(empty_hi), out)
+    v = np.array(out[:], np.float64)
+    return ok, v[:3], v[3], v[4], v[5]
+
+
+def test_plane_values_outside_the_half_space_exceed_the_empty_values(oracle):
+    """Random planes (normal, rotation, non-uniform scale, position): at FP32
+    points w just outside G.w + H = a + b |w|_1 -- the bound with P = |w|_1,
+    which bounds |o| + |d| |tmax| for a ray through w from the origin -- the
+    oracle's FP32 plane value (bit-identical to the device's) exceeds the
+    EMPTY values, and some of them come close (the bound is tight enough to
+    matter)."""
+    from rkifield_b200 import _abi as abi
+    lib = abi.load_library()
+    rng = np.random.default_rng(7)
+    worst = np.inf
+    for trial in range(120):
+        nrm = rng.normal(size=3)
+        if trial % 4 == 0:
+            nrm = np.eye(3)[trial % 3] * rng.choice([-1.0, 1.0])  # axis-aligned, as a ground plane
+        centre = tuple(float(x) for x in rng.uniform(-80.0, 80.0, 3))
+        scale = tuple(float(x) for x in rng.uniform(0.3, 3.0, 3)) if trial % 3 else (1.0, 1.0, 1.0)
+        rot = _rotation(rng.normal(size=3), rng.uniform(0, np.pi)) if trial % 2 else np.eye(3)
+        obj = _transformed(5, centre, tuple(float(x) for x in nrm) + (0.0,), rot, scale, 1, 1)
+        ok, G, H, a, b = _plane_bound(lib, obj)
+        assert ok, f"trial {trial}: no half-space"
+        assert np.linalg.norm(G) > 0 and a > EMPTY_HI
+        # points on the boundary (fixed point for the |w|_1 term), then just outside
+        q = rng.uniform(-150.0, 150.0, (3000, 3))
+        g2 = float(G @ G)
+        w = q.copy()
+        for _ in range(6):
+            k = a + b * np.abs(w).sum(axis=1)
+            w = q + ((k - (q @ G + H)) / g2)[:, None] * G
+        w = w + (1e-6 * (1.0 + np.abs(w).max(axis=1)) / np.sqrt(g2))[:, None] * G
+        pts = w.astype(np.float32)
+        outside = (pts.astype(np.float64) @ G + H) > a + b * np.abs(pts.astype(np.float64)).sum(axis=1)
+        assert outside.mean() > 0.99
+        d, _, _ = oracle.query_points(oracle.Scene([obj]), pts[outside].ravel())
+        assert (d > EMPTY_HI).all(), (trial, float(d.min()))
+        worst = min(worst, float(d.min()))
+    assert worst < 1.05 * EMPTY_HI, worst  # measured 0.16047 against 0.16000: the bound is tight
+
+
+def test_planes_without_a_half_space():
+    from rkifield_b200 import _abi as abi
+    lib = abi.load_library()
+    zero = _transformed(5, (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), np.eye(3), (1.0, 1.0, 1.0), 1, 1)
+    assert _plane_bound(lib, zero)[0] == 0  # no normal
+    sphere = _transformed(0, (1.0, 2.0, 3.0), (1.0,), np.eye(3), (1.0, 1.0, 1.0), 1, 1)
+    assert _plane_bound(lib, sphere)[0] == 0  # not a plane
+    neg = _transformed(5, (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), np.eye(3), (1.0, -1.0, 1.0), 1, 1)
+    assert _plane_bound(lib, neg)[0] == 0  # min_scale <= 0
