@@ -79,11 +79,19 @@ def test_march_argument_checks_leave_the_context_usable(small_scene):
         for k in before:
             assert_bits_equal(after[k], before[k], f"after refused calls: {k}")
 
-        # more objects than the persistent kernel's object table holds
+        # more objects than the launch parameters hold: marched from the
+        # device object table (tests/test_many_objects_gpu.py checks the
+        # values), and the tiled strategy refuses more than its 256
         many = list(objs) + [_analytic(0, (40.0 + 3 * i, 0.0, 0.0), (1.0,), (1.0, 1.0, 1.0), 5, 10 + i)
                              for i in range(33 - len(objs))]
         ctx.upload_objects(many)
-        assert _status(lambda: ctx.march(cam, p, w, h)) == abi.RKF_UNSUPPORTED
+        g33 = ctx.march(cam, p, w, h)
+        assert ctx.lib.rkf_testing_last_variant(ctx.h) == 0
+        assert (g33["flags"] & 1).any()
+        many = list(objs) + [_analytic(0, (40.0 + 3 * (i % 40), 3.0 * (i // 40), 0.0), (1.0,), (1.0, 1.0, 1.0), 5,
+                                       10 + i % 200) for i in range(257 - len(objs))]
+        ctx.upload_objects(many)
+        assert _status(lambda: ctx.march(cam, tiled, w, h)) == abi.RKF_UNSUPPORTED
         ctx.upload_objects(objs)
         again = ctx.march(cam, p, w, h)
         for k in before:
