@@ -121,7 +121,9 @@ typedef enum rkf_strategy {
     RKF_STRATEGY_BRUTE = 0,  /* ray_march_brute (:776-858): every object each */
                              /* step, in index order                          */
     RKF_STRATEGY_TILED = 1,  /* ray_march_tiled (:874-985): coarse-field skips */
-                             /* and per-16x16-tile object lists; views only   */
+                             /* and per-16x16-tile object lists; views only;  */
+                             /* at most 256 objects (RKF_UNSUPPORTED beyond;  */
+                             /* brute and BVH take any count)                 */
     RKF_STRATEGY_BVH = 2     /* ray_march_bvh (:641-773): each step walks the  */
                              /* imported BVH (rkf_bvh_import), skipping nodes */
                              /* farther than the best distance so far; views  */
